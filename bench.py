@@ -1,0 +1,321 @@
+"""Benchmark of the Fisher-Kolmogorov RD hot path on B200.
+
+One step = one pass of the fused RD kernel (ReactionDiffusionOperator<3> +
+UpdateTumor<3>) over the 256^3-equivalent frozen uniform topology of the
+adaptive FP32 configuration: 32768 blocks of 8^3 cells, FP32 storage (the
+reference's default Real), Dw = 0.2 cm^2/day, rho = 0.05/day, seeded synthetic
+anatomy.  ``value`` is whole-job cell-updates/s with the fields resident in
+HBM; ``e2e`` is the same metric through the public API with host buffers
+(H2D of phi, p_w, p_g and D2H of phi inside every timed step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gbfk|reference]
+
+Multi-GPU: one process per GPU (torchrun); a single solve does not shard
+(256^3 fits one GPU), so N GPUs run N independent replicas ("weak").
+``--impl reference`` times the reference's own CPU operators (oracle/_ref,
+threaded TBB stand-in) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from gliomasolver_b200.anatomy import make_case  # noqa: E402
+from gliomasolver_b200.schedule import make_schedule  # noqa: E402
+
+METRIC = "RD cell-updates/s & % HBM roofline"
+UNIT = "cell-updates/s"
+N_GRID = 256
+DW, RHO, TEND, L_CM = 0.2, 0.05, 300.0, 25.6
+SEED = 0
+CPU_SAMPLE_N = 64
+PROFILE_SUMMARY = ROOT / "profiles" / "rd_step_f32_n256.md"
+
+
+def workload_config(n, precision):
+    return {
+        "workload": f"fused RD step (ReactionDiffusionOperator<3> + UpdateTumor<3>), {n}^3 uniform frozen "
+                    f"topology, {(n // 8) ** 3} blocks of 8^3, {'FP32' if precision == 'f32' else 'FP64'} storage",
+        "n": n, "blocks": (n // 8) ** 3, "precision": precision,
+        "Dw_cm2_day": DW, "rho_day": RHO, "L_cm": L_CM, "anatomy_seed": SEED,
+        "l2": "inputs larger than L2: phi in/out + p_w + p_g = %d MB per step" % (16 * n ** 3 // 2 ** 20),
+    }
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per launch of the fused kernel from the committed ncu summary."""
+    if not PROFILE_SUMMARY.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", PROFILE_SUMMARY.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_run(steps, warmup, n_sample=CPU_SAMPLE_N, precision="f32", target_s=None):
+    """The reference's own operators on the host cores (oracle/_ref), else the
+    oracle restatement on one core.  Returns (record, kind, cores, n, steps)."""
+    from oracle import oracle as O
+
+    pw, pg, c0, _ = make_case(n_sample, SEED)
+    s = make_schedule(DW, RHO, TEND, L_CM, n_sample // 8, precision)
+    cores = os.cpu_count() or 1
+    if O.ref_available(precision):
+        if target_s is not None:
+            probe = O.ref_time(pw, pg, c0, s.Dw, s.Dg, s.rho, s.dt, 3, precision, threads=cores, warmup=1)
+            per = probe["seconds"] / 3
+            steps = int(max(3, min(2000, target_s / max(per, 1e-6))))
+        rec = O.ref_time(pw, pg, c0, s.Dw, s.Dg, s.rho, s.dt, steps, precision, threads=cores, warmup=warmup)
+        return rec, "reference", rec["threads"], n_sample, steps
+    R = np.float32 if precision == "f32" else np.float64
+    a, b, c = (x.astype(R) for x in (pw, pg, c0))
+    if target_s is not None:
+        t = time.perf_counter()
+        O.rd_steps_dense(a, b, c, s.Dw, s.Dg, s.rho, s.h, s.dt, 1)
+        steps = int(max(1, min(500, target_s / max(time.perf_counter() - t, 1e-6))))
+    O.rd_steps_dense(a, b, c, s.Dw, s.Dg, s.rho, s.h, s.dt, warmup)
+    t = time.perf_counter()
+    O.rd_steps_dense(a, b, c, s.Dw, s.Dg, s.rho, s.h, s.dt, steps)
+    dt = time.perf_counter() - t
+    cells = n_sample ** 3
+    return {"cells": cells, "steps": steps, "seconds": dt, "threads": 1,
+            "cell_updates_per_s": cells * steps / dt}, "port", 1, n_sample, steps
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n_sample = CPU_SAMPLE_N
+    # keep the whole run within a few minutes
+    rec, kind, cores, n_s, steps = cpu_reference_run(3, 1, n_sample, args.precision)
+    per_step = rec["seconds"] / rec["steps"]
+    if per_step * (args.steps + args.warmup) > 150:
+        n_sample = 32
+    rec, kind, cores, n_s, steps = cpu_reference_run(args.steps, args.warmup, n_sample, args.precision)
+    value = rec["cell_updates_per_s"]
+    sample = (f"{n_s}^3 uniform grid of the same synthetic anatomy (same brain fraction as {N_GRID}^3), "
+              f"{steps} timed steps after {args.warmup} warm-up steps, stepping loop only")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * rec["seconds"] / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
+        "data": "synthetic", "config": workload_config(N_GRID, args.precision),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    from gliomasolver_b200 import BlockPool
+    from gliomasolver_b200.build import build_library
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and world > 1:
+        print(f"WORLD_SIZE={world} but --gpus {args.gpus}", file=sys.stderr)
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    build_library()
+
+    n, prec = args.n, args.precision
+    R = np.float32 if prec == "f32" else np.float64
+    pw, pg, c0, _ = make_case(n, SEED)
+    pw, pg, c0 = (a.astype(R) for a in (pw, pg, c0))
+    s = make_schedule(DW, RHO, TEND, L_CM, n // 8, prec)
+    cells = n ** 3
+    stream = torch.cuda.current_stream()
+    pool = BlockPool((n // 8) ** 3, prec, device=local, stream=stream.cuda_stream)
+    pool.set_uniform(n // 8)
+    pool.upload_dense("p_w", pw)
+    pool.upload_dense("p_g", pg)
+    pool.upload_dense("phi", c0)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident throughput -------------------------------------
+    for _ in range(args.warmup):
+        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = pool.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = pool.launches - launches0
+    clk = clocks.stop()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * cells * args.steps / (ms / 1e3)
+
+    # ---- roofline of the fused kernel (one launch per step) --------------
+    word = 4 if prec == "f32" else 8
+    alg_bytes = 4 * word * cells  # read phi, p_w, p_g; write phi
+    kernel_s = (ms / 1e3) / max(launches, 1) if launches == args.steps else (ms / 1e3) / args.steps
+    achieved = alg_bytes / kernel_s / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profiled_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "algorithmic_bytes_per_launch": alg_bytes}
+
+    # ---- end to end through the public API with host buffers -------------
+    e2e_steps = max(1, min(args.steps, 50))
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    hpw, hpg, hphi = pin(pw), pin(pg), pin(c0)
+    hout = torch.empty((n, n, n), dtype=torch.float32 if prec == "f32" else torch.float64).pin_memory().numpy()
+    barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(e2e_steps):
+        pool.upload_dense("p_w", hpw)
+        pool.upload_dense("p_g", hpg)
+        pool.upload_dense("phi", hphi)
+        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1)
+        pool._check(pool.lib.gbfk_download_dense(pool.ctx, 0, hout.ctypes.data, n))
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = {"value": world * cells * e2e_steps / (ms_e2e / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": 3 * word * cells, "d2h_bytes_per_step": word * cells,
+           "steps": e2e_steps,
+           "api": "BlockPool.upload_dense x3 + rd_step + gbfk_download_dense (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rec, kind, cores, n_s, st = cpu_reference_run(0, 2, CPU_SAMPLE_N, prec, target_s=15.0)
+        cpu = {"value": rec["cell_updates_per_s"], "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"{n_s}^3 grid of the same synthetic anatomy, {st} steps of the stepping loop "
+                         f"({rec['seconds']:.1f} s) on {cores} host threads"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": prec, "data": "synthetic", "config": workload_config(n, prec),
+            "parallelism": "replicas" if world > 1 else "single",
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    pool.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="gbfk", choices=["gbfk", "reference"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--n", type=int, default=N_GRID)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,111 @@
+"""ctypes binding of libgbfk.so (the C ABI declared in include/gbfk.h).
+
+The library is built in-tree (``gliomasolver_b200/libgbfk.so``) by
+``gliomasolver_b200.build.build_library``.  There is no fallback: if the
+shared object is missing or does not load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libgbfk.so"
+
+GBFK_OK = 0
+STATUS = {
+    0: "GBFK_OK",
+    1: "GBFK_E_INVALID",
+    2: "GBFK_E_CUDA",
+    3: "GBFK_E_OOM",
+    4: "GBFK_E_NAN",
+    5: "GBFK_E_TIMEOUT",
+    6: "GBFK_E_STATE",
+}
+GBFK_F64, GBFK_F32 = 0, 1
+GBFK_PHI, GBFK_PW, GBFK_PG = 0, 1, 2
+
+# Every symbol include/gbfk.h declares (checked by the CPU test suite).
+EXPORTS = (
+    "gbfk_create", "gbfk_destroy", "gbfk_last_error", "gbfk_sync", "gbfk_launch_count",
+    "gbfk_set_uniform", "gbfk_set_topology", "gbfk_num_blocks",
+    "gbfk_upload_field", "gbfk_download_field", "gbfk_upload_dense", "gbfk_download_dense",
+    "gbfk_rd_step", "gbfk_rd_rhs", "gbfk_fwt_details", "gbfk_split", "gbfk_collapse",
+)
+
+
+class GbfkError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS.get(code, code)}: {message}")
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("precision", ctypes.c_int),
+        ("max_blocks", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("stream", ctypes.c_void_p),
+    ]
+
+
+class BlockInfo(ctypes.Structure):
+    _fields_ = [
+        ("slot", ctypes.c_int),
+        ("level", ctypes.c_int),
+        ("index", ctypes.c_int * 3),
+        ("h", ctypes.c_double),
+    ]
+
+
+class GhostCSR(ctypes.Structure):
+    _fields_ = [
+        ("nrows", ctypes.c_int64),
+        ("row_ptr", ctypes.c_void_p),
+        ("src", ctypes.c_void_p),
+        ("w0", ctypes.c_void_p),
+        ("w1", ctypes.c_void_p),
+        ("w2", ctypes.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def load(path: Path | str | None = None):
+    """Load libgbfk.so (once) and declare its signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ImportError(
+            f"{p} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+            "(the CUDA extension is required; there is no CPU fallback)")
+    L = ctypes.CDLL(str(p))
+    P, I, I64, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double
+    sig = {
+        "gbfk_create": (I, [ctypes.POINTER(Config), ctypes.POINTER(P)]),
+        "gbfk_destroy": (I, [P]),
+        "gbfk_last_error": (ctypes.c_char_p, [P]),
+        "gbfk_sync": (I, [P]),
+        "gbfk_launch_count": (I64, [P]),
+        "gbfk_set_uniform": (I, [P, I]),
+        "gbfk_set_topology": (I, [P, P, I, ctypes.POINTER(GhostCSR)]),
+        "gbfk_num_blocks": (I, [P]),
+        "gbfk_upload_field": (I, [P, I, P, I64, I64]),
+        "gbfk_download_field": (I, [P, I, P, I64, I64]),
+        "gbfk_upload_dense": (I, [P, I, P, I]),
+        "gbfk_download_dense": (I, [P, I, P, I]),
+        "gbfk_rd_step": (I, [P, D, D, D, D, I, I]),
+        "gbfk_rd_rhs": (I, [P, D, D, D, P]),
+        "gbfk_fwt_details": (I, [P, P]),
+        "gbfk_split": (I, [P, I, P, P]),
+        "gbfk_collapse": (I, [P, I, P, P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L

@@ -1,0 +1,718 @@
+// C ABI of the gbfk library (include/gbfk.h): context, topology, data
+// movement and the hot-path entry points.  Host code only; kernels live in
+// gbfk_kernels.cu.
+#include "gbfk.h"
+#include "gbfk_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace gbfk {
+cudaError_t upload_ghost_table();
+void init_ghost_table_host(short *table);
+}  // namespace gbfk
+
+using namespace gbfk;
+
+struct gbfk_ctx {
+    int precision = GBFK_F64;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int max_blocks = 0;
+    size_t rsize = 8;  // sizeof(Real)
+
+    // block pool (Real): phi is double-buffered across steps
+    void *phi[2] = {nullptr, nullptr};
+    int cur = 0;
+    void *pw = nullptr, *pg = nullptr;
+
+    // topology
+    int nblocks = 0;
+    bool have_topology = false;
+    bool uniform = false;
+    int bpd = 0;
+    std::vector<int> h_slot;
+    std::vector<double> h_h;
+    int *d_slot = nullptr;
+    int *d_nbr = nullptr;
+    void *d_h = nullptr;
+    // ghost CSR (rows = nblocks * 488)
+    bool have_csr = false;
+    int64_t nrows = 0;
+    int64_t *d_row_ptr = nullptr;
+    int *d_src = nullptr;
+    void *d_w = nullptr;
+    int *d_step_rows = nullptr;
+    int64_t n_step_rows = 0;
+    int *d_all_rows = nullptr;
+    void *d_gpw = nullptr, *d_gpg = nullptr, *d_gphi = nullptr;
+    bool static_ghosts_dirty = true;
+
+    // scratch
+    unsigned *d_nan = nullptr;
+    void *d_stage = nullptr;
+    size_t stage_bytes = 0;
+    double *d_fwt = nullptr;
+    int *d_ints = nullptr;
+    size_t ints_cap = 0;
+
+    int64_t launches = 0;
+    std::string err;
+};
+
+namespace {
+
+int fail(gbfk_ctx *c, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                      \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? GBFK_E_OOM : GBFK_E_CUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                           \
+    } while (0)
+
+std::mutex g_table_mutex;
+std::vector<int> g_table_ready;  // per device
+
+int ensure_table(gbfk_ctx *ctx)
+{
+    std::lock_guard<std::mutex> lk(g_table_mutex);
+    if ((int)g_table_ready.size() <= ctx->device) g_table_ready.resize(ctx->device + 1, 0);
+    if (!g_table_ready[ctx->device]) {
+        CK(upload_ghost_table());
+        g_table_ready[ctx->device] = 1;
+    }
+    return GBFK_OK;
+}
+
+void free_topology(gbfk_ctx *c)
+{
+    void **ptrs[] = {(void **)&c->d_slot, (void **)&c->d_nbr, &c->d_h, (void **)&c->d_row_ptr, (void **)&c->d_src,
+                     &c->d_w, (void **)&c->d_step_rows, (void **)&c->d_all_rows, &c->d_gpw, &c->d_gpg,
+                     &c->d_gphi, (void **)&c->d_fwt};
+    for (void **p : ptrs) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    c->have_topology = c->have_csr = c->uniform = false;
+    c->nblocks = 0;
+    c->nrows = c->n_step_rows = 0;
+    c->h_slot.clear();
+    c->h_h.clear();
+    c->static_ghosts_dirty = true;
+}
+
+template <typename Real>
+PoolView<Real> view(gbfk_ctx *c)
+{
+    PoolView<Real> v;
+    v.slot = c->d_slot;
+    v.nbr = c->d_nbr;
+    v.hblk = (const Real *)c->d_h;
+    v.gpw = (const Real *)c->d_gpw;
+    v.gpg = (const Real *)c->d_gpg;
+    v.gphi = (const Real *)c->d_gphi;
+    v.pw = (const Real *)c->pw;
+    v.pg = (const Real *)c->pg;
+    v.nblocks = c->nblocks;
+    return v;
+}
+
+int ints_scratch(gbfk_ctx *ctx, size_t n)
+{
+    if (ctx->ints_cap >= n) return GBFK_OK;
+    if (ctx->d_ints) cudaFree(ctx->d_ints);
+    ctx->d_ints = nullptr;
+    ctx->ints_cap = 0;
+    CK(cudaMalloc(&ctx->d_ints, n * sizeof(int)));
+    ctx->ints_cap = n;
+    return GBFK_OK;
+}
+
+// Lab positions of face f (0..5) in face_cell order, with the source cell in
+// the same-level neighbour.
+void face_positions(int f, int p, int &lx, int &ly, int &lz, int &src_cell)
+{
+    const int a = p & 7, b = p >> 3;
+    const int d = f >> 1, plus = f & 1;
+    const int c_lab = plus ? kBS : -1;
+    const int c_src = plus ? 0 : kBS - 1;
+    if (d == 0) { lx = c_lab; ly = a; lz = b; src_cell = c_src + kBS * (a + kBS * b); }
+    else if (d == 1) { lx = a; ly = c_lab; lz = b; src_cell = a + kBS * (c_src + kBS * b); }
+    else { lx = a; ly = b; lz = c_lab; src_cell = a + kBS * (b + kBS * c_src); }
+}
+
+inline int lab_idx(int x, int y, int z) { return (x + 1) + kLab * ((y + 1) + kLab * (z + 1)); }
+
+template <typename Real>
+int set_csr(gbfk_ctx *ctx, const std::vector<int64_t> &row_ptr, const std::vector<int> &src,
+            const std::vector<double> &w0, const std::vector<double> &w1, const std::vector<double> &w2,
+            bool detect_direct)
+{
+    const int nb = ctx->nblocks;
+    const int64_t nrows = (int64_t)nb * kLabGhosts;
+    const int64_t nnz = row_ptr[nrows];
+    std::vector<Real> w(nnz);
+    for (int64_t k = 0; k < nnz; k++) w[k] = ((Real)w0[k] * (Real)w1[k]) * (Real)w2[k];
+
+    short table[kLab3];
+    init_ghost_table_host(table);
+
+    // same-level faces: every row one entry of weight 1 from one neighbour
+    std::vector<int> nbr((size_t)nb * 6, -1);
+    std::vector<int> step_rows;
+    for (int b = 0; b < nb; b++) {
+        for (int f = 0; f < 6; f++) {
+            int nb_slot = -2;
+            bool direct = detect_direct;
+            for (int p = 0; p < kFaceCells && direct; p++) {
+                int lx, ly, lz, sc;
+                face_positions(f, p, lx, ly, lz, sc);
+                const int64_t r = (int64_t)b * kLabGhosts + table[lab_idx(lx, ly, lz)];
+                if (row_ptr[r + 1] - row_ptr[r] != 1) { direct = false; break; }
+                const int64_t k = row_ptr[r];
+                if (!(w[k] == (Real)1)) { direct = false; break; }
+                const int s = src[k] / kBS3, cell = src[k] % kBS3;
+                if (cell != sc) { direct = false; break; }
+                if (nb_slot == -2) nb_slot = s;
+                else if (nb_slot != s) { direct = false; break; }
+            }
+            if (direct) {
+                nbr[(size_t)b * 6 + f] = nb_slot;
+            } else {
+                for (int p = 0; p < kFaceCells; p++) {
+                    int lx, ly, lz, sc;
+                    face_positions(f, p, lx, ly, lz, sc);
+                    step_rows.push_back(b * kLabGhosts + table[lab_idx(lx, ly, lz)]);
+                }
+            }
+        }
+    }
+    std::vector<int> all_rows(nrows);
+    for (int64_t r = 0; r < nrows; r++) all_rows[r] = (int)r;
+
+    CK(cudaMalloc(&ctx->d_row_ptr, (nrows + 1) * sizeof(int64_t)));
+    CK(cudaMalloc(&ctx->d_src, std::max<int64_t>(nnz, 1) * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_w, std::max<int64_t>(nnz, 1) * sizeof(Real)));
+    CK(cudaMalloc(&ctx->d_nbr, (size_t)nb * 6 * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_all_rows, nrows * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_step_rows, std::max<size_t>(step_rows.size(), 1) * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_gpw, nrows * sizeof(Real)));
+    CK(cudaMalloc(&ctx->d_gpg, nrows * sizeof(Real)));
+    CK(cudaMalloc(&ctx->d_gphi, nrows * sizeof(Real)));
+    CK(cudaMemcpy(ctx->d_row_ptr, row_ptr.data(), (nrows + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
+    if (nnz) {
+        CK(cudaMemcpy(ctx->d_src, src.data(), nnz * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->d_w, w.data(), nnz * sizeof(Real), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemcpy(ctx->d_nbr, nbr.data(), (size_t)nb * 6 * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_all_rows, all_rows.data(), nrows * sizeof(int), cudaMemcpyHostToDevice));
+    if (!step_rows.empty())
+        CK(cudaMemcpy(ctx->d_step_rows, step_rows.data(), step_rows.size() * sizeof(int), cudaMemcpyHostToDevice));
+    ctx->n_step_rows = (int64_t)step_rows.size();
+    ctx->nrows = nrows;
+    ctx->have_csr = true;
+    ctx->static_ghosts_dirty = true;
+    return GBFK_OK;
+}
+
+// Same-level periodic ghost lists of a uniform grid, as the reference's
+// BBInfoCreator builds them for equal-level neighbours (one entry, weights
+// 1*1*1), so that the ghost-reading kernels (details, split) work on it.
+int build_uniform_csr(gbfk_ctx *ctx)
+{
+    const int bpd = ctx->bpd, nb = ctx->nblocks;
+    short table[kLab3];
+    init_ghost_table_host(table);
+    const int64_t nrows = (int64_t)nb * kLabGhosts;
+    std::vector<int64_t> row_ptr(nrows + 1);
+    std::vector<int> src(nrows);
+    std::vector<double> ones(nrows, 1.0);
+    for (int64_t r = 0; r <= nrows; r++) row_ptr[r] = r;
+    for (int bz = 0; bz < bpd; bz++)
+        for (int by = 0; by < bpd; by++)
+            for (int bx = 0; bx < bpd; bx++) {
+                const int b = bx + bpd * (by + bpd * bz);
+                for (int z = -1; z < 9; z++)
+                    for (int y = -1; y < 9; y++)
+                        for (int x = -1; x < 9; x++) {
+                            const int g = table[lab_idx(x, y, z)];
+                            if (g < 0) continue;
+                            const int gx = bx * 8 + x, gy = by * 8 + y, gz = bz * 8 + z;
+                            const int n = bpd * 8;
+                            const int wx = (gx + n) % n, wy = (gy + n) % n, wz = (gz + n) % n;
+                            const int sb = (wx >> 3) + bpd * ((wy >> 3) + bpd * (wz >> 3));
+                            src[(int64_t)b * kLabGhosts + g] = sb * kBS3 + (wx & 7) + 8 * ((wy & 7) + 8 * (wz & 7));
+                        }
+            }
+    if (ctx->d_nbr) { cudaFree(ctx->d_nbr); ctx->d_nbr = nullptr; }
+    return ctx->precision == GBFK_F64 ? set_csr<double>(ctx, row_ptr, src, ones, ones, ones, true)
+                                      : set_csr<float>(ctx, row_ptr, src, ones, ones, ones, true);
+}
+
+template <typename Real>
+int refresh_static_ghosts(gbfk_ctx *ctx)
+{
+    if (!ctx->have_csr || !ctx->static_ghosts_dirty) return GBFK_OK;
+    CK(launch_fill_ghosts<Real>(ctx->d_all_rows, ctx->nrows, ctx->d_row_ptr, ctx->d_src, (const Real *)ctx->d_w,
+                                (const Real *)ctx->pw, (Real *)ctx->d_gpw, ctx->stream));
+    CK(launch_fill_ghosts<Real>(ctx->d_all_rows, ctx->nrows, ctx->d_row_ptr, ctx->d_src, (const Real *)ctx->d_w,
+                                (const Real *)ctx->pg, (Real *)ctx->d_gpg, ctx->stream));
+    ctx->launches += 2;
+    ctx->static_ghosts_dirty = false;
+    return GBFK_OK;
+}
+
+template <typename Real>
+int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int nsteps, int check_nan)
+{
+    int rc = refresh_static_ghosts<Real>(ctx);
+    if (rc) return rc;
+    PoolView<Real> v = view<Real>(ctx);
+    if (check_nan) CK(cudaMemsetAsync(ctx->d_nan, 0, sizeof(unsigned), ctx->stream));
+    for (int s = 0; s < nsteps; s++) {
+        const Real *in = (const Real *)ctx->phi[ctx->cur];
+        Real *out = (Real *)ctx->phi[ctx->cur ^ 1];
+        if (ctx->n_step_rows > 0) {
+            CK(launch_fill_ghosts<Real>(ctx->d_step_rows, ctx->n_step_rows, ctx->d_row_ptr, ctx->d_src,
+                                        (const Real *)ctx->d_w, in, (Real *)ctx->d_gphi, ctx->stream));
+            ctx->launches++;
+        }
+        CK(launch_rd_step<Real>(v, in, out, nullptr, (Real)Dw, (Real)Dg, (Real)rho, dt, ctx->d_nan, ctx->stream));
+        ctx->launches++;
+        ctx->cur ^= 1;
+    }
+    if (check_nan) {
+        unsigned flag = 0;
+        CK(cudaMemcpyAsync(&flag, ctx->d_nan, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (flag) return fail(ctx, GBFK_E_NAN, "phi became NaN during the step");
+    }
+    return GBFK_OK;
+}
+
+template <typename Real>
+int rd_rhs_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, void *host)
+{
+    int rc = refresh_static_ghosts<Real>(ctx);
+    if (rc) return rc;
+    const size_t bytes = (size_t)ctx->nblocks * kBS3 * sizeof(Real);
+    Real *d_out = nullptr;
+    CK(cudaMalloc(&d_out, bytes));
+    PoolView<Real> v = view<Real>(ctx);
+    const Real *in = (const Real *)ctx->phi[ctx->cur];
+    cudaError_t e = cudaSuccess;
+    if (ctx->n_step_rows > 0) {
+        e = launch_fill_ghosts<Real>(ctx->d_step_rows, ctx->n_step_rows, ctx->d_row_ptr, ctx->d_src,
+                                     (const Real *)ctx->d_w, in, (Real *)ctx->d_gphi, ctx->stream);
+        ctx->launches++;
+    }
+    if (e == cudaSuccess) {
+        e = launch_rd_step<Real>(v, in, nullptr, d_out, (Real)Dw, (Real)Dg, (Real)rho, 0.0, ctx->d_nan, ctx->stream);
+        ctx->launches++;
+    }
+    // dphidt leaves in topology order: block i's 512 cells at i*512
+    if (e == cudaSuccess) {
+        for (int i = 0; i < ctx->nblocks && e == cudaSuccess; i++)
+            e = cudaMemcpyAsync((char *)host + (size_t)i * kBS3 * sizeof(Real),
+                                (const char *)d_out + (size_t)ctx->h_slot[i] * kBS3 * sizeof(Real),
+                                kBS3 * sizeof(Real), cudaMemcpyDeviceToHost, ctx->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_out);
+    CK(e);
+    return GBFK_OK;
+}
+
+template <typename Real>
+int fwt_impl(gbfk_ctx *ctx, double *out)
+{
+    if (!ctx->have_csr && ctx->uniform) {
+        int rc = build_uniform_csr(ctx);
+        if (rc) return rc;
+    }
+    int rc = refresh_static_ghosts<Real>(ctx);
+    if (rc) return rc;
+    const Real *phi = (const Real *)ctx->phi[ctx->cur];
+    CK(launch_fill_ghosts<Real>(ctx->d_all_rows, ctx->nrows, ctx->d_row_ptr, ctx->d_src, (const Real *)ctx->d_w,
+                                phi, (Real *)ctx->d_gphi, ctx->stream));
+    if (!ctx->d_fwt) CK(cudaMalloc(&ctx->d_fwt, (size_t)ctx->nblocks * sizeof(double)));
+    CK(launch_fwt_details<Real>(view<Real>(ctx), phi, ctx->d_fwt, ctx->stream));
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(out, ctx->d_fwt, (size_t)ctx->nblocks * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GBFK_OK;
+}
+
+template <typename Real>
+int split_impl(gbfk_ctx *ctx, int nsplit, const int *parents, const int *children)
+{
+    if (!ctx->have_csr && ctx->uniform) {
+        int rc = build_uniform_csr(ctx);
+        if (rc) return rc;
+    }
+    int rc = refresh_static_ghosts<Real>(ctx);
+    if (rc) return rc;
+    for (int i = 0; i < nsplit; i++) {
+        if (parents[i] < 0 || parents[i] >= ctx->nblocks)
+            return fail(ctx, GBFK_E_INVALID, "split: parent %d is not a block of the topology", parents[i]);
+        for (int c = 0; c < 8; c++)
+            if (children[8 * i + c] < 0 || children[8 * i + c] >= ctx->max_blocks)
+                return fail(ctx, GBFK_E_INVALID, "split: child slot %d out of range", children[8 * i + c]);
+    }
+    const Real *phi = (const Real *)ctx->phi[ctx->cur];
+    CK(launch_fill_ghosts<Real>(ctx->d_all_rows, ctx->nrows, ctx->d_row_ptr, ctx->d_src, (const Real *)ctx->d_w,
+                                phi, (Real *)ctx->d_gphi, ctx->stream));
+    rc = ints_scratch(ctx, (size_t)nsplit * 9);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->d_ints, parents, nsplit * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_ints + nsplit, children, (size_t)nsplit * 8 * sizeof(int), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(launch_split<Real>(view<Real>(ctx), nsplit, ctx->d_ints, ctx->d_ints + nsplit, (Real *)ctx->phi[ctx->cur],
+                          (Real *)ctx->pw, (Real *)ctx->pg, ctx->stream));
+    ctx->launches += 2;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GBFK_OK;
+}
+
+template <typename Real>
+int collapse_impl(gbfk_ctx *ctx, int n, const int *children, const int *parents)
+{
+    for (int i = 0; i < n; i++) {
+        if (parents[i] < 0 || parents[i] >= ctx->max_blocks)
+            return fail(ctx, GBFK_E_INVALID, "collapse: parent slot %d out of range", parents[i]);
+        for (int c = 0; c < 8; c++)
+            if (children[8 * i + c] < 0 || children[8 * i + c] >= ctx->max_blocks)
+                return fail(ctx, GBFK_E_INVALID, "collapse: child slot %d out of range", children[8 * i + c]);
+    }
+    int rc = ints_scratch(ctx, (size_t)n * 9);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->d_ints, children, (size_t)n * 8 * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_ints + (size_t)n * 8, parents, n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_collapse<Real>(n, ctx->d_ints, ctx->d_ints + (size_t)n * 8, (Real *)ctx->phi[ctx->cur],
+                             (Real *)ctx->pw, (Real *)ctx->pg, ctx->stream));
+    ctx->launches++;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GBFK_OK;
+}
+
+void *field_ptr(gbfk_ctx *c, int field)
+{
+    switch (field) {
+    case GBFK_PHI: return c->phi[c->cur];
+    case GBFK_PW: return c->pw;
+    case GBFK_PG: return c->pg;
+    default: return nullptr;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int gbfk_create(const gbfk_config *cfg, gbfk_ctx **out)
+{
+    if (!cfg || !out) return GBFK_E_INVALID;
+    *out = nullptr;
+    if (cfg->precision != GBFK_F64 && cfg->precision != GBFK_F32) return GBFK_E_INVALID;
+    if (cfg->max_blocks <= 0 || (int64_t)cfg->max_blocks * kBS3 > INT32_MAX) return GBFK_E_INVALID;
+    gbfk_ctx *ctx = new gbfk_ctx();
+    ctx->precision = cfg->precision;
+    ctx->rsize = cfg->precision == GBFK_F64 ? sizeof(double) : sizeof(float);
+    ctx->device = cfg->device;
+    ctx->max_blocks = cfg->max_blocks;
+    auto bail = [&](int rc) {
+        gbfk_destroy(ctx);
+        return rc;
+    };
+    if (cudaSetDevice(cfg->device) != cudaSuccess) return bail(GBFK_E_CUDA);
+    if (cfg->stream) {
+        ctx->stream = (cudaStream_t)cfg->stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GBFK_E_CUDA);
+        ctx->own_stream = true;
+    }
+    const size_t bytes = (size_t)cfg->max_blocks * kBS3 * ctx->rsize;
+    if (cudaMalloc(&ctx->phi[0], bytes) != cudaSuccess || cudaMalloc(&ctx->phi[1], bytes) != cudaSuccess ||
+        cudaMalloc(&ctx->pw, bytes) != cudaSuccess || cudaMalloc(&ctx->pg, bytes) != cudaSuccess ||
+        cudaMalloc(&ctx->d_nan, sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(GBFK_E_OOM);
+    }
+    cudaMemset(ctx->phi[0], 0, bytes);
+    cudaMemset(ctx->phi[1], 0, bytes);
+    cudaMemset(ctx->pw, 0, bytes);
+    cudaMemset(ctx->pg, 0, bytes);
+    cudaMemset(ctx->d_nan, 0, sizeof(unsigned));
+    if (ensure_table(ctx) != GBFK_OK) return bail(GBFK_E_CUDA);
+    *out = ctx;
+    return GBFK_OK;
+}
+
+int gbfk_destroy(gbfk_ctx *ctx)
+{
+    if (!ctx) return GBFK_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_topology(ctx);
+    void *ptrs[] = {ctx->phi[0], ctx->phi[1], ctx->pw, ctx->pg, ctx->d_nan, ctx->d_stage, ctx->d_ints};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return GBFK_OK;
+}
+
+const char *gbfk_last_error(const gbfk_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int gbfk_sync(gbfk_ctx *ctx)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GBFK_OK;
+}
+
+int64_t gbfk_launch_count(const gbfk_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int gbfk_num_blocks(const gbfk_ctx *ctx) { return ctx ? ctx->nblocks : 0; }
+
+int gbfk_set_uniform(gbfk_ctx *ctx, int bpd)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (bpd <= 0 || (int64_t)bpd * bpd * bpd > ctx->max_blocks)
+        return fail(ctx, GBFK_E_INVALID, "uniform grid of %d^3 blocks does not fit %d slots", bpd, ctx->max_blocks);
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    free_topology(ctx);
+    const int nb = bpd * bpd * bpd;
+    ctx->nblocks = nb;
+    ctx->bpd = bpd;
+    ctx->uniform = true;
+    ctx->h_slot.resize(nb);
+    std::vector<int> nbr((size_t)nb * 6);
+    for (int bz = 0; bz < bpd; bz++)
+        for (int by = 0; by < bpd; by++)
+            for (int bx = 0; bx < bpd; bx++) {
+                const int b = bx + bpd * (by + bpd * bz);
+                ctx->h_slot[b] = b;
+                auto id = [&](int x, int y, int z) {
+                    x = (x + bpd) % bpd; y = (y + bpd) % bpd; z = (z + bpd) % bpd;
+                    return x + bpd * (y + bpd * z);
+                };
+                int *n = &nbr[(size_t)b * 6];
+                n[0] = id(bx - 1, by, bz); n[1] = id(bx + 1, by, bz);
+                n[2] = id(bx, by - 1, bz); n[3] = id(bx, by + 1, bz);
+                n[4] = id(bx, by, bz - 1); n[5] = id(bx, by, bz + 1);
+            }
+    const double h = 1.0 / (8.0 * bpd);
+    ctx->h_h.assign(nb, h);
+    CK(cudaMalloc(&ctx->d_slot, nb * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_nbr, (size_t)nb * 6 * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_h, nb * ctx->rsize));
+    CK(cudaMemcpy(ctx->d_slot, ctx->h_slot.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_nbr, nbr.data(), (size_t)nb * 6 * sizeof(int), cudaMemcpyHostToDevice));
+    if (ctx->precision == GBFK_F64) {
+        std::vector<double> hv(nb, h);
+        CK(cudaMemcpy(ctx->d_h, hv.data(), nb * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> hv(nb, (float)h);
+        CK(cudaMemcpy(ctx->d_h, hv.data(), nb * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    ctx->have_topology = true;
+    return GBFK_OK;
+}
+
+int gbfk_set_topology(gbfk_ctx *ctx, const gbfk_blockinfo *blocks, int nblocks, const gbfk_ghost_csr *g)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!blocks || !g || nblocks <= 0) return fail(ctx, GBFK_E_INVALID, "set_topology: null or empty input");
+    if (nblocks > ctx->max_blocks) return fail(ctx, GBFK_E_OOM, "set_topology: %d blocks > %d slots", nblocks, ctx->max_blocks);
+    if (g->nrows != (int64_t)nblocks * kLabGhosts)
+        return fail(ctx, GBFK_E_INVALID, "set_topology: %lld ghost rows, expected %d*488", (long long)g->nrows, nblocks);
+    std::vector<char> used(ctx->max_blocks, 0);
+    for (int i = 0; i < nblocks; i++) {
+        const int s = blocks[i].slot;
+        if (s < 0 || s >= ctx->max_blocks || used[s])
+            return fail(ctx, GBFK_E_INVALID, "set_topology: bad or repeated slot %d", s);
+        used[s] = 1;
+    }
+    const int64_t nnz = g->row_ptr[g->nrows];
+    if (g->row_ptr[0] != 0 || nnz < 0) return fail(ctx, GBFK_E_INVALID, "set_topology: malformed row_ptr");
+    std::vector<int> src(nnz);
+    for (int64_t k = 0; k < nnz; k++) {
+        const int64_t s = g->src[k];
+        if (s < 0 || s >= (int64_t)ctx->max_blocks * kBS3 || !used[s / kBS3])
+            return fail(ctx, GBFK_E_INVALID, "set_topology: ghost source %lld is not in a current block", (long long)s);
+        src[k] = (int)s;
+    }
+    for (int64_t r = 0; r < g->nrows; r++)
+        if (g->row_ptr[r + 1] < g->row_ptr[r]) return fail(ctx, GBFK_E_INVALID, "set_topology: row_ptr not monotone");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    free_topology(ctx);
+    ctx->nblocks = nblocks;
+    ctx->h_slot.resize(nblocks);
+    ctx->h_h.resize(nblocks);
+    for (int i = 0; i < nblocks; i++) {
+        ctx->h_slot[i] = blocks[i].slot;
+        ctx->h_h[i] = blocks[i].h;
+    }
+    CK(cudaMalloc(&ctx->d_slot, nblocks * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_h, nblocks * ctx->rsize));
+    CK(cudaMemcpy(ctx->d_slot, ctx->h_slot.data(), nblocks * sizeof(int), cudaMemcpyHostToDevice));
+    if (ctx->precision == GBFK_F64) {
+        CK(cudaMemcpy(ctx->d_h, ctx->h_h.data(), nblocks * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> hv(nblocks);
+        for (int i = 0; i < nblocks; i++) hv[i] = (float)ctx->h_h[i];
+        CK(cudaMemcpy(ctx->d_h, hv.data(), nblocks * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    std::vector<int64_t> row_ptr(g->row_ptr, g->row_ptr + g->nrows + 1);
+    std::vector<double> w0(g->w0, g->w0 + nnz), w1(g->w1, g->w1 + nnz), w2(g->w2, g->w2 + nnz);
+    int rc = ctx->precision == GBFK_F64 ? set_csr<double>(ctx, row_ptr, src, w0, w1, w2, true)
+                                        : set_csr<float>(ctx, row_ptr, src, w0, w1, w2, true);
+    if (rc) return rc;
+    ctx->have_topology = true;
+    return GBFK_OK;
+}
+
+int gbfk_upload_field(gbfk_ctx *ctx, int field, const void *host, int64_t first, int64_t ncells)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    void *p = field_ptr(ctx, field);
+    if (!p || !host || first < 0 || ncells < 0 || first + ncells > (int64_t)ctx->max_blocks * kBS3)
+        return fail(ctx, GBFK_E_INVALID, "upload_field: bad field or range");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync((char *)p + first * ctx->rsize, host, ncells * ctx->rsize, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    if (field != GBFK_PHI) ctx->static_ghosts_dirty = true;
+    return GBFK_OK;
+}
+
+int gbfk_download_field(gbfk_ctx *ctx, int field, void *host, int64_t first, int64_t ncells)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    void *p = field_ptr(ctx, field);
+    if (!p || !host || first < 0 || ncells < 0 || first + ncells > (int64_t)ctx->max_blocks * kBS3)
+        return fail(ctx, GBFK_E_INVALID, "download_field: bad field or range");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(host, (const char *)p + first * ctx->rsize, ncells * ctx->rsize, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GBFK_OK;
+}
+
+static int dense_io(gbfk_ctx *ctx, int field, void *host, int n, bool up)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!ctx->uniform || n != 8 * ctx->bpd)
+        return fail(ctx, GBFK_E_STATE, "dense transfer needs a uniform topology with n = 8*bpd");
+    void *p = field_ptr(ctx, field);
+    if (!p || !host) return fail(ctx, GBFK_E_INVALID, "dense transfer: bad field or buffer");
+    CK(cudaSetDevice(ctx->device));
+    const size_t bytes = (size_t)n * n * n * ctx->rsize;
+    if (ctx->stage_bytes < bytes) {
+        if (ctx->d_stage) cudaFree(ctx->d_stage);
+        ctx->d_stage = nullptr;
+        ctx->stage_bytes = 0;
+        CK(cudaMalloc(&ctx->d_stage, bytes));
+        ctx->stage_bytes = bytes;
+    }
+    if (up) {
+        CK(cudaMemcpyAsync(ctx->d_stage, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        if (ctx->precision == GBFK_F64)
+            CK(launch_dense_scatter<double>((const double *)ctx->d_stage, (double *)p, n, true, ctx->stream));
+        else
+            CK(launch_dense_scatter<float>((const float *)ctx->d_stage, (float *)p, n, true, ctx->stream));
+        ctx->launches++;
+        if (field != GBFK_PHI) ctx->static_ghosts_dirty = true;
+    } else {
+        if (ctx->precision == GBFK_F64)
+            CK(launch_dense_scatter<double>((const double *)p, (double *)ctx->d_stage, n, false, ctx->stream));
+        else
+            CK(launch_dense_scatter<float>((const float *)p, (float *)ctx->d_stage, n, false, ctx->stream));
+        ctx->launches++;
+        CK(cudaMemcpyAsync(host, ctx->d_stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return GBFK_OK;
+}
+
+int gbfk_upload_dense(gbfk_ctx *ctx, int field, const void *host, int n)
+{
+    return dense_io(ctx, field, const_cast<void *>(host), n, true);
+}
+
+int gbfk_download_dense(gbfk_ctx *ctx, int field, void *host, int n) { return dense_io(ctx, field, host, n, false); }
+
+int gbfk_rd_step(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int nsteps, int check_nan)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!ctx->have_topology) return fail(ctx, GBFK_E_STATE, "rd_step: no topology");
+    if (nsteps < 0) return fail(ctx, GBFK_E_INVALID, "rd_step: negative step count");
+    CK(cudaSetDevice(ctx->device));
+    return ctx->precision == GBFK_F64 ? rd_step_impl<double>(ctx, Dw, Dg, rho, dt, nsteps, check_nan)
+                                      : rd_step_impl<float>(ctx, Dw, Dg, rho, dt, nsteps, check_nan);
+}
+
+int gbfk_rd_rhs(gbfk_ctx *ctx, double Dw, double Dg, double rho, void *host)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!ctx->have_topology) return fail(ctx, GBFK_E_STATE, "rd_rhs: no topology");
+    if (!host) return fail(ctx, GBFK_E_INVALID, "rd_rhs: null output");
+    CK(cudaSetDevice(ctx->device));
+    return ctx->precision == GBFK_F64 ? rd_rhs_impl<double>(ctx, Dw, Dg, rho, host)
+                                      : rd_rhs_impl<float>(ctx, Dw, Dg, rho, host);
+}
+
+int gbfk_fwt_details(gbfk_ctx *ctx, double *out)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!ctx->have_topology) return fail(ctx, GBFK_E_STATE, "fwt_details: no topology");
+    if (!out) return fail(ctx, GBFK_E_INVALID, "fwt_details: null output");
+    CK(cudaSetDevice(ctx->device));
+    return ctx->precision == GBFK_F64 ? fwt_impl<double>(ctx, out) : fwt_impl<float>(ctx, out);
+}
+
+int gbfk_split(gbfk_ctx *ctx, int nsplit, const int *parents, const int *children)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!ctx->have_topology) return fail(ctx, GBFK_E_STATE, "split: no topology");
+    if (nsplit < 0 || (nsplit && (!parents || !children))) return fail(ctx, GBFK_E_INVALID, "split: bad arguments");
+    if (nsplit == 0) return GBFK_OK;
+    CK(cudaSetDevice(ctx->device));
+    return ctx->precision == GBFK_F64 ? split_impl<double>(ctx, nsplit, parents, children)
+                                      : split_impl<float>(ctx, nsplit, parents, children);
+}
+
+int gbfk_collapse(gbfk_ctx *ctx, int n, const int *children, const int *parents)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (n < 0 || (n && (!parents || !children))) return fail(ctx, GBFK_E_INVALID, "collapse: bad arguments");
+    if (n == 0) return GBFK_OK;
+    CK(cudaSetDevice(ctx->device));
+    return ctx->precision == GBFK_F64 ? collapse_impl<double>(ctx, n, children, parents)
+                                      : collapse_impl<float>(ctx, n, children, parents);
+}
+
+}  // extern "C"

@@ -1,0 +1,161 @@
+/*
+ * gbfk -- B200-native Fisher-Kolmogorov reaction-diffusion step on MRAG's
+ * block grid (GliomaSolver's RD hot path), C ABI.
+ *
+ * The reference runs the path as two block sweeps issued by
+ * Glioma_ReactionDiffusion::_reactionDiffusionStep
+ * (Glioma/Glioma_ReactionDiffusion.cpp:176-187):
+ *   blockProcessing.pipeline_process(vInfo, collection, boundaryInfo,
+ *                                    ReactionDiffusionOperator<3>(Dw, Dg, rho));
+ *   BlockProcessing::process(vInfo, collection, UpdateTumor<3>(dt), gran);
+ * with ghost cells reconstructed per block by BlockLab::load
+ * (MRAG/MRAGcore/MRAGBlockLab.h:154-301) from BoundaryInfoBlock instruction
+ * lists (MRAG/MRAGcore/MRAGBoundaryBlockInfo.h:69-176).  This library keeps
+ * the block data resident in GPU memory and replaces those sweeps, the ghost
+ * reconstruction, the wavelet detail sweep that drives refinement
+ * (MRAG/MRAGcore/MRAGBlockFWT.h:447-478) and the split/collapse data movement
+ * (MRAG/MRAGcore/MRAGBlockSplitter.h:24-99, MRAGBlockCollapser.h:22-84).
+ * The block tree and the refine/compress planning stay with the caller.
+ *
+ * Conventions
+ *  - Every function returns GBFK_OK (0) or a GBFK_E_* code; the message of
+ *    the last failure is gbfk_last_error(ctx).  Nothing aborts.
+ *  - A context owns one CUDA stream; calls on one context are serialised by
+ *    the caller; different contexts may be used from different threads.
+ *  - Work is asynchronous on the context's stream; gbfk_sync waits.
+ *  - "Real" is the precision the context was created with: double
+ *    (GBFK_F64, the reference built with -D_MRAG_REAL_=double) or float
+ *    (GBFK_F32, the reference's default Real, MRAG/MRAGcore/MRAGCommon.h:43-47).
+ *    Host buffers passed to upload/download functions hold Real values.
+ *  - Block data: 8x8x8 cells per block, x fastest (MRAG/MRAGcore/MRAGBlock.h:40).
+ *    A pool "slot" holds one block; cell c of slot s is element s*512 + c.
+ */
+#ifndef GBFK_H
+#define GBFK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GBFK_BLOCK_SIZE 8
+#define GBFK_BLOCK_CELLS 512
+#define GBFK_LAB_GHOSTS 488 /* (8+2)^3 - 8^3 ghosts of a lab with stencil [-1,2) */
+
+enum gbfk_status {
+    GBFK_OK = 0,
+    GBFK_E_INVALID = 1, /* bad argument or call order */
+    GBFK_E_CUDA = 2,    /* a CUDA runtime call failed */
+    GBFK_E_OOM = 3,     /* device allocation failed or pool too small */
+    GBFK_E_NAN = 4,     /* a step produced NaN/Inf in phi */
+    GBFK_E_TIMEOUT = 5, /* a bounded device wait gave up */
+    GBFK_E_STATE = 6    /* required data (topology, fields) not uploaded */
+};
+
+enum gbfk_precision { GBFK_F64 = 0, GBFK_F32 = 1 };
+
+/* Fields of the reference's Cell (Glioma/Glioma_Types.h:21-59) that the path uses. */
+enum gbfk_field { GBFK_PHI = 0, GBFK_PW = 1, GBFK_PG = 2 };
+
+typedef struct gbfk_ctx gbfk_ctx;
+
+typedef struct {
+    int precision;  /* enum gbfk_precision */
+    int max_blocks; /* pool capacity in blocks (slots) */
+    int device;     /* CUDA device ordinal */
+    void *stream;   /* cudaStream_t to use, or NULL for a context-owned stream */
+} gbfk_config;
+
+/* One leaf block, as MRAG::BlockInfo (MRAG/MRAGcore/MRAGCommon.h:166-260). */
+typedef struct {
+    int slot;        /* pool slot holding the block's data */
+    int level;       /* BlockInfo::level */
+    int index[3];    /* BlockInfo::index */
+    double h;        /* BlockInfo::h[0]: grid spacing, 2^-level / 8 */
+} gbfk_blockinfo;
+
+/* Ghost reconstruction lists of every block, flattened from
+ * BoundaryInfoBlock (MRAGBoundaryBlockInfo.h:69-176).  Block i of the
+ * topology owns rows [i*488, (i+1)*488), in the order BlockLab::load visits
+ * its ghosts (MRAGBlockLab.h:256-279: codes 0..26 without 13, then z, y, x of
+ * the code's region) for the lab range [-1, 9)^3.  Row r's value is
+ *   ghost = 0; for k in [row_ptr[r], row_ptr[r+1]): ghost += field[src[k]] * w(k)
+ * with w(k) = (Real(w0[k]) * Real(w1[k])) * Real(w2[k]) in Real, exactly as
+ * BlockLab::load (MRAGBlockLab.h:286-291).  src[k] = slot * 512 + cell. */
+typedef struct {
+    int64_t nrows;          /* = nblocks * 488 */
+    const int64_t *row_ptr; /* nrows + 1 */
+    const int64_t *src;
+    const double *w0, *w1, *w2;
+} gbfk_ghost_csr;
+
+/* --- context ---------------------------------------------------------- */
+/* Replaces the BlockCollection + BlockProcessing objects of the driver
+ * (Glioma/Glioma_ReactionDiffusion.h:18-19). */
+int gbfk_create(const gbfk_config *cfg, gbfk_ctx **out);
+int gbfk_destroy(gbfk_ctx *ctx);
+const char *gbfk_last_error(const gbfk_ctx *ctx);
+int gbfk_sync(gbfk_ctx *ctx);
+/* Kernels this context launched since it was created (a launch counter). */
+int64_t gbfk_launch_count(const gbfk_ctx *ctx);
+
+/* --- topology --------------------------------------------------------- */
+/* A uniform, periodic bpd^3 grid of one level (MRAG::Grid(bpd,bpd,bpd),
+ * MRAG/MRAGcore/MRAGrid.inl:57-111 with periodic ghosts :930-1076); block
+ * (bx,by,bz) lives in slot bx + bpd*(by + bpd*bz); h = 1/(8*bpd). */
+int gbfk_set_uniform(gbfk_ctx *ctx, int bpd);
+/* Any leaf set with its ghost lists (Grid::getBlocksInfo +
+ * Grid::getBoundaryInfo, MRAGrid.inl:190-219,514-560). */
+int gbfk_set_topology(gbfk_ctx *ctx, const gbfk_blockinfo *blocks, int nblocks,
+                      const gbfk_ghost_csr *ghosts);
+int gbfk_num_blocks(const gbfk_ctx *ctx);
+
+/* --- data ------------------------------------------------------------- */
+/* Copy ncells Real values between host memory and the pool, starting at
+ * pool element first_cell (= slot * 512 + cell). */
+int gbfk_upload_field(gbfk_ctx *ctx, int field, const void *host, int64_t first_cell,
+                      int64_t ncells);
+int gbfk_download_field(gbfk_ctx *ctx, int field, void *host, int64_t first_cell,
+                        int64_t ncells);
+/* Uniform grids only: a dense n^3 volume (x fastest, n = 8*bpd) of Real,
+ * scattered into / gathered from the blocks on the device. */
+int gbfk_upload_dense(gbfk_ctx *ctx, int field, const void *host, int n);
+int gbfk_download_dense(gbfk_ctx *ctx, int field, void *host, int n);
+
+/* --- the hot path ----------------------------------------------------- */
+/* nsteps explicit Euler steps: each is ReactionDiffusionOperator<3>(Dw,Dg,rho)
+ * over all blocks (Glioma/Operators/ReactionDiffusionOperator.h:47-138)
+ * followed by UpdateTumor<3>(dt) (:189-226), fused into one kernel per step
+ * (plus a ghost fill of phi where the grid has coarse-fine faces).  Dw, Dg,
+ * rho are the rescaled Real values of Glioma_ReactionDiffusion::run
+ * (Glioma_ReactionDiffusion.cpp:302-307).  If check_nan is non-zero the call
+ * synchronises and returns GBFK_E_NAN when phi became NaN/Inf. */
+int gbfk_rd_step(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int nsteps,
+                 int check_nan);
+/* The operator alone: writes dphidt (Real, pool order, nblocks*512 cells) to
+ * host memory; phi is unchanged.  (ReactionDiffusionOperator.h:47-138.) */
+int gbfk_rd_rhs(gbfk_ctx *ctx, double Dw, double Dg, double rho, void *host_dphidt);
+
+/* --- adaptivity ------------------------------------------------------- */
+/* Per block of the topology (in upload order) the max |detail| of the
+ * one-level interpolating-wavelet transform of phi, as
+ * FWTReport::getOverAll_DetailMaxMag after BlockFWT::multichannel_fwt<0,0>
+ * (MRAG/MRAGcore/MRAGBlockFWT.h:109-120,219-298,447-478).  out: nblocks doubles. */
+int gbfk_fwt_details(gbfk_ctx *ctx, double *out);
+/* Split nsplit parents into 8 children each by Hs synthesis
+ * (BlockSplitter::_splitBlocks, MRAGBlockSplitter.h:24-99), all three fields.
+ * parents[i] is a block index of the current topology (its lab ghosts are
+ * used); children[8*i + c] is the destination slot of child
+ * c = cx + 2*(cy + 2*cz).  Destination slots must not hold current blocks. */
+int gbfk_split(gbfk_ctx *ctx, int nsplit, const int *parents, const int *children);
+/* Collapse ncollapse groups of 8 sibling slots into one parent slot by Ha
+ * analysis (injection; BlockCollapser::_collapseBlocks, MRAGBlockCollapser.h:
+ * 22-84).  children[8*i + c] as for gbfk_split; parents[i] is a slot. */
+int gbfk_collapse(gbfk_ctx *ctx, int ncollapse, const int *children, const int *parents);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GBFK_H */

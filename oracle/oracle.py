@@ -1,0 +1,203 @@
+"""Python access to the oracle: the C restatement (oracle/liboracle.so) and the
+reference's own operators (oracle/_ref/ref_harness_{f64,f32}).
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / ``--impl reference`` legs of bench.py import this module,
+and only as the checker or as the timed CPU baseline.  The product
+(``gliomasolver_b200``) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+LAB_GHOSTS = 488
+
+_lib = None
+
+
+def build_port() -> Path:
+    """Compile the C restatement (``make -C oracle port``)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "port"], check=True)
+    return HERE / "liboracle.so"
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            build_port()
+        _lib = ctypes.CDLL(str(path))
+        _declare(_lib)
+    return _lib
+
+
+class GhostCSR(ctypes.Structure):
+    _fields_ = [
+        ("nrows", ctypes.c_int64),
+        ("row_ptr", ctypes.c_void_p),
+        ("src", ctypes.c_void_p),
+        ("w0", ctypes.c_void_p),
+        ("w1", ctypes.c_void_p),
+        ("w2", ctypes.c_void_p),
+    ]
+
+
+def _declare(L):
+    P = ctypes.c_void_p
+    I, I64, D, F = ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_float
+    L.orc_rd_rhs_dense_f64.argtypes = [I, P, P, P, D, D, D, D, P]
+    L.orc_rd_rhs_dense_f32.argtypes = [I, P, P, P, F, F, F, F, P]
+    L.orc_rd_steps_dense_f64.argtypes = [I, P, P, P, D, D, D, D, D, I, P]
+    L.orc_rd_steps_dense_f32.argtypes = [I, P, P, P, F, F, F, F, D, I, P]
+    L.orc_fill_ghosts_f64.argtypes = [P, P, P]
+    L.orc_fill_ghosts_f32.argtypes = [P, P, P]
+    L.orc_rd_rhs_pool_f64.argtypes = [I, P, P, P, P, P, P, P, D, D, D, P]
+    L.orc_rd_rhs_pool_f32.argtypes = [I, P, P, P, P, P, P, P, F, F, F, P]
+    L.orc_update_f64.argtypes = [I64, P, P, D]
+    L.orc_update_f32.argtypes = [I64, P, P, D]
+    L.orc_fwt_detail_pool_f64.argtypes = [I, P, P, P]
+    L.orc_fwt_detail_pool_f32.argtypes = [I, P, P, P]
+    L.orc_split_block_f64.argtypes = [P, P, P]
+    L.orc_split_block_f32.argtypes = [P, P, P]
+    L.orc_collapse_blocks_f64.argtypes = [P, P]
+    L.orc_collapse_blocks_f32.argtypes = [P, P]
+
+
+def _p(a: np.ndarray):
+    assert a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _sfx(dtype):
+    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+
+# ---------------------------------------------------------------- dense grid
+def rd_rhs_dense(pw, pg, phi, Dw, Dg, rho, h):
+    R = pw.dtype.type
+    out = np.empty_like(phi)
+    getattr(lib(), "orc_rd_rhs_dense_" + _sfx(R))(
+        phi.shape[0], _p(pw), _p(pg), _p(phi), R(Dw), R(Dg), R(rho), R(h), _p(out))
+    return out
+
+
+def rd_steps_dense(pw, pg, phi, Dw, Dg, rho, h, dt, nsteps):
+    """``nsteps`` reference steps on a dense periodic grid; returns the new phi."""
+    R = pw.dtype.type
+    out = np.array(phi, copy=True)
+    scratch = np.empty_like(phi)
+    getattr(lib(), "orc_rd_steps_dense_" + _sfx(R))(
+        phi.shape[0], _p(pw), _p(pg), _p(out), R(Dw), R(Dg), R(rho), R(h), float(dt),
+        int(nsteps), _p(scratch))
+    return out
+
+
+# ---------------------------------------------------------------- block pool
+def fill_ghosts(csr: dict, field: np.ndarray):
+    g = GhostCSR(csr["row_ptr"].size - 1, _p(csr["row_ptr"]).value, _p(csr["src"]).value,
+                 _p(csr["w0"]).value, _p(csr["w1"]).value, _p(csr["w2"]).value)
+    out = np.empty(csr["row_ptr"].size - 1, dtype=field.dtype)
+    getattr(lib(), "orc_fill_ghosts_" + _sfx(field.dtype))(ctypes.byref(g), _p(field), _p(out))
+    return out
+
+
+def rd_rhs_pool(h, pw, pg, phi, gpw, gpg, gphi, Dw, Dg, rho):
+    R = pw.dtype.type
+    nb = pw.size // 512
+    out = np.empty_like(phi)
+    getattr(lib(), "orc_rd_rhs_pool_" + _sfx(R))(
+        nb, _p(np.ascontiguousarray(h, dtype=R)), _p(pw), _p(pg), _p(phi), _p(gpw), _p(gpg),
+        _p(gphi), R(Dw), R(Dg), R(rho), _p(out))
+    return out
+
+
+def update(phi, dphidt, dt):
+    out = np.array(phi, copy=True)
+    getattr(lib(), "orc_update_" + _sfx(phi.dtype))(out.size, _p(out), _p(dphidt), float(dt))
+    return out
+
+
+def fwt_detail_pool(phi, gphi):
+    nb = phi.size // 512
+    out = np.empty(nb, dtype=np.float64)
+    getattr(lib(), "orc_fwt_detail_pool_" + _sfx(phi.dtype))(nb, _p(phi), _p(gphi), _p(out))
+    return out
+
+
+def split_block(parent, gparent):
+    out = np.empty(8 * 512, dtype=parent.dtype)
+    getattr(lib(), "orc_split_block_" + _sfx(parent.dtype))(_p(parent), _p(gparent), _p(out))
+    return out
+
+
+def collapse_blocks(children):
+    out = np.empty(512, dtype=children.dtype)
+    getattr(lib(), "orc_collapse_blocks_" + _sfx(children.dtype))(_p(children), _p(out))
+    return out
+
+
+# ------------------------------------------------- the reference's own code
+def ref_available(precision: str = "f64") -> bool:
+    return (REF_DIR / f"ref_harness_{precision}").exists()
+
+
+def _write_dense(path, pw, pg, phi):
+    n = pw.shape[0]
+    with open(path, "wb") as f:
+        f.write(np.int32(n).tobytes())
+        for a in (pw, pg, phi):
+            f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+
+
+def _fmt(x: float) -> str:
+    return repr(float(x))
+
+
+def ref_uniform(pw, pg, phi, Dw, Dg, rho, dt, nsteps, precision="f64", threads=None):
+    """Run ``nsteps`` steps of the reference's own operators on a uniform grid."""
+    n = pw.shape[0]
+    env = dict(os.environ)
+    if threads:
+        env["GBFK_ORACLE_THREADS"] = str(threads)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        _write_dense(fin, pw, pg, phi)
+        subprocess.run([str(REF_DIR / f"ref_harness_{precision}"), "uniform", fin, fout,
+                        _fmt(Dw), _fmt(Dg), _fmt(rho), _fmt(dt), str(int(nsteps))],
+                       check=True, env=env)
+        return np.fromfile(fout, dtype=np.float64).reshape(n, n, n)
+
+
+def ref_rhs(pw, pg, phi, Dw, Dg, rho, precision="f64"):
+    n = pw.shape[0]
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        _write_dense(fin, pw, pg, phi)
+        subprocess.run([str(REF_DIR / f"ref_harness_{precision}"), "rhs", fin, fout,
+                        _fmt(Dw), _fmt(Dg), _fmt(rho)], check=True)
+        return np.fromfile(fout, dtype=np.float64).reshape(n, n, n)
+
+
+def ref_time(pw, pg, phi, Dw, Dg, rho, dt, nsteps, precision="f32", threads=None, warmup=0):
+    """Time the reference's stepping loop (after ``warmup`` untimed steps);
+    returns its JSON record."""
+    env = dict(os.environ)
+    if threads:
+        env["GBFK_ORACLE_THREADS"] = str(threads)
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        _write_dense(fin, pw, pg, phi)
+        r = subprocess.run([str(REF_DIR / f"ref_harness_{precision}"), "time", fin,
+                            _fmt(Dw), _fmt(Dg), _fmt(rho), _fmt(dt), str(int(nsteps)), str(int(warmup))],
+                           check=True, env=env, capture_output=True, text=True)
+        return json.loads(r.stdout.strip().splitlines()[-1])

@@ -1,0 +1,319 @@
+/*
+ * CPU restatement of GliomaSolver's Fisher-Kolmogorov path (the oracle).
+ * TEST INFRASTRUCTURE ONLY -- see rd_oracle.h for who may use it and how it
+ * is pinned to the reference.
+ *
+ * The arithmetic is written with the same operand order and the same
+ * Real/double mix as the reference expressions it restates; C's usual
+ * arithmetic conversions then round exactly where the C++ reference rounds.
+ * Built with -ffp-contract=off so no multiply-add is fused.
+ */
+#include "rd_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define BS 8
+#define BS3 512
+#define LAB 10 /* lab extent per direction: [-1, 9) */
+
+/* Index of lab position (ix, iy, iz) in [-1,9)^3 among the 488 ghosts, in the
+ * order BlockLab::load visits them (MRAGBlockLab.h:256-279); -1 for interior. */
+static int g_ghost_id[LAB * LAB * LAB];
+static int g_ghost_ready = 0;
+
+static void build_ghost_ids(void)
+{
+    if (g_ghost_ready) return;
+    for (int i = 0; i < LAB * LAB * LAB; i++) g_ghost_id[i] = -1;
+    int k = 0;
+    for (int icode = 0; icode < 27; icode++) {
+        if (icode == 13) continue;
+        const int code[3] = {icode % 3 - 1, (icode / 3) % 3 - 1, (icode / 9) % 3 - 1};
+        int s[3], e[3];
+        for (int d = 0; d < 3; d++) {
+            s[d] = code[d] < 1 ? (code[d] < 0 ? -1 : 0) : BS;
+            e[d] = code[d] < 1 ? (code[d] < 0 ? 0 : BS) : BS + 1;
+        }
+        for (int iz = s[2]; iz < e[2]; iz++)
+            for (int iy = s[1]; iy < e[1]; iy++)
+                for (int ix = s[0]; ix < e[0]; ix++)
+                    g_ghost_id[(ix + 1) + LAB * ((iy + 1) + LAB * (iz + 1))] = k++;
+    }
+    g_ghost_ready = 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* ReactionDiffusionOperator<3>::operator() for one cell, given the 7 lab
+ * values of (p_w, p_g, phi): index 0 = centre, 1..6 = x-, x+, y-, y+, z-, z+
+ * (ReactionDiffusionOperator.h:103-138, _harmonic_mean :148-163,
+ * _applyNoFluxBC :166-181). */
+#define DEFINE_CELL_RHS(SFX, REAL)                                                      \
+    static REAL cell_rhs_##SFX(const REAL *pw, const REAL *pg, const REAL *ph, REAL Dw,  \
+                               REAL Dg, REAL rho, double ih2)                            \
+    {                                                                                   \
+        REAL df[6], chf[6], df_loc;                                                     \
+        if (!(pw[0] + pg[0] + ph[0] > 0.)) return (REAL)0.;                             \
+        df_loc = pw[0] * Dw + pg[0] * Dg;                                               \
+        for (int i = 0; i < 6; i++) df[i] = pw[i + 1] * Dw + pg[i + 1] * Dg;            \
+        {                                                                               \
+            REAL eps = 1.0e-08;                                                         \
+            for (int i = 0; i < 6; i++)                                                 \
+                df[i] = (df[i] + df_loc < eps) ? 0. : 2. * df[i] * df_loc / (df[i] + df_loc); \
+        }                                                                               \
+        for (int i = 0; i < 6; i++) chf[i] = ph[i + 1] + pw[i + 1] + pg[i + 1];         \
+        {                                                                               \
+            REAL eps = 0.1;                                                             \
+            if (chf[0] < eps) { df[1] *= 2.0; }                                         \
+            if (chf[1] < eps) { df[0] *= 2.0; }                                         \
+            if (chf[2] < eps) { df[3] *= 2.0; }                                         \
+            if (chf[3] < eps) { df[2] *= 2.0; }                                         \
+            if (chf[4] < eps) { df[5] *= 2.0; }                                         \
+            if (chf[5] < eps) { df[4] *= 2.0; }                                         \
+        }                                                                               \
+        double diffusionFluxIn = ih2 * (df[0] * ph[1] + df[1] * ph[2] + df[2] * ph[3] + \
+                                        df[3] * ph[4] + df[4] * ph[5] + df[5] * ph[6]); \
+        double diffusionFluxOut =                                                       \
+            -((df[0] + df[1] + df[2] + df[3] + df[4] + df[5]) * ph[0] * ih2);            \
+        double reactionFlux = rho * ph[0] * (1. - ph[0]);                                \
+        return diffusionFluxOut + diffusionFluxIn + reactionFlux;                       \
+    }
+
+DEFINE_CELL_RHS(f64, double)
+DEFINE_CELL_RHS(f32, float)
+
+/* UpdateTumor<3>::operator() for one cell (ReactionDiffusionOperator.h:
+ * 215-222) with MRAG's max/min macros (MRAGCommon.h:19-37). */
+#define DEFINE_UPDATE(SFX, REAL)                                                        \
+    static inline REAL cell_update_##SFX(REAL phi, REAL dphidt, double dt)             \
+    {                                                                                   \
+        phi += dt * dphidt;                                                             \
+        phi = (((REAL)0.) >= (phi)) ? ((REAL)0.) : (phi);                               \
+        phi = (((REAL)1.) < (phi)) ? ((REAL)1.) : (phi);                                \
+        return phi;                                                                     \
+    }                                                                                   \
+    void orc_update_##SFX(int64_t ncells, REAL *phi, const REAL *dphidt, double dt)    \
+    {                                                                                   \
+        for (int64_t i = 0; i < ncells; i++) phi[i] = cell_update_##SFX(phi[i], dphidt[i], dt); \
+    }
+
+DEFINE_UPDATE(f64, double)
+DEFINE_UPDATE(f32, float)
+
+/* ------------------------------------------------------------------------ */
+/* Dense periodic grid. */
+#define DEFINE_DENSE(SFX, REAL)                                                         \
+    void orc_rd_rhs_dense_##SFX(int n, const REAL *pw, const REAL *pg, const REAL *phi,  \
+                                REAL Dw, REAL Dg, REAL rho, REAL hr, REAL *dphidt)       \
+    {                                                                                   \
+        double h = hr;                                                                  \
+        double ih2 = 1. / (h * h);                                                      \
+        const int64_t nn = n;                                                           \
+        for (int iz = 0; iz < n; iz++)                                                  \
+            for (int iy = 0; iy < n; iy++)                                              \
+                for (int ix = 0; ix < n; ix++) {                                        \
+                    const int xm = (ix + n - 1) % n, xp = (ix + 1) % n;                 \
+                    const int ym = (iy + n - 1) % n, yp = (iy + 1) % n;                 \
+                    const int zm = (iz + n - 1) % n, zp = (iz + 1) % n;                 \
+                    const int64_t id[7] = {                                             \
+                        ix + nn * (iy + nn * iz), xm + nn * (iy + nn * iz),             \
+                        xp + nn * (iy + nn * iz), ix + nn * (ym + nn * iz),             \
+                        ix + nn * (yp + nn * iz), ix + nn * (iy + nn * zm),             \
+                        ix + nn * (iy + nn * zp)};                                      \
+                    REAL a[7], b[7], c[7];                                              \
+                    for (int k = 0; k < 7; k++) {                                       \
+                        a[k] = pw[id[k]]; b[k] = pg[id[k]]; c[k] = phi[id[k]];          \
+                    }                                                                   \
+                    dphidt[id[0]] = cell_rhs_##SFX(a, b, c, Dw, Dg, rho, ih2);          \
+                }                                                                       \
+    }
+
+DEFINE_DENSE(f64, double)
+DEFINE_DENSE(f32, float)
+
+void orc_rd_steps_dense_f64(int n, const double *pw, const double *pg, double *phi,
+                            double Dw, double Dg, double rho, double h, double dt, int nsteps,
+                            double *scratch)
+{
+    const int64_t N = (int64_t)n * n * n;
+    for (int s = 0; s < nsteps; s++) {
+        orc_rd_rhs_dense_f64(n, pw, pg, phi, Dw, Dg, rho, h, scratch);
+        orc_update_f64(N, phi, scratch, dt);
+    }
+}
+
+void orc_rd_steps_dense_f32(int n, const float *pw, const float *pg, float *phi,
+                            float Dw, float Dg, float rho, float h, double dt, int nsteps,
+                            float *scratch)
+{
+    const int64_t N = (int64_t)n * n * n;
+    for (int s = 0; s < nsteps; s++) {
+        orc_rd_rhs_dense_f32(n, pw, pg, phi, Dw, Dg, rho, h, scratch);
+        orc_update_f32(N, phi, scratch, dt);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Block pool with lab ghosts. */
+#define DEFINE_POOL(SFX, REAL)                                                          \
+    void orc_fill_ghosts_##SFX(const orc_ghost_csr *g, const REAL *field, REAL *out)    \
+    {                                                                                   \
+        for (int64_t r = 0; r < g->nrows; r++) {                                        \
+            REAL ghost = 0;                                                             \
+            for (int64_t k = g->row_ptr[r]; k < g->row_ptr[r + 1]; k++) {               \
+                const REAL w = ((REAL)g->w0[k] * (REAL)g->w1[k]) * (REAL)g->w2[k];      \
+                ghost += field[g->src[k]] * w;                                          \
+            }                                                                           \
+            out[r] = ghost;                                                             \
+        }                                                                               \
+    }                                                                                   \
+    static inline REAL lab_##SFX(const REAL *blk, const REAL *ghosts, int ix, int iy, int iz) \
+    {                                                                                   \
+        if (ix >= 0 && ix < BS && iy >= 0 && iy < BS && iz >= 0 && iz < BS)             \
+            return blk[ix + BS * (iy + BS * iz)];                                       \
+        return ghosts[g_ghost_id[(ix + 1) + LAB * ((iy + 1) + LAB * (iz + 1))]];        \
+    }                                                                                   \
+    void orc_rd_rhs_pool_##SFX(int nblocks, const REAL *h, const REAL *pw, const REAL *pg, \
+                               const REAL *phi, const REAL *gpw, const REAL *gpg,        \
+                               const REAL *gphi, REAL Dw, REAL Dg, REAL rho, REAL *dphidt) \
+    {                                                                                   \
+        build_ghost_ids();                                                              \
+        static const int off[7][3] = {{0, 0, 0}, {-1, 0, 0}, {1, 0, 0}, {0, -1, 0},     \
+                                      {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};                \
+        for (int b = 0; b < nblocks; b++) {                                             \
+            double hb = h[b];                                                           \
+            double ih2 = 1. / (hb * hb);                                                \
+            const REAL *bw = pw + (int64_t)b * BS3, *bg = pg + (int64_t)b * BS3;        \
+            const REAL *bp = phi + (int64_t)b * BS3;                                    \
+            const REAL *gw = gpw + (int64_t)b * ORC_LAB_GHOSTS;                         \
+            const REAL *gg = gpg + (int64_t)b * ORC_LAB_GHOSTS;                         \
+            const REAL *gp = gphi + (int64_t)b * ORC_LAB_GHOSTS;                        \
+            for (int iz = 0; iz < BS; iz++)                                             \
+                for (int iy = 0; iy < BS; iy++)                                         \
+                    for (int ix = 0; ix < BS; ix++) {                                   \
+                        REAL a[7], bb[7], c[7];                                         \
+                        for (int k = 0; k < 7; k++) {                                   \
+                            const int x = ix + off[k][0], y = iy + off[k][1], z = iz + off[k][2]; \
+                            a[k] = lab_##SFX(bw, gw, x, y, z);                          \
+                            bb[k] = lab_##SFX(bg, gg, x, y, z);                         \
+                            c[k] = lab_##SFX(bp, gp, x, y, z);                          \
+                        }                                                               \
+                        dphidt[(int64_t)b * BS3 + ix + BS * (iy + BS * iz)] =           \
+                            cell_rhs_##SFX(a, bb, c, Dw, Dg, rho, ih2);                 \
+                    }                                                                   \
+        }                                                                               \
+    }
+
+DEFINE_POOL(f64, double)
+DEFINE_POOL(f32, float)
+
+/* ------------------------------------------------------------------------ */
+/* Interpolating 2nd-order wavelets (MRAG/MRAGcore/MRAGWavelets_StaticData.cpp:
+ * 13-21): Ha = {1} on [0,1), Ga = {-.5, 1, -.5} on [-2,1), Hs = {.5, 1, .5}
+ * on [-1,2). */
+static const double kGa[3] = {-0.5, 1., -0.5};
+static const double kHs[3] = {0.5, 1., 0.5};
+
+/* BlockFWT::_filter (MRAGBlockFWT.h:219-257): for subband bits (wx, wy, wz) the
+ * filter runs z, then y, then x over the support, reading lab(o - i), and
+ * accumulates phi * (wZ*wY * wX) in Real. */
+#define DEFINE_FWT(SFX, REAL)                                                           \
+    static REAL fwt_filter_##SFX(const REAL *blk, const REAL *gh, int wx, int wy, int wz, \
+                                 int dx, int dy, int dz)                                 \
+    {                                                                                   \
+        const REAL Ga[3] = {(REAL)kGa[0], (REAL)kGa[1], (REAL)kGa[2]};                  \
+        const REAL Ha0 = (REAL)1;                                                       \
+        const int s[3] = {wx ? -2 : 0, wy ? -2 : 0, wz ? -2 : 0};                       \
+        const int e[3] = {1, 1, 1};                                                     \
+        const int o[3] = {2 * dx, 2 * dy, 2 * dz};                                      \
+        REAL result = 0;                                                                \
+        for (int iz = s[2]; iz < e[2]; iz++) {                                          \
+            const REAL wZ = wz ? Ga[iz + 2] : Ha0;                                      \
+            for (int iy = s[1]; iy < e[1]; iy++) {                                      \
+                const REAL wY = wy ? Ga[iy + 2] : Ha0;                                  \
+                const REAL wZwY = wZ * wY;                                              \
+                for (int ix = s[0]; ix < e[0]; ix++) {                                  \
+                    const REAL wX = wx ? Ga[ix + 2] : Ha0;                              \
+                    result += lab_##SFX(blk, gh, o[0] - ix, o[1] - iy, o[2] - iz) * (wZwY * wX); \
+                }                                                                       \
+            }                                                                           \
+        }                                                                               \
+        return result;                                                                  \
+    }                                                                                   \
+    void orc_fwt_detail_pool_##SFX(int nblocks, const REAL *phi, const REAL *gphi, double *out) \
+    {                                                                                   \
+        build_ghost_ids();                                                              \
+        for (int b = 0; b < nblocks; b++) {                                             \
+            const REAL *blk = phi + (int64_t)b * BS3;                                   \
+            const REAL *gh = gphi + (int64_t)b * ORC_LAB_GHOSTS;                        \
+            double maxv[8] = {0, 0, 0, 0, 0, 0, 0, 0};                                  \
+            for (int iz = 0; iz < BS / 2; iz++)                                         \
+                for (int iy = 0; iy < BS / 2; iy++)                                     \
+                    for (int ix = 0; ix < BS / 2; ix++)                                 \
+                        for (int code = 0; code < 8; code++) {                          \
+                            const REAL v = fwt_filter_##SFX(blk, gh, code & 1, (code >> 1) & 1, \
+                                                            (code >> 2) & 1, ix, iy, iz); \
+                            const double a = fabs(v);                                   \
+                            if (!(a < maxv[code])) maxv[code] = a;                      \
+                        }                                                               \
+            double m = maxv[1];                                                         \
+            for (int code = 2; code < 8; code++) m = (m < maxv[code]) ? maxv[code] : m; \
+            out[b] = m;                                                                 \
+        }                                                                               \
+    }
+
+DEFINE_FWT(f64, double)
+DEFINE_FWT(f32, float)
+
+/* BlockSplitter::_splitBlocks (MRAGBlockSplitter.h:49-98) for Interp2ndOrder:
+ * coarse lab points s in [0, 9)^3 (z, y, x order) scatter to fine points d in
+ * [2s-1, 2s+2) clipped to [0,16) with weight Hs(2s-d), the weight product in
+ * double (wZ*wY)*wX and then converted to Real (Cell*Real, Glioma_Types.h). */
+#define DEFINE_SPLIT(SFX, REAL)                                                         \
+    void orc_split_block_##SFX(const REAL *parent, const REAL *gparent, REAL *children) \
+    {                                                                                   \
+        build_ghost_ids();                                                              \
+        memset(children, 0, sizeof(REAL) * 8 * BS3);                                    \
+        for (int sz = 0; sz < BS + 1; sz++)                                             \
+            for (int sy = 0; sy < BS + 1; sy++)                                         \
+                for (int sx = 0; sx < BS + 1; sx++) {                                   \
+                    const int st[3] = {2 * sx - 1 < 0 ? 0 : 2 * sx - 1,                 \
+                                       2 * sy - 1 < 0 ? 0 : 2 * sy - 1,                 \
+                                       2 * sz - 1 < 0 ? 0 : 2 * sz - 1};                \
+                    const int en[3] = {2 * sx + 2 > 2 * BS ? 2 * BS : 2 * sx + 2,        \
+                                       2 * sy + 2 > 2 * BS ? 2 * BS : 2 * sy + 2,        \
+                                       2 * sz + 2 > 2 * BS ? 2 * BS : 2 * sz + 2};       \
+                    const REAL v = lab_##SFX(parent, gparent, sx, sy, sz);              \
+                    for (int dz = st[2]; dz < en[2]; dz++) {                            \
+                        const double wZ = kHs[2 * sz - dz + 1];                         \
+                        for (int dy = st[1]; dy < en[1]; dy++) {                        \
+                            const double wY = kHs[2 * sy - dy + 1];                     \
+                            const double wZwY = wZ * wY;                                \
+                            for (int dx = st[0]; dx < en[0]; dx++) {                    \
+                                const int cx = dx / BS, cy = dy / BS, cz = dz / BS;     \
+                                REAL *child = children + (cx + 2 * (cy + 2 * cz)) * BS3; \
+                                const REAL w = (REAL)(wZwY * kHs[2 * sx - dx + 1]);     \
+                                child[(dx - cx * BS) + BS * ((dy - cy * BS) + BS * (dz - cz * BS))] += v * w; \
+                            }                                                           \
+                        }                                                               \
+                    }                                                                   \
+                }                                                                       \
+    }                                                                                   \
+    void orc_collapse_blocks_##SFX(const REAL *children, REAL *parent)                  \
+    {                                                                                   \
+        for (int c = 0; c < 8; c++) {                                                   \
+            const int cx = c & 1, cy = (c >> 1) & 1, cz = (c >> 2) & 1;                 \
+            const REAL *src = children + c * BS3;                                       \
+            for (int iz = 0; iz < BS / 2; iz++)                                         \
+                for (int iy = 0; iy < BS / 2; iy++)                                     \
+                    for (int ix = 0; ix < BS / 2; ix++) {                               \
+                        REAL r = 0;                                                     \
+                        r += src[2 * ix + BS * (2 * iy + BS * 2 * iz)] * (REAL)(1.0 * 1.0 * 1.0); \
+                        parent[(cx * 4 + ix) + BS * ((cy * 4 + iy) + BS * (cz * 4 + iz))] = r; \
+                    }                                                                   \
+        }                                                                               \
+    }
+
+DEFINE_SPLIT(f64, double)
+DEFINE_SPLIT(f32, float)

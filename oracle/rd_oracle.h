@@ -1,0 +1,102 @@
+/*
+ * CPU restatement of GliomaSolver's Fisher-Kolmogorov path (the oracle).
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline leg of bench.py may load this library, and only as the checker
+ * or the timed CPU baseline.  The product (libgbfk) never calls it.
+ *
+ * Every function restates the reference's arithmetic operation by operation,
+ * in the reference's Real type, so that results can be compared bit for bit:
+ *   *_f64  = reference built with -D_MRAG_REAL_=double
+ *   *_f32  = reference default build (Real = float, MRAGCommon.h:43-47), in
+ *            which the operator still evaluates ih2, the harmonic-mean
+ *            quotient, the flux sums and the reaction term in double
+ *            (Glioma/Operators/ReactionDiffusionOperator.h:49-52,124-135).
+ * The restatement is pinned against the reference itself: oracle/_ref is the
+ * reference's own operator code (oracle/ref_harness.cpp), and the golden
+ * fixtures under tests/golden/ were produced by it.
+ *
+ * Layouts
+ *   dense  : n^3 cells, x fastest, periodic wrap (the uniform MRAG grid with
+ *            periodic ghosts, MRAG/MRAGcore/MRAGrid.inl:37-39,930-1076).
+ *   pool   : nblocks x 512 cells (8^3 block, x fastest, MRAGBlock.h:40) plus a
+ *            per-block lab halo of 488 ghost cells filled from a ghost CSR
+ *            (the instruction lists of MRAGBoundaryBlockInfo.h:69-176, as
+ *            executed by BlockLab::load, MRAGBlockLab.h:254-295).
+ */
+#ifndef GBFK_RD_ORACLE_H
+#define GBFK_RD_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* dphidt of one ReactionDiffusionOperator<3> sweep on a dense periodic grid
+ * (ReactionDiffusionOperator.h:97-138). */
+void orc_rd_rhs_dense_f64(int n, const double *pw, const double *pg, const double *phi,
+                          double Dw, double Dg, double rho, double h, double *dphidt);
+void orc_rd_rhs_dense_f32(int n, const float *pw, const float *pg, const float *phi,
+                          float Dw, float Dg, float rho, float h, float *dphidt);
+
+/* nsteps explicit Euler steps (operator + UpdateTumor, ReactionDiffusionOperator.h:
+ * 189-226) on a dense periodic grid, in place on phi; scratch holds n^3 Reals. */
+void orc_rd_steps_dense_f64(int n, const double *pw, const double *pg, double *phi,
+                            double Dw, double Dg, double rho, double h, double dt, int nsteps,
+                            double *scratch);
+void orc_rd_steps_dense_f32(int n, const float *pw, const float *pg, float *phi,
+                            float Dw, float Dg, float rho, float h, double dt, int nsteps,
+                            float *scratch);
+
+/* Ghost CSR: one row per lab ghost cell of each block, rows ordered block by
+ * block, and inside a block by BlockLab::load's loop order (codes 0..26 without
+ * 13, then z, y, x of the code's region, MRAGBlockLab.h:256-279) for the lab
+ * range [-1, 9) in every direction (the grid's max stencil [-1, 2),
+ * MRAG/MRAGcore/MRAGrid.inl:761-789), i.e. 488 rows per block.  Entry k of a
+ * row reads cell src[k] (= source block slot * 512 + cell index) with the
+ * three weights w0[k], w1[k], w2[k] (doubles of BoundaryInfoBlock::weightsPool). */
+typedef struct {
+    int64_t nrows;
+    const int64_t *row_ptr;   /* nrows + 1 */
+    const int64_t *src;
+    const double *w0, *w1, *w2;
+} orc_ghost_csr;
+
+#define ORC_LAB_GHOSTS 488
+
+/* Fill the lab ghosts of every block for one field (BlockLab::load step 3:
+ * ghost = 0; ghost += v * ((w0*w1)*w2), in Real). out: nblocks * 488. */
+void orc_fill_ghosts_f64(const orc_ghost_csr *g, const double *field, double *out);
+void orc_fill_ghosts_f32(const orc_ghost_csr *g, const float *field, float *out);
+
+/* One operator sweep (+ optional update) over a block pool with lab ghosts.
+ * h[b] is BlockInfo::h[0] of block b (in Real). */
+void orc_rd_rhs_pool_f64(int nblocks, const double *h, const double *pw, const double *pg,
+                         const double *phi, const double *gpw, const double *gpg,
+                         const double *gphi, double Dw, double Dg, double rho, double *dphidt);
+void orc_rd_rhs_pool_f32(int nblocks, const float *h, const float *pw, const float *pg,
+                         const float *phi, const float *gpw, const float *gpg,
+                         const float *gphi, float Dw, float Dg, float rho, float *dphidt);
+void orc_update_f64(int64_t ncells, double *phi, const double *dphidt, double dt);
+void orc_update_f32(int64_t ncells, float *phi, const float *dphidt, double dt);
+
+/* Max |detail| of the one-level interpolating-wavelet transform of phi per
+ * block (BlockFWT::_fwt/_filter + FWTReport::getOverAll_DetailMaxMag,
+ * MRAG/MRAGcore/MRAGBlockFWT.h:109-120,219-298). out: nblocks doubles. */
+void orc_fwt_detail_pool_f64(int nblocks, const double *phi, const double *gphi, double *out);
+void orc_fwt_detail_pool_f32(int nblocks, const float *phi, const float *gphi, double *out);
+
+/* Children of a block by Hs synthesis (BlockSplitter::_splitBlocks,
+ * MRAG/MRAGcore/MRAGBlockSplitter.h:24-99): child[c] for c = cx + 2*(cy + 2*cz)
+ * gets 512 cells; reads the parent's lab (interior + ghosts). */
+void orc_split_block_f64(const double *parent, const double *gparent, double *children);
+void orc_split_block_f32(const float *parent, const float *gparent, float *children);
+
+/* Parent of eight siblings by Ha analysis (injection; BlockCollapser::
+ * _collapseBlocks, MRAG/MRAGcore/MRAGBlockCollapser.h:22-84). */
+void orc_collapse_blocks_f64(const double *children, double *parent);
+void orc_collapse_blocks_f32(const float *children, float *parent);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
