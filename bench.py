@@ -201,8 +201,13 @@ def gpu_arm(args):
     pw, pg, c0 = (a.astype(R) for a in (pw, pg, c0))
     s = make_schedule(DW, RHO, TEND, L_CM, n // 8, prec)
     cells = n ** 3
-    stream = torch.cuda.current_stream()
+    # an explicit stream: the library treats a NULL handle (torch's legacy
+    # default stream) as "create a private stream", which events on the
+    # default stream would not see
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
     pool = BlockPool((n // 8) ** 3, prec, device=local, stream=stream.cuda_stream)
+    assert stream.cuda_stream != 0
     pool.set_uniform(n // 8)
     pool.upload_dense("p_w", pw)
     pool.upload_dense("p_g", pg)

@@ -56,6 +56,15 @@ struct gbfk_ctx {
     void *d_gpw = nullptr, *d_gpg = nullptr, *d_gphi = nullptr;
     bool static_ghosts_dirty = true;
 
+    // static per (topology, p_w, p_g): cell classes; per (.., Dw, Dg): face coefficients
+    unsigned short *d_meta = nullptr; // max_blocks * 512 meta words, indexed like the pool
+    unsigned char *d_btype = nullptr; // nblocks block types
+    bool identity_slots = false;
+    void *d_H = nullptr;              // nblocks * 1728 Real
+    double *d_ih2 = nullptr;          // nblocks: 1/(h*h) in double
+    bool faces_valid = false;
+    double faces_Dw = 0, faces_Dg = 0;
+
     // scratch
     unsigned *d_nan = nullptr;
     void *d_stage = nullptr;
@@ -107,7 +116,7 @@ void free_topology(gbfk_ctx *c)
 {
     void **ptrs[] = {(void **)&c->d_slot, (void **)&c->d_nbr, &c->d_h, (void **)&c->d_row_ptr, (void **)&c->d_src,
                      &c->d_w, (void **)&c->d_step_rows, (void **)&c->d_all_rows, &c->d_gpw, &c->d_gpg,
-                     &c->d_gphi, (void **)&c->d_fwt};
+                     &c->d_gphi, (void **)&c->d_fwt, &c->d_H, (void **)&c->d_ih2, (void **)&c->d_btype};
     for (void **p : ptrs) {
         if (*p) cudaFree(*p);
         *p = nullptr;
@@ -118,6 +127,27 @@ void free_topology(gbfk_ctx *c)
     c->h_slot.clear();
     c->h_h.clear();
     c->static_ghosts_dirty = true;
+    c->faces_valid = false;
+}
+
+// Something the face coefficients or classes depend on changed.
+void invalidate_static(gbfk_ctx *c)
+{
+    c->static_ghosts_dirty = true;
+    c->faces_valid = false;
+}
+
+// Per-block 1/(h*h) in double, as the operator forms it (ReactionDiffusionOperator.h:49-50).
+int upload_ih2(gbfk_ctx *ctx)
+{
+    std::vector<double> v(ctx->nblocks);
+    for (int i = 0; i < ctx->nblocks; i++) {
+        const double h = ctx->precision == GBFK_F64 ? ctx->h_h[i] : (double)(float)ctx->h_h[i];
+        v[i] = 1. / (h * h);
+    }
+    CK(cudaMalloc(&ctx->d_ih2, ctx->nblocks * sizeof(double)));
+    CK(cudaMemcpy(ctx->d_ih2, v.data(), ctx->nblocks * sizeof(double), cudaMemcpyHostToDevice));
+    return GBFK_OK;
 }
 
 template <typename Real>
@@ -132,7 +162,15 @@ PoolView<Real> view(gbfk_ctx *c)
     v.gphi = (const Real *)c->d_gphi;
     v.pw = (const Real *)c->pw;
     v.pg = (const Real *)c->pg;
+    v.btype = c->d_btype;
     v.nblocks = c->nblocks;
+    v.identity_slots = c->identity_slots ? 1 : 0;
+    v.log2_bpd = -1;
+    if (c->uniform && !c->have_csr && (c->bpd & (c->bpd - 1)) == 0) {
+        int L = 0;
+        while ((1 << L) < c->bpd) L++;
+        v.log2_bpd = L;
+    }
     return v;
 }
 
@@ -230,7 +268,7 @@ int set_csr(gbfk_ctx *ctx, const std::vector<int64_t> &row_ptr, const std::vecto
     ctx->n_step_rows = (int64_t)step_rows.size();
     ctx->nrows = nrows;
     ctx->have_csr = true;
-    ctx->static_ghosts_dirty = true;
+    invalidate_static(ctx);
     return GBFK_OK;
 }
 
@@ -281,10 +319,31 @@ int refresh_static_ghosts(gbfk_ctx *ctx)
     return GBFK_OK;
 }
 
+// Ghosts of p_w/p_g, cell classes and the face coefficients for (Dw, Dg):
+// everything of a step that does not depend on phi.
+template <typename Real>
+int prepare_static(gbfk_ctx *ctx, double Dw, double Dg)
+{
+    int rc = refresh_static_ghosts<Real>(ctx);
+    if (rc) return rc;
+    const double kDw = (double)(Real)Dw, kDg = (double)(Real)Dg;
+    if (!ctx->faces_valid || ctx->faces_Dw != kDw || ctx->faces_Dg != kDg) {
+        if (!ctx->d_H) CK(cudaMalloc(&ctx->d_H, (size_t)ctx->nblocks * kFacesPerBlock * sizeof(Real)));
+        if (!ctx->d_btype) CK(cudaMalloc(&ctx->d_btype, (size_t)ctx->nblocks));
+        CK(launch_faces<Real>(view<Real>(ctx), (Real)Dw, (Real)Dg, (Real *)ctx->d_H, ctx->d_meta, ctx->d_btype,
+                              ctx->stream));
+        ctx->launches++;
+        ctx->faces_valid = true;
+        ctx->faces_Dw = kDw;
+        ctx->faces_Dg = kDg;
+    }
+    return GBFK_OK;
+}
+
 template <typename Real>
 int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int nsteps, int check_nan)
 {
-    int rc = refresh_static_ghosts<Real>(ctx);
+    int rc = prepare_static<Real>(ctx, Dw, Dg);
     if (rc) return rc;
     PoolView<Real> v = view<Real>(ctx);
     if (check_nan) CK(cudaMemsetAsync(ctx->d_nan, 0, sizeof(unsigned), ctx->stream));
@@ -296,7 +355,8 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
                                         (const Real *)ctx->d_w, in, (Real *)ctx->d_gphi, ctx->stream));
             ctx->launches++;
         }
-        CK(launch_rd_step<Real>(v, in, out, nullptr, (Real)Dw, (Real)Dg, (Real)rho, dt, ctx->d_nan, ctx->stream));
+        CK(launch_rd_step<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, in, out, nullptr, (Real)rho, dt,
+                                ctx->d_nan, ctx->stream));
         ctx->launches++;
         ctx->cur ^= 1;
     }
@@ -312,7 +372,7 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
 template <typename Real>
 int rd_rhs_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, void *host)
 {
-    int rc = refresh_static_ghosts<Real>(ctx);
+    int rc = prepare_static<Real>(ctx, Dw, Dg);
     if (rc) return rc;
     const size_t bytes = (size_t)ctx->nblocks * kBS3 * sizeof(Real);
     Real *d_out = nullptr;
@@ -326,7 +386,8 @@ int rd_rhs_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, void *host)
         ctx->launches++;
     }
     if (e == cudaSuccess) {
-        e = launch_rd_step<Real>(v, in, nullptr, d_out, (Real)Dw, (Real)Dg, (Real)rho, 0.0, ctx->d_nan, ctx->stream);
+        e = launch_rd_step<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, in, nullptr, d_out, (Real)rho,
+                                 0.0, ctx->d_nan, ctx->stream);
         ctx->launches++;
     }
     // dphidt leaves in topology order: block i's 512 cells at i*512
@@ -389,6 +450,7 @@ int split_impl(gbfk_ctx *ctx, int nsplit, const int *parents, const int *childre
     CK(launch_split<Real>(view<Real>(ctx), nsplit, ctx->d_ints, ctx->d_ints + nsplit, (Real *)ctx->phi[ctx->cur],
                           (Real *)ctx->pw, (Real *)ctx->pg, ctx->stream));
     ctx->launches += 2;
+    invalidate_static(ctx);
     CK(cudaStreamSynchronize(ctx->stream));
     return GBFK_OK;
 }
@@ -410,6 +472,7 @@ int collapse_impl(gbfk_ctx *ctx, int n, const int *children, const int *parents)
     CK(launch_collapse<Real>(n, ctx->d_ints, ctx->d_ints + (size_t)n * 8, (Real *)ctx->phi[ctx->cur],
                              (Real *)ctx->pw, (Real *)ctx->pg, ctx->stream));
     ctx->launches++;
+    invalidate_static(ctx);
     CK(cudaStreamSynchronize(ctx->stream));
     return GBFK_OK;
 }
@@ -454,7 +517,8 @@ int gbfk_create(const gbfk_config *cfg, gbfk_ctx **out)
     const size_t bytes = (size_t)cfg->max_blocks * kBS3 * ctx->rsize;
     if (cudaMalloc(&ctx->phi[0], bytes) != cudaSuccess || cudaMalloc(&ctx->phi[1], bytes) != cudaSuccess ||
         cudaMalloc(&ctx->pw, bytes) != cudaSuccess || cudaMalloc(&ctx->pg, bytes) != cudaSuccess ||
-        cudaMalloc(&ctx->d_nan, sizeof(unsigned)) != cudaSuccess) {
+        cudaMalloc(&ctx->d_nan, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_meta, (size_t)cfg->max_blocks * kBS3 * sizeof(unsigned short)) != cudaSuccess) {
         cudaGetLastError();
         return bail(GBFK_E_OOM);
     }
@@ -474,7 +538,7 @@ int gbfk_destroy(gbfk_ctx *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_topology(ctx);
-    void *ptrs[] = {ctx->phi[0], ctx->phi[1], ctx->pw, ctx->pg, ctx->d_nan, ctx->d_stage, ctx->d_ints};
+    void *ptrs[] = {ctx->phi[0], ctx->phi[1], ctx->pw, ctx->pg, ctx->d_nan, ctx->d_stage, ctx->d_ints, ctx->d_meta};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -526,6 +590,7 @@ int gbfk_set_uniform(gbfk_ctx *ctx, int bpd)
             }
     const double h = 1.0 / (8.0 * bpd);
     ctx->h_h.assign(nb, h);
+    ctx->identity_slots = true;
     CK(cudaMalloc(&ctx->d_slot, nb * sizeof(int)));
     CK(cudaMalloc(&ctx->d_nbr, (size_t)nb * 6 * sizeof(int)));
     CK(cudaMalloc(&ctx->d_h, nb * ctx->rsize));
@@ -538,6 +603,8 @@ int gbfk_set_uniform(gbfk_ctx *ctx, int bpd)
         std::vector<float> hv(nb, (float)h);
         CK(cudaMemcpy(ctx->d_h, hv.data(), nb * sizeof(float), cudaMemcpyHostToDevice));
     }
+    int rc = upload_ih2(ctx);
+    if (rc) return rc;
     ctx->have_topology = true;
     return GBFK_OK;
 }
@@ -573,9 +640,11 @@ int gbfk_set_topology(gbfk_ctx *ctx, const gbfk_blockinfo *blocks, int nblocks, 
     ctx->nblocks = nblocks;
     ctx->h_slot.resize(nblocks);
     ctx->h_h.resize(nblocks);
+    ctx->identity_slots = true;
     for (int i = 0; i < nblocks; i++) {
         ctx->h_slot[i] = blocks[i].slot;
         ctx->h_h[i] = blocks[i].h;
+        if (blocks[i].slot != i) ctx->identity_slots = false;
     }
     CK(cudaMalloc(&ctx->d_slot, nblocks * sizeof(int)));
     CK(cudaMalloc(&ctx->d_h, nblocks * ctx->rsize));
@@ -592,6 +661,8 @@ int gbfk_set_topology(gbfk_ctx *ctx, const gbfk_blockinfo *blocks, int nblocks, 
     int rc = ctx->precision == GBFK_F64 ? set_csr<double>(ctx, row_ptr, src, w0, w1, w2, true)
                                         : set_csr<float>(ctx, row_ptr, src, w0, w1, w2, true);
     if (rc) return rc;
+    rc = upload_ih2(ctx);
+    if (rc) return rc;
     ctx->have_topology = true;
     return GBFK_OK;
 }
@@ -605,7 +676,7 @@ int gbfk_upload_field(gbfk_ctx *ctx, int field, const void *host, int64_t first,
     CK(cudaSetDevice(ctx->device));
     CK(cudaMemcpyAsync((char *)p + first * ctx->rsize, host, ncells * ctx->rsize, cudaMemcpyHostToDevice,
                        ctx->stream));
-    if (field != GBFK_PHI) ctx->static_ghosts_dirty = true;
+    if (field != GBFK_PHI) invalidate_static(ctx);
     return GBFK_OK;
 }
 
@@ -645,7 +716,7 @@ static int dense_io(gbfk_ctx *ctx, int field, void *host, int n, bool up)
         else
             CK(launch_dense_scatter<float>((const float *)ctx->d_stage, (float *)p, n, true, ctx->stream));
         ctx->launches++;
-        if (field != GBFK_PHI) ctx->static_ghosts_dirty = true;
+        if (field != GBFK_PHI) invalidate_static(ctx);
     } else {
         if (ctx->precision == GBFK_F64)
             CK(launch_dense_scatter<double>((const double *)p, (double *)ctx->d_stage, n, false, ctx->stream));

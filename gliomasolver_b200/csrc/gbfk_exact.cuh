@@ -85,12 +85,51 @@ __device__ __forceinline__ Real cell_rhs(Real df0, Real df1, Real df2, Real df3,
     return to_real<Real>(__dadd_rn(__dadd_rn(fluxOut, fluxIn), reaction));
 }
 
+// The same with the six no-flux tests already decided: low[k] is
+// chf[k] < 0.1 of neighbour k (x-, x+, y-, y+, z-, z+).
+template <typename Real>
+__device__ __forceinline__ Real cell_rhs_flags(Real df0, Real df1, Real df2, Real df3, Real df4, Real df5,
+                                               const bool low[6], const Real phn[6], Real phi, Real rho,
+                                               double ih2)
+{
+    if (low[0]) df1 = rmul(df1, (Real)2.0);
+    if (low[1]) df0 = rmul(df0, (Real)2.0);
+    if (low[2]) df3 = rmul(df3, (Real)2.0);
+    if (low[3]) df2 = rmul(df2, (Real)2.0);
+    if (low[4]) df5 = rmul(df5, (Real)2.0);
+    if (low[5]) df4 = rmul(df4, (Real)2.0);
+
+    Real sin_ = rmul(df0, phn[0]);
+    sin_ = radd(sin_, rmul(df1, phn[1]));
+    sin_ = radd(sin_, rmul(df2, phn[2]));
+    sin_ = radd(sin_, rmul(df3, phn[3]));
+    sin_ = radd(sin_, rmul(df4, phn[4]));
+    sin_ = radd(sin_, rmul(df5, phn[5]));
+    const double fluxIn = __dmul_rn(ih2, (double)sin_);
+
+    Real sdf = radd(radd(radd(radd(radd(df0, df1), df2), df3), df4), df5);
+    const double fluxOut = -__dmul_rn((double)rmul(sdf, phi), ih2);
+
+    const double reaction = __dmul_rn((double)rmul(rho, phi), __dadd_rn(1., -(double)phi));
+    return to_real<Real>(__dadd_rn(__dadd_rn(fluxOut, fluxIn), reaction));
+}
+
 // UpdateTumor<3> (ReactionDiffusionOperator.h:219-221) with MRAG's max/min
 // macros (MRAG/MRAGcore/MRAGCommon.h:19-37): phi += dt*dphidt; clamp to [0,1].
 template <typename Real>
 __device__ __forceinline__ Real cell_update(Real phi, Real dphidt, double dt)
 {
     Real p = to_real<Real>(__dadd_rn((double)phi, __dmul_rn(dt, (double)dphidt)));
+    p = ((Real)0. >= p) ? (Real)0. : p;
+    p = ((Real)1. < p) ? (Real)1. : p;
+    return p;
+}
+
+// The clamp of UpdateTumor alone: what the update leaves of phi when
+// dphidt = 0 and dt is finite (phi + dt*0 rounds back to phi).
+template <typename Real>
+__device__ __forceinline__ Real clamp01(Real p)
+{
     p = ((Real)0. >= p) ? (Real)0. : p;
     p = ((Real)1. < p) ? (Real)1. : p;
     return p;

@@ -30,41 +30,63 @@ __device__ __forceinline__ void face_cell(int f, int p, int &lx, int &ly, int &l
 }
 
 // ---------------------------------------------------------------------------
-// Fused step: ReactionDiffusionOperator<3> + UpdateTumor<3> for one block per
-// CTA.  The block and its six face halos of (p_w, p_g, phi) are staged in
-// shared memory; the diffusivity df of every staged cell is computed once;
-// the harmonic mean of every face is computed once and shared by the two
-// cells of the face (it is bit-identical from either side, see
-// face_harmonic); then each thread finishes two cells.
+// Cell classes: which exact shortcut the step may take for the domain test
+// p_w + p_g + phi > 0 (ReactionDiffusionOperator.h:103) and the no-flux test
+// chf = phi + p_w + p_g < 0.1 (:115-122, :166-181) of a cell.
+//   kEmpty : p_w == 0 and p_g == 0, so chf == phi and the domain test is phi > 0;
+//   kTissue: t = p_w + p_g >= 0.1 in Real.  Rounding is monotone, so for
+//            phi >= 0 both chf >= t >= 0.1 (no doubling) and t + phi > 0 hold;
+//   kOther : evaluated exactly from p_w and p_g.
+// meta words of a cell whose own class and all six neighbour classes are kEmpty / kTissue
+constexpr unsigned kMetaAllEmpty = kEmpty | (0x3fu << 2);
+constexpr unsigned kMetaAllTissue = kTissue;
+
 template <typename Real>
-struct StepSmem {
-    Real pw[kLab3], pg[kLab3], ph[kLab3], df[kLab3];
-    Real hx[8 * 8 * 9], hy[8 * 8 * 9], hz[8 * 8 * 9];
+__device__ __forceinline__ unsigned cell_class(Real pw, Real pg)
+{
+    if (pw == (Real)0 && pg == (Real)0) return kEmpty;
+    if (radd(pw, pg) >= (Real)0.1) return kTissue;
+    return kOther;
+}
+
+// ---------------------------------------------------------------------------
+// Static coefficients.  The harmonic means of ReactionDiffusionOperator<3>
+// (_harmonic_mean, ReactionDiffusionOperator.h:148-163) depend only on p_w,
+// p_g, Dw and Dg, never on phi, so they are computed once per topology and
+// coefficient pair instead of on every step.  One CTA per block: the block's
+// p_w, p_g and their six face halos are staged in shared memory, df =
+// p_w*Dw + p_g*Dg is formed once per staged cell, and the harmonic mean of
+// each of the 3 x 576 faces of the block (including its boundary faces, seen
+// from this block's own lab) is written to global memory:
+//   x faces: H[(z*8 + y)*9 + fx],   fx in [0,9) between x = fx-1 and fx
+//   y faces: H[576 + (z*9 + fy)*8 + x]
+//   z faces: H[1152 + (fz*8 + y)*8 + x]
+// The value is bit-identical from either cell of a face (face_harmonic).
+// The same pass writes every cell's 16-bit meta word (indexed like the pool):
+//   bits 0-1  the cell's class
+//   bits 2-7  neighbour k (x-, x+, y-, y+, z-, z+) is kEmpty
+//   bits 8-13 neighbour k is kOther
+template <typename Real>
+struct FaceSmem {
+    Real pw[kLab3], pg[kLab3], df[kLab3];
+    unsigned char cl[kLab3];
 };
 
-template <typename Real, bool kWriteRhs>
+template <typename Real>
 __global__ void __launch_bounds__(256)
-rd_step_kernel(PoolView<Real> v, const Real *__restrict__ phi_in, Real *__restrict__ phi_out,
-               Real *__restrict__ dphidt_out, Real Dw, Real Dg, Real rho, double dt,
-               unsigned *nan_flag)
+face_kernel(PoolView<Real> v, Real Dw, Real Dg, Real *__restrict__ H, unsigned short *__restrict__ meta,
+            unsigned char *__restrict__ btype)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    StepSmem<Real> &S = *reinterpret_cast<StepSmem<Real> *>(smem_raw);
+    FaceSmem<Real> &S = *reinterpret_cast<FaceSmem<Real> *>(smem_raw);
     const int blk = blockIdx.x;
     const int t = threadIdx.x;
-    const int slot = v.slot[blk];
-    const int64_t base = (int64_t)slot * kBS3;
-
-    // 1. interior: 512 cells of each field, coalesced
+    const int64_t base = (int64_t)v.slot[blk] * kBS3;
     for (int c = t; c < kBS3; c += 256) {
-        const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
-        const int l = lab_index(x, y, z);
+        const int l = lab_index(c & 7, (c >> 3) & 7, c >> 6);
         S.pw[l] = v.pw[base + c];
         S.pg[l] = v.pg[base + c];
-        S.ph[l] = phi_in[base + c];
     }
-    // 2. face halos: same-level neighbours are read directly, the others
-    //    from the lab ghosts reconstructed by the ghost fill
     for (int q = t; q < 6 * kFaceCells; q += 256) {
         const int f = q >> 6, p = q & 63;
         int lx, ly, lz, sc;
@@ -72,96 +94,307 @@ rd_step_kernel(PoolView<Real> v, const Real *__restrict__ phi_in, Real *__restri
         const int l = lab_index(lx, ly, lz);
         const int nb = v.nbr[blk * 6 + f];
         if (nb >= 0) {
-            const int64_t g = (int64_t)nb * kBS3 + sc;
-            S.pw[l] = v.pw[g];
-            S.pg[l] = v.pg[g];
-            S.ph[l] = phi_in[g];
+            S.pw[l] = v.pw[(int64_t)nb * kBS3 + sc];
+            S.pg[l] = v.pg[(int64_t)nb * kBS3 + sc];
         } else {
             const int64_t g = (int64_t)blk * kLabGhosts + c_ghost_id[l];
             S.pw[l] = v.gpw[g];
             S.pg[l] = v.gpg[g];
-            S.ph[l] = v.gphi[g];
         }
     }
     __syncthreads();
-
-    // 3. df = p_w*Dw + p_g*Dg for the interior and the face halos
     for (int c = t; c < kBS3; c += 256) {
         const int l = lab_index(c & 7, (c >> 3) & 7, c >> 6);
         S.df[l] = diffusivity(S.pw[l], S.pg[l], Dw, Dg);
+        S.cl[l] = (unsigned char)cell_class(S.pw[l], S.pg[l]);
     }
     for (int q = t; q < 6 * kFaceCells; q += 256) {
         int lx, ly, lz, sc;
         face_cell(q >> 6, q & 63, lx, ly, lz, sc);
         const int l = lab_index(lx, ly, lz);
         S.df[l] = diffusivity(S.pw[l], S.pg[l], Dw, Dg);
+        S.cl[l] = (unsigned char)cell_class(S.pw[l], S.pg[l]);
     }
     __syncthreads();
-
-    // 4. harmonic means of the 3 x 576 faces
-    for (int q = t; q < 3 * 576; q += 256) {
-        const int d = q / 576, r = q - d * 576;
-        const int f = r % 9, a = (r / 9) & 7, b = r / 72;
-        int l0, l1;
-        Real *H;
-        if (d == 0) { l0 = lab_index(f - 1, a, b); l1 = lab_index(f, a, b); H = S.hx; }
-        else if (d == 1) { l0 = lab_index(a, f - 1, b); l1 = lab_index(a, f, b); H = S.hy; }
-        else { l0 = lab_index(a, b, f - 1); l1 = lab_index(a, b, f); H = S.hz; }
-        H[r] = face_harmonic(S.df[l0], S.df[l1]);
+    Real *Hb = H + (int64_t)blk * kFacesPerBlock;
+    for (int q = t; q < 576; q += 256) {
+        {
+            const int fx = q % 9, y = (q / 9) & 7, z = q / 72;
+            Hb[q] = face_harmonic(S.df[lab_index(fx - 1, y, z)], S.df[lab_index(fx, y, z)]);
+        }
+        {
+            const int x = q & 7, fy = (q >> 3) % 9, z = (q >> 3) / 9;
+            Hb[576 + q] = face_harmonic(S.df[lab_index(x, fy - 1, z)], S.df[lab_index(x, fy, z)]);
+        }
+        {
+            const int x = q & 7, y = (q >> 3) & 7, fz = q >> 6;
+            Hb[1152 + q] = face_harmonic(S.df[lab_index(x, y, fz - 1)], S.df[lab_index(x, y, fz)]);
+        }
     }
+    bool all_empty = true, all_tissue = true;
+    for (int c = t; c < kBS3; c += 256) {
+        const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
+        const int ln[6] = {lab_index(x - 1, y, z), lab_index(x + 1, y, z), lab_index(x, y - 1, z),
+                           lab_index(x, y + 1, z), lab_index(x, y, z - 1), lab_index(x, y, z + 1)};
+        unsigned m = S.cl[lab_index(x, y, z)];
+        for (int k = 0; k < 6; k++) {
+            const unsigned ck = S.cl[ln[k]];
+            if (ck == kEmpty) m |= 1u << (2 + k);
+            if (ck == kOther) m |= 1u << (8 + k);
+        }
+        meta[base + c] = (unsigned short)m;
+        all_empty &= (m == kMetaAllEmpty);
+        all_tissue &= (m == kMetaAllTissue);
+    }
+    all_empty = __syncthreads_and(all_empty);
+    all_tissue = __syncthreads_and(all_tissue);
+    if (t == 0) btype[blk] = all_empty ? kBlockEmpty : all_tissue ? kBlockTissue : kBlockMixed;
+}
+
+template <typename Real>
+cudaError_t launch_faces(const PoolView<Real> &v, Real Dw, Real Dg, Real *H, unsigned short *meta,
+                         unsigned char *btype, cudaStream_t s)
+{
+    if (v.nblocks <= 0) return cudaSuccess;
+    const size_t smem = sizeof(FaceSmem<Real>);
+    auto k = face_kernel<Real>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<v.nblocks, 256, smem, s>>>(v, Dw, Dg, H, meta, btype);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// The step: ReactionDiffusionOperator<3> + UpdateTumor<3> fused, one 8^3
+// block per CTA of 128 threads, four consecutive x cells per thread.  phi of
+// the block and of its six face halos is staged in shared memory (same-level
+// neighbours read directly, coarse-fine faces from the lab ghosts); the
+// static face coefficients and meta words come from global memory.  The
+// class shortcuts are exact; any other case reads p_w and p_g and evaluates
+// the reference expressions.  Cells outside the domain get dphidt = 0, and
+// with a finite dt their update phi + dt*0 rounds back to phi, so only the
+// clamp remains.
+constexpr int kPitch = 16;                  // shared lab row: x in [-1,9) at offsets 3..12
+constexpr int kPlane = kPitch * kLab;
+constexpr int kStepLab = kPlane * kLab;
+
+__device__ __forceinline__ int lab_p(int x, int y, int z) { return (x + 4) + kPitch * ((y + 1) + kLab * (z + 1)); }
+
+template <typename Real>
+__device__ __forceinline__ void lab_pwpg(const PoolView<Real> &v, int blk, int64_t base, int lx, int ly, int lz,
+                                         Real &pw, Real &pg)
+{
+    if (lx >= 0 && lx < kBS && ly >= 0 && ly < kBS && lz >= 0 && lz < kBS) {
+        const int64_t g = base + lx + kBS * (ly + kBS * lz);
+        pw = v.pw[g];
+        pg = v.pg[g];
+        return;
+    }
+    const int f = lx < 0 ? 0 : lx >= kBS ? 1 : ly < 0 ? 2 : ly >= kBS ? 3 : lz < 0 ? 4 : 5;
+    const int nb = v.nbr[blk * 6 + f];
+    if (nb >= 0) {
+        const int sx = (lx + kBS) & 7, sy = (ly + kBS) & 7, sz = (lz + kBS) & 7;
+        const int64_t g = (int64_t)nb * kBS3 + sx + kBS * (sy + kBS * sz);
+        pw = v.pw[g];
+        pg = v.pg[g];
+    } else {
+        const int64_t g = (int64_t)blk * kLabGhosts + c_ghost_id[lab_index(lx, ly, lz)];
+        pw = v.gpw[g];
+        pg = v.gpg[g];
+    }
+}
+
+template <typename Real> struct Vec4;
+template <> struct Vec4<float> {
+    float v[4];
+    __device__ __forceinline__ void load(const float *p)
+    {
+        const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    }
+    __device__ __forceinline__ void store(float *p) const
+    {
+        *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+};
+template <> struct Vec4<double> {
+    double v[4];
+    __device__ __forceinline__ void load(const double *p)
+    {
+        const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+        const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+    __device__ __forceinline__ void store(double *p) const
+    {
+        reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+    }
+};
+
+// Same-level neighbour block of face f: arithmetic on a uniform periodic
+// power-of-two grid, else the neighbour table.
+template <typename Real>
+__device__ __forceinline__ int face_neighbour(const PoolView<Real> &v, int blk, int f)
+{
+    if (v.log2_bpd >= 0) {
+        const int L = v.log2_bpd, m = (1 << L) - 1;
+        int bx = blk & m, by = (blk >> L) & m, bz = blk >> (2 * L);
+        const int d = f >> 1, s = (f & 1) ? 1 : -1;
+        if (d == 0) bx = (bx + s) & m;
+        else if (d == 1) by = (by + s) & m;
+        else bz = (bz + s) & m;
+        return bx | (by << L) | (bz << (2 * L));
+    }
+    return v.nbr[blk * 6 + f];
+}
+
+template <typename Real, bool kWriteRhs>
+__global__ void __launch_bounds__(128, sizeof(Real) == 4 ? 8 : 5)
+rd_step_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
+               const double *__restrict__ ih2blk, const Real *__restrict__ phi_in, Real *__restrict__ phi_out,
+               Real *__restrict__ dphidt_out, Real rho, double dt, int dt_finite, unsigned *nan_flag)
+{
+    __shared__ __align__(16) Real ph[kStepLab];
+    const int blk = blockIdx.x;
+    const int t = threadIdx.x;
+    const int64_t base = (int64_t)(v.identity_slots ? blk : v.slot[blk]) * kBS3;
+    const int x4 = (t & 1) * 4, y = (t >> 1) & 7, z = t >> 4;
+    const int c0 = x4 + kBS * (y + kBS * z);
+    const int l0 = lab_p(x4, y, z);
+
+    // one round trip: own cells, block type (and meta if mixed), face halos
+    Vec4<Real> p;
+    p.load(phi_in + base + c0);
+    const unsigned char bt = __ldg(v.btype + blk);
+    Real halo[3];
+    int hlab[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const int q = t + 128 * i;
+        const int f = q >> 6, pc = q & 63;  // f is uniform across a warp
+        int lx, ly, lz, sc;
+        face_cell(f, pc, lx, ly, lz, sc);
+        hlab[i] = lab_p(lx, ly, lz);
+        const int nb = face_neighbour(v, blk, f);
+        if (nb >= 0) halo[i] = phi_in[(int64_t)nb * kBS3 + sc];
+        else halo[i] = v.gphi[(int64_t)blk * kLabGhosts + c_ghost_id[lab_index(lx, ly, lz)]];
+    }
+    unsigned mw[4];
+    if (bt == kBlockMixed) {
+        const uint2 mraw = __ldg(reinterpret_cast<const uint2 *>(meta + base + c0));
+        mw[0] = mraw.x & 0xffffu; mw[1] = mraw.x >> 16; mw[2] = mraw.y & 0xffffu; mw[3] = mraw.y >> 16;
+    } else {
+        const unsigned m = bt == kBlockEmpty ? kMetaAllEmpty : kMetaAllTissue;
+        mw[0] = mw[1] = mw[2] = mw[3] = m;
+    }
+
+    bool dom[4];
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const unsigned cls = mw[i] & 3u;
+        const Real phi = p.v[i];
+        if (cls == kTissue && phi >= (Real)0) dom[i] = true;
+        else if (cls == kEmpty) dom[i] = phi > (Real)0;
+        else {
+            Real pw, pg;
+            lab_pwpg(v, blk, base, x4 + i, y, z, pw, pg);
+            dom[i] = in_domain(pw, pg, phi);
+        }
+        any |= dom[i];
+    }
+    // face coefficients of the cells inside the domain, issued before the barrier
+    Real hx[5];
+    Vec4<Real> hym, hyp, hzm, hzp;
+    if (any) {
+        const Real *Hb = H + (int64_t)blk * kFacesPerBlock;
+        const int rx = (z * 8 + y) * 9 + x4;
+#pragma unroll
+        for (int i = 0; i < 5; i++) hx[i] = __ldg(Hb + rx + i);
+        hym.load(Hb + 576 + (z * 9 + y) * 8 + x4);
+        hyp.load(Hb + 576 + (z * 9 + y + 1) * 8 + x4);
+        hzm.load(Hb + 1152 + (z * 8 + y) * 8 + x4);
+        hzp.load(Hb + 1152 + ((z + 1) * 8 + y) * 8 + x4);
+    }
+    p.store(ph + l0);
+#pragma unroll
+    for (int i = 0; i < 3; i++) ph[hlab[i]] = halo[i];
     __syncthreads();
 
-    // 5. flux, reaction and update: thread -> (x, y) column, z = t>>6 and +4
-    const double h = (double)v.hblk[blk];
-    const double ih2 = 1. / (h * h);
-    const int x = t & 7, y = (t >> 3) & 7;
+    Vec4<Real> out;
     bool bad = false;
+    if (any) {
+        const double ih2 = ih2blk[blk];
+        const Real eps = (Real)0.1;
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const int z = (t >> 6) + 4 * k;
-        const int l = lab_index(x, y, z);
-        const Real phi = S.ph[l];
-        Real dphidt = (Real)0.;
-        if (in_domain(S.pw[l], S.pg[l], phi)) {
-            const int ln[6] = {lab_index(x - 1, y, z), lab_index(x + 1, y, z), lab_index(x, y - 1, z),
-                               lab_index(x, y + 1, z), lab_index(x, y, z - 1), lab_index(x, y, z + 1)};
-            Real chf[6], phn[6];
+        for (int i = 0; i < 4; i++) {
+            const Real phi = p.v[i];
+            Real dphidt = (Real)0.;
+            if (dom[i]) {
+                const int l = l0 + i;
+                Real phn[6];
+                phn[0] = i == 0 ? ph[l - 1] : p.v[i - 1];
+                phn[1] = i == 3 ? ph[l + 1] : p.v[i + 1];
+                phn[2] = ph[l - kPitch];
+                phn[3] = ph[l + kPitch];
+                phn[4] = ph[l - kPlane];
+                phn[5] = ph[l + kPlane];
+                bool low[6];
 #pragma unroll
-            for (int i = 0; i < 6; i++) {
-                phn[i] = S.ph[ln[i]];
-                chf[i] = domain_chf(phn[i], S.pw[ln[i]], S.pg[ln[i]]);
+                for (int k = 0; k < 6; k++) {
+                    if ((mw[i] >> (2 + k)) & 1u) {
+                        low[k] = phn[k] < eps;
+                    } else if (!((mw[i] >> (8 + k)) & 1u) && phn[k] >= (Real)0) {
+                        low[k] = false;
+                    } else {
+                        const int x = x4 + i;
+                        const int nx = x + (k == 0 ? -1 : k == 1 ? 1 : 0);
+                        const int ny = y + (k == 2 ? -1 : k == 3 ? 1 : 0);
+                        const int nz = z + (k == 4 ? -1 : k == 5 ? 1 : 0);
+                        Real pw, pg;
+                        lab_pwpg(v, blk, base, nx, ny, nz, pw, pg);
+                        low[k] = domain_chf(phn[k], pw, pg) < eps;
+                    }
+                }
+                dphidt = cell_rhs_flags<Real>(hx[i], hx[i + 1], hym.v[i], hyp.v[i], hzm.v[i], hzp.v[i], low, phn,
+                                              phi, rho, ih2);
             }
-            const int rx = (z * 8 + y) * 9, ry = (z * 8 + x) * 9, rz = (y * 8 + x) * 9;
-            dphidt = cell_rhs<Real>(S.hx[rx + x], S.hx[rx + x + 1], S.hy[ry + y], S.hy[ry + y + 1],
-                                    S.hz[rz + z], S.hz[rz + z + 1], chf, phn, phi, rho, ih2);
+            if (kWriteRhs) out.v[i] = dphidt;
+            else {
+                const Real q = (!dom[i] && dt_finite) ? clamp01(phi) : cell_update(phi, dphidt, dt);
+                bad |= (q != q);
+                out.v[i] = q;
+            }
         }
-        const int c = x + kBS * (y + kBS * z);
-        if (kWriteRhs) {
-            dphidt_out[base + c] = dphidt;
-        } else {
-            const Real p = cell_update(phi, dphidt, dt);
-            bad |= (p != p);
-            phi_out[base + c] = p;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            if (kWriteRhs) out.v[i] = (Real)0.;
+            else {
+                const Real q = dt_finite ? clamp01(p.v[i]) : cell_update(p.v[i], (Real)0., dt);
+                bad |= (q != q);
+                out.v[i] = q;
+            }
         }
     }
+    if (kWriteRhs) out.store(dphidt_out + base + c0);
+    else out.store(phi_out + base + c0);
     if (!kWriteRhs && bad) atomicOr(nan_flag, 1u);
 }
 
 template <typename Real>
-cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *phi_in, Real *phi_out, Real *dphidt_out,
-                           Real Dw, Real Dg, Real rho, double dt, unsigned *nan_flag, cudaStream_t s)
+cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigned short *meta, const double *ih2,
+                           const Real *phi_in, Real *phi_out, Real *dphidt_out, Real rho, double dt,
+                           unsigned *nan_flag, cudaStream_t s)
 {
     if (v.nblocks <= 0) return cudaSuccess;
-    const size_t smem = sizeof(StepSmem<Real>);
-    if (dphidt_out) {
-        auto k = rd_step_kernel<Real, true>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<v.nblocks, 256, smem, s>>>(v, phi_in, phi_out, dphidt_out, Dw, Dg, rho, dt, nan_flag);
-    } else {
-        auto k = rd_step_kernel<Real, false>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<v.nblocks, 256, smem, s>>>(v, phi_in, phi_out, dphidt_out, Dw, Dg, rho, dt, nan_flag);
-    }
+    const int dt_finite = isfinite(dt) ? 1 : 0;
+    if (dphidt_out)
+        rd_step_kernel<Real, true><<<v.nblocks, 128, 0, s>>>(v, H, meta, ih2, phi_in, phi_out, dphidt_out, rho, dt,
+                                                             dt_finite, nan_flag);
+    else
+        rd_step_kernel<Real, false><<<v.nblocks, 128, 0, s>>>(v, H, meta, ih2, phi_in, phi_out, dphidt_out, rho,
+                                                              dt, dt_finite, nan_flag);
     return cudaGetLastError();
 }
 
@@ -417,8 +650,11 @@ cudaError_t upload_ghost_table()
 }
 
 #define GBFK_INSTANTIATE(Real)                                                                               \
-    template cudaError_t launch_rd_step<Real>(const PoolView<Real> &, const Real *, Real *, Real *, Real, Real, \
-                                              Real, double, unsigned *, cudaStream_t);                       \
+    template cudaError_t launch_rd_step<Real>(const PoolView<Real> &, const Real *, const unsigned short *,    \
+                                              const double *, const Real *, Real *, Real *, Real, double,     \
+                                              unsigned *, cudaStream_t);                                      \
+    template cudaError_t launch_faces<Real>(const PoolView<Real> &, Real, Real, Real *, unsigned short *,       \
+                                            unsigned char *, cudaStream_t);                                   \
     template cudaError_t launch_fill_ghosts<Real>(const int *, int64_t, const int64_t *, const int *,         \
                                                   const Real *, const Real *, Real *, cudaStream_t);          \
     template cudaError_t launch_fwt_details<Real>(const PoolView<Real> &, const Real *, double *, cudaStream_t); \

@@ -11,6 +11,10 @@ constexpr int kLab = 10;          // lab extent per direction, [-1, 9)
 constexpr int kLab3 = 1000;
 constexpr int kLabGhosts = 488;
 constexpr int kFaceCells = 64;
+constexpr int kFacesPerBlock = 3 * 576;  // x, y, z faces of a block incl. its boundary faces
+
+// cell classes for the step's exact shortcuts (see cell_class)
+constexpr unsigned char kEmpty = 0, kTissue = 1, kOther = 2;
 
 // Per-topology device data shared by the kernels.
 template <typename Real>
@@ -23,13 +27,28 @@ struct PoolView {
     const Real *gphi;      // [nblocks*488] lab ghosts of phi (refreshed per step where needed)
     const Real *pw;        // pool fields
     const Real *pg;
+    const unsigned char *btype;  // [nblocks] block type of the step (kBlockEmpty / kBlockTissue / kBlockMixed)
     int nblocks;
+    int identity_slots;    // slot[i] == i for every block
+    int log2_bpd;          // uniform periodic grid of 2^log2_bpd blocks per direction, else -1
 };
 
+// Block types: every cell of the block and of its face halos is kEmpty
+// (kBlockEmpty) or kTissue (kBlockTissue); otherwise the per-cell meta words
+// are read (kBlockMixed).
+constexpr unsigned char kBlockEmpty = 0, kBlockTissue = 1, kBlockMixed = 2;
+
+// Harmonic means of all faces of every block for (Dw, Dg): H[nblocks * 1728],
+// and the per-cell meta words (class + neighbour class masks, pool-indexed).
 template <typename Real>
-cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *phi_in, Real *phi_out, Real *dphidt_out,
-                           Real Dw, Real Dg, Real rho, double dt, unsigned *nan_flag,
-                           cudaStream_t s);
+cudaError_t launch_faces(const PoolView<Real> &v, Real Dw, Real Dg, Real *H, unsigned short *meta,
+                         unsigned char *btype, cudaStream_t s);
+
+// One fused step (or, with dphidt_out, the operator alone).
+template <typename Real>
+cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigned short *meta, const double *ih2,
+                           const Real *phi_in, Real *phi_out, Real *dphidt_out, Real rho, double dt,
+                           unsigned *nan_flag, cudaStream_t s);
 
 template <typename Real>
 cudaError_t launch_fill_ghosts(const int *rows, int64_t nrows, const int64_t *row_ptr, const int *src,
