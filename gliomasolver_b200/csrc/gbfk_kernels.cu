@@ -262,23 +262,10 @@ rd_step_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned shor
     const int c0 = x4 + kBS * (y + kBS * z);
     const int l0 = lab_p(x4, y, z);
 
-    // one round trip: own cells, block type (and meta if mixed), face halos
+    // own cells, block type (and meta words if the block is mixed)
     Vec4<Real> p;
     p.load(phi_in + base + c0);
     const unsigned char bt = __ldg(v.btype + blk);
-    Real halo[3];
-    int hlab[3];
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-        const int q = t + 128 * i;
-        const int f = q >> 6, pc = q & 63;  // f is uniform across a warp
-        int lx, ly, lz, sc;
-        face_cell(f, pc, lx, ly, lz, sc);
-        hlab[i] = lab_p(lx, ly, lz);
-        const int nb = face_neighbour(v, blk, f);
-        if (nb >= 0) halo[i] = phi_in[(int64_t)nb * kBS3 + sc];
-        else halo[i] = v.gphi[(int64_t)blk * kLabGhosts + c_ghost_id[lab_index(lx, ly, lz)]];
-    }
     unsigned mw[4];
     if (bt == kBlockMixed) {
         const uint2 mraw = __ldg(reinterpret_cast<const uint2 *>(meta + base + c0));
@@ -287,7 +274,6 @@ rd_step_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned shor
         const unsigned m = bt == kBlockEmpty ? kMetaAllEmpty : kMetaAllTissue;
         mw[0] = mw[1] = mw[2] = mw[3] = m;
     }
-
     bool dom[4];
     bool any = false;
 #pragma unroll
@@ -303,7 +289,42 @@ rd_step_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned shor
         }
         any |= dom[i];
     }
-    // face coefficients of the cells inside the domain, issued before the barrier
+
+    Vec4<Real> out;
+    bool bad = false;
+    // a block with no cell inside the domain only needs the clamp of the
+    // update (dphidt = 0 everywhere): no halo, no face coefficients
+    if (!__syncthreads_or(any)) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            if (kWriteRhs) out.v[i] = (Real)0.;
+            else {
+                const Real q = dt_finite ? clamp01(p.v[i]) : cell_update(p.v[i], (Real)0., dt);
+                bad |= (q != q);
+                out.v[i] = q;
+            }
+        }
+        if (kWriteRhs) out.store(dphidt_out + base + c0);
+        else out.store(phi_out + base + c0);
+        if (!kWriteRhs && bad) atomicOr(nan_flag, 1u);
+        return;
+    }
+
+    // face halos: 3 per thread, the face index is uniform across a warp
+    Real halo[3];
+    int hlab[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const int q = t + 128 * i;
+        const int f = q >> 6, pc = q & 63;
+        int lx, ly, lz, sc;
+        face_cell(f, pc, lx, ly, lz, sc);
+        hlab[i] = lab_p(lx, ly, lz);
+        const int nb = face_neighbour(v, blk, f);
+        if (nb >= 0) halo[i] = phi_in[(int64_t)nb * kBS3 + sc];
+        else halo[i] = v.gphi[(int64_t)blk * kLabGhosts + c_ghost_id[lab_index(lx, ly, lz)]];
+    }
+    // face coefficients of the own cells inside the domain
     Real hx[5];
     Vec4<Real> hym, hyp, hzm, hzp;
     if (any) {
@@ -321,60 +342,56 @@ rd_step_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned shor
     for (int i = 0; i < 3; i++) ph[hlab[i]] = halo[i];
     __syncthreads();
 
-    Vec4<Real> out;
-    bool bad = false;
-    if (any) {
-        const double ih2 = ih2blk[blk];
-        const Real eps = (Real)0.1;
+    const double ih2 = ih2blk[blk];
+    const Real eps = (Real)0.1;
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const Real phi = p.v[i];
-            Real dphidt = (Real)0.;
-            if (dom[i]) {
-                const int l = l0 + i;
-                Real phn[6];
-                phn[0] = i == 0 ? ph[l - 1] : p.v[i - 1];
-                phn[1] = i == 3 ? ph[l + 1] : p.v[i + 1];
-                phn[2] = ph[l - kPitch];
-                phn[3] = ph[l + kPitch];
-                phn[4] = ph[l - kPlane];
-                phn[5] = ph[l + kPlane];
-                bool low[6];
+    for (int i = 0; i < 4; i++) {
+        const Real phi = p.v[i];
+        Real dphidt = (Real)0.;
+        if (dom[i]) {
+            const int l = l0 + i;
+            Real phn[6];
+            phn[0] = i == 0 ? ph[l - 1] : p.v[i - 1];
+            phn[1] = i == 3 ? ph[l + 1] : p.v[i + 1];
+            phn[2] = ph[l - kPitch];
+            phn[3] = ph[l + kPitch];
+            phn[4] = ph[l - kPlane];
+            phn[5] = ph[l + kPlane];
+            bool low[6];
 #pragma unroll
-                for (int k = 0; k < 6; k++) {
-                    if ((mw[i] >> (2 + k)) & 1u) {
-                        low[k] = phn[k] < eps;
-                    } else if (!((mw[i] >> (8 + k)) & 1u) && phn[k] >= (Real)0) {
-                        low[k] = false;
-                    } else {
-                        const int x = x4 + i;
-                        const int nx = x + (k == 0 ? -1 : k == 1 ? 1 : 0);
-                        const int ny = y + (k == 2 ? -1 : k == 3 ? 1 : 0);
-                        const int nz = z + (k == 4 ? -1 : k == 5 ? 1 : 0);
-                        Real pw, pg;
-                        lab_pwpg(v, blk, base, nx, ny, nz, pw, pg);
-                        low[k] = domain_chf(phn[k], pw, pg) < eps;
-                    }
+            for (int k = 0; k < 6; k++) {
+                bool slow;
+                if (bt == kBlockTissue) {
+                    low[k] = false;
+                    slow = !(phn[k] >= (Real)0);
+                } else if (bt == kBlockEmpty) {
+                    low[k] = phn[k] < eps;
+                    slow = false;
+                } else if ((mw[i] >> (2 + k)) & 1u) {
+                    low[k] = phn[k] < eps;
+                    slow = false;
+                } else {
+                    low[k] = false;
+                    slow = ((mw[i] >> (8 + k)) & 1u) || !(phn[k] >= (Real)0);
                 }
-                dphidt = cell_rhs_flags<Real>(hx[i], hx[i + 1], hym.v[i], hyp.v[i], hzm.v[i], hzp.v[i], low, phn,
-                                              phi, rho, ih2);
+                if (slow) {
+                    const int x = x4 + i;
+                    const int nx = x + (k == 0 ? -1 : k == 1 ? 1 : 0);
+                    const int ny = y + (k == 2 ? -1 : k == 3 ? 1 : 0);
+                    const int nz = z + (k == 4 ? -1 : k == 5 ? 1 : 0);
+                    Real pw, pg;
+                    lab_pwpg(v, blk, base, nx, ny, nz, pw, pg);
+                    low[k] = domain_chf(phn[k], pw, pg) < eps;
+                }
             }
-            if (kWriteRhs) out.v[i] = dphidt;
-            else {
-                const Real q = (!dom[i] && dt_finite) ? clamp01(phi) : cell_update(phi, dphidt, dt);
-                bad |= (q != q);
-                out.v[i] = q;
-            }
+            dphidt = cell_rhs_flags<Real>(hx[i], hx[i + 1], hym.v[i], hyp.v[i], hzm.v[i], hzp.v[i], low, phn, phi,
+                                          rho, ih2);
         }
-    } else {
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            if (kWriteRhs) out.v[i] = (Real)0.;
-            else {
-                const Real q = dt_finite ? clamp01(p.v[i]) : cell_update(p.v[i], (Real)0., dt);
-                bad |= (q != q);
-                out.v[i] = q;
-            }
+        if (kWriteRhs) out.v[i] = dphidt;
+        else {
+            const Real q = (!dom[i] && dt_finite) ? clamp01(phi) : cell_update(phi, dphidt, dt);
+            bad |= (q != q);
+            out.v[i] = q;
         }
     }
     if (kWriteRhs) out.store(dphidt_out + base + c0);
