@@ -21,6 +21,7 @@ STATUS = {
     4: "GBFK_E_NAN",
     5: "GBFK_E_TIMEOUT",
     6: "GBFK_E_STATE",
+    7: "GBFK_E_TOO_LARGE",
 }
 GBFK_F64, GBFK_F32 = 0, 1
 GBFK_PHI, GBFK_PW, GBFK_PG = 0, 1, 2
@@ -31,6 +32,7 @@ EXPORTS = (
     "gbfk_set_uniform", "gbfk_set_topology", "gbfk_num_blocks",
     "gbfk_upload_field", "gbfk_download_field", "gbfk_upload_dense", "gbfk_download_dense",
     "gbfk_rd_step", "gbfk_rd_rhs", "gbfk_fwt_details", "gbfk_split", "gbfk_collapse",
+    "gbfk_rd_step_static",
 )
 
 
@@ -102,6 +104,7 @@ def load(path: Path | str | None = None):
         "gbfk_fwt_details": (I, [P, P]),
         "gbfk_split": (I, [P, I, P, P]),
         "gbfk_collapse": (I, [P, I, P, P]),
+        "gbfk_rd_step_static": (I, [I, I, P, P, P, P, D, D, D, D, P, I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -51,7 +51,8 @@ enum gbfk_status {
     GBFK_E_OOM = 3,     /* device allocation failed or pool too small */
     GBFK_E_NAN = 4,     /* a step produced NaN/Inf in phi */
     GBFK_E_TIMEOUT = 5, /* a bounded device wait gave up */
-    GBFK_E_STATE = 6    /* required data (topology, fields) not uploaded */
+    GBFK_E_STATE = 6,   /* required data (topology, fields) not uploaded */
+    GBFK_E_TOO_LARGE = 7 /* grid larger than gbfk_rd_step_static's fixed scratch */
 };
 
 enum gbfk_precision { GBFK_F64 = 0, GBFK_F32 = 1 };
@@ -154,6 +155,31 @@ int gbfk_split(gbfk_ctx *ctx, int nsplit, const int *parents, const int *childre
  * analysis (injection; BlockCollapser::_collapseBlocks, MRAGBlockCollapser.h:
  * 22-84).  children[8*i + c] as for gbfk_split; parents[i] is a slot. */
 int gbfk_collapse(gbfk_ctx *ctx, int ncollapse, const int *children, const int *parents);
+
+/* --- allocation-free step -------------------------------------------- */
+/* No counterpart in the reference.  One fused RD step (the operator and the
+ * update of gbfk_rd_step) on a uniform periodic bpd^3 grid, for callers that
+ * cannot let the library call cudaMalloc: code whose device memory belongs to
+ * another allocator that reserved it up front, or a time loop that must not
+ * pay cudaMalloc's device-wide synchronisation.  It allocates nothing and
+ * frees nothing: its scratch (face coefficients, meta words, block types,
+ * neighbour table) is one fixed device array of about 7.3 MiB that every GPU
+ * loading the library holds until the process exits.
+ *   pw, pg, phi_in : device arrays of bpd^3 * 512 Real in block-pool order
+ *                    (block (bx,by,bz) at slot bx + bpd*(by + bpd*bz));
+ *   phi_out        : device array of the same size, not phi_in;
+ *   Dw, Dg, rho, dt: as for gbfk_rd_step; stream: cudaStream_t or NULL for
+ *                    the legacy default stream; device: CUDA ordinal.
+ * Returns GBFK_E_TOO_LARGE when bpd^3 > GBFK_STATIC_MAX_BLOCKS.  Every call
+ * on a device shares the scratch array (it keeps the last call's contents and
+ * is fully rewritten by each call), so calls that overlap on the GPU race:
+ * serialise them.  The first call on a device looks up the array's address
+ * with that device current; make it before any stream capture.  The work is
+ * asynchronous on the stream. */
+#define GBFK_STATIC_MAX_BLOCKS 512
+int gbfk_rd_step_static(int precision, int bpd, const void *pw, const void *pg, const void *phi_in,
+                        void *phi_out, double Dw, double Dg, double rho, double dt, void *stream,
+                        int device);
 
 #ifdef __cplusplus
 }
