@@ -248,8 +248,16 @@ __device__ __forceinline__ int face_neighbour(const PoolView<Real> &v, int blk, 
     return v.nbr[blk * 6 + f];
 }
 
+// resident CTAs per SM the register allocation targets (FP32 / FP64)
+#ifndef GBFK_STEP_MIN_BLOCKS_F32
+#define GBFK_STEP_MIN_BLOCKS_F32 16
+#endif
+#ifndef GBFK_STEP_MIN_BLOCKS_F64
+#define GBFK_STEP_MIN_BLOCKS_F64 5
+#endif
+
 template <typename Real, bool kWriteRhs>
-__global__ void __launch_bounds__(128, sizeof(Real) == 4 ? 8 : 5)
+__global__ void __launch_bounds__(128, sizeof(Real) == 4 ? GBFK_STEP_MIN_BLOCKS_F32 : GBFK_STEP_MIN_BLOCKS_F64)
 rd_step_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
                const double *__restrict__ ih2blk, const Real *__restrict__ phi_in, Real *__restrict__ phi_out,
                Real *__restrict__ dphidt_out, Real rho, double dt, int dt_finite, unsigned *nan_flag)
