@@ -33,6 +33,7 @@ EXPORTS = (
     "gbfk_upload_field", "gbfk_download_field", "gbfk_upload_dense", "gbfk_download_dense",
     "gbfk_rd_step", "gbfk_rd_rhs", "gbfk_fwt_details", "gbfk_split", "gbfk_collapse",
     "gbfk_rd_step_static",
+    "gbfk_set_observations", "gbfk_uq_dump", "gbfk_log_likelihood",
 )
 
 
@@ -57,6 +58,18 @@ class BlockInfo(ctypes.Structure):
         ("level", ctypes.c_int),
         ("index", ctypes.c_int * 3),
         ("h", ctypes.c_double),
+    ]
+
+
+class LikelihoodParams(ctypes.Structure):
+    _fields_ = [
+        ("pet_sigma2", ctypes.c_double),
+        ("pet_scale", ctypes.c_double),
+        ("t1_uc", ctypes.c_double),
+        ("t2_uc", ctypes.c_double),
+        ("slope", ctypes.c_double),
+        ("step_pet", ctypes.c_int),
+        ("step_mri", ctypes.c_int),
     ]
 
 
@@ -105,6 +118,9 @@ def load(path: Path | str | None = None):
         "gbfk_split": (I, [P, I, P, P]),
         "gbfk_collapse": (I, [P, I, P, P]),
         "gbfk_rd_step_static": (I, [I, I, P, P, P, P, D, D, D, D, P, I]),
+        "gbfk_set_observations": (I, [P, I, P, P, P, P, I]),
+        "gbfk_uq_dump": (I, [P, I, P]),
+        "gbfk_log_likelihood": (I, [P, ctypes.POINTER(LikelihoodParams), P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

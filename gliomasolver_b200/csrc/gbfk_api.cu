@@ -57,6 +57,19 @@ struct gbfk_ctx {
     bool static_ghosts_dirty = true;
 
     // static per (topology, p_w, p_g): cell classes; per (.., Dw, Dg): face coefficients
+    void *d_origin = nullptr;         // nblocks * 3 Real: BlockInfo::origin
+
+    // observations for the likelihood (n^3 grid)
+    int obs_n = 0;
+    unsigned char *d_t1c = nullptr, *d_flair = nullptr;
+    double *d_pet = nullptr;
+    int *d_roi = nullptr;
+    int nroi = 0;
+    double *d_model = nullptr;        // dump grid
+    size_t model_bytes = 0;
+    double *d_partial = nullptr;      // likelihood partial sums
+    double *d_lik = nullptr;          // 4 results
+
     unsigned short *d_meta = nullptr; // max_blocks * 512 meta words, indexed like the pool
     unsigned char *d_btype = nullptr; // nblocks block types
     bool identity_slots = false;
@@ -116,7 +129,7 @@ void free_topology(gbfk_ctx *c)
 {
     void **ptrs[] = {(void **)&c->d_slot, (void **)&c->d_nbr, &c->d_h, (void **)&c->d_row_ptr, (void **)&c->d_src,
                      &c->d_w, (void **)&c->d_step_rows, (void **)&c->d_all_rows, &c->d_gpw, &c->d_gpg,
-                     &c->d_gphi, (void **)&c->d_fwt, &c->d_H, (void **)&c->d_ih2, (void **)&c->d_btype};
+                     &c->d_gphi, (void **)&c->d_fwt, &c->d_H, (void **)&c->d_ih2, (void **)&c->d_btype, &c->d_origin};
     for (void **p : ptrs) {
         if (*p) cudaFree(*p);
         *p = nullptr;
@@ -135,6 +148,23 @@ void invalidate_static(gbfk_ctx *c)
 {
     c->static_ghosts_dirty = true;
     c->faces_valid = false;
+}
+
+// Per-block BlockInfo::origin = index * 2^-level in Real (MRAGrid.inl:208-212).
+int upload_origin(gbfk_ctx *ctx, const std::vector<int> &level, const std::vector<int> &index)
+{
+    const int nb = ctx->nblocks;
+    std::vector<double> o(3 * (size_t)nb);
+    for (int i = 0; i < nb; i++)
+        for (int d = 0; d < 3; d++) o[3 * i + d] = index[3 * i + d] * ldexp(1.0, -level[i]);
+    CK(cudaMalloc(&ctx->d_origin, 3 * (size_t)nb * ctx->rsize));
+    if (ctx->precision == GBFK_F64) {
+        CK(cudaMemcpy(ctx->d_origin, o.data(), o.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(o.begin(), o.end());
+        CK(cudaMemcpy(ctx->d_origin, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return GBFK_OK;
 }
 
 // Per-block 1/(h*h) in double, as the operator forms it (ReactionDiffusionOperator.h:49-50).
@@ -538,7 +568,8 @@ int gbfk_destroy(gbfk_ctx *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_topology(ctx);
-    void *ptrs[] = {ctx->phi[0], ctx->phi[1], ctx->pw, ctx->pg, ctx->d_nan, ctx->d_stage, ctx->d_ints, ctx->d_meta};
+    void *ptrs[] = {ctx->phi[0], ctx->phi[1], ctx->pw, ctx->pg, ctx->d_nan, ctx->d_stage, ctx->d_ints, ctx->d_meta,
+                    ctx->d_t1c, ctx->d_flair, ctx->d_pet, ctx->d_roi, ctx->d_model, ctx->d_partial, ctx->d_lik};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -605,6 +636,18 @@ int gbfk_set_uniform(gbfk_ctx *ctx, int bpd)
     }
     int rc = upload_ih2(ctx);
     if (rc) return rc;
+    {
+        int L = 0;
+        while ((1 << L) < bpd) L++;
+        std::vector<int> level(nb, L), index(3 * (size_t)nb);
+        for (int b = 0; b < nb; b++) {
+            index[3 * b] = b % bpd;
+            index[3 * b + 1] = (b / bpd) % bpd;
+            index[3 * b + 2] = b / (bpd * bpd);
+        }
+        if ((1 << L) == bpd) rc = upload_origin(ctx, level, index);
+    }
+    if (rc) return rc;
     ctx->have_topology = true;
     return GBFK_OK;
 }
@@ -663,6 +706,15 @@ int gbfk_set_topology(gbfk_ctx *ctx, const gbfk_blockinfo *blocks, int nblocks, 
     if (rc) return rc;
     rc = upload_ih2(ctx);
     if (rc) return rc;
+    {
+        std::vector<int> level(nblocks), index(3 * (size_t)nblocks);
+        for (int i = 0; i < nblocks; i++) {
+            level[i] = blocks[i].level;
+            for (int d = 0; d < 3; d++) index[3 * i + d] = blocks[i].index[d];
+        }
+        rc = upload_origin(ctx, level, index);
+        if (rc) return rc;
+    }
     ctx->have_topology = true;
     return GBFK_OK;
 }
@@ -784,6 +836,111 @@ int gbfk_collapse(gbfk_ctx *ctx, int n, const int *children, const int *parents)
     CK(cudaSetDevice(ctx->device));
     return ctx->precision == GBFK_F64 ? collapse_impl<double>(ctx, n, children, parents)
                                       : collapse_impl<float>(ctx, n, children, parents);
+}
+
+static int dump_to_device(gbfk_ctx *ctx, int n)
+{
+    if (!ctx->have_topology) return fail(ctx, GBFK_E_STATE, "uq_dump: no topology");
+    if (!ctx->d_origin) return fail(ctx, GBFK_E_STATE, "uq_dump: block origins unknown (non power-of-two uniform grid)");
+    if (n <= 0 || (int64_t)n * n * n > ((int64_t)1 << 34)) return fail(ctx, GBFK_E_INVALID, "uq_dump: bad grid size %d", n);
+    const size_t bytes = (size_t)n * n * n * sizeof(double);
+    if (ctx->model_bytes < bytes) {
+        if (ctx->d_model) cudaFree(ctx->d_model);
+        ctx->d_model = nullptr;
+        ctx->model_bytes = 0;
+        CK(cudaMalloc(&ctx->d_model, bytes));
+        ctx->model_bytes = bytes;
+    }
+    if (ctx->precision == GBFK_F64)
+        CK(launch_uq_dump<double>(ctx->d_slot, (const double *)ctx->d_origin, (const double *)ctx->d_h, ctx->nblocks,
+                                  (const double *)ctx->phi[ctx->cur], n, ctx->d_model, ctx->stream));
+    else
+        CK(launch_uq_dump<float>(ctx->d_slot, (const float *)ctx->d_origin, (const float *)ctx->d_h, ctx->nblocks,
+                                 (const float *)ctx->phi[ctx->cur], n, ctx->d_model, ctx->stream));
+    ctx->launches++;
+    return GBFK_OK;
+}
+
+int gbfk_uq_dump(gbfk_ctx *ctx, int n, double *host_out)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!host_out) return fail(ctx, GBFK_E_INVALID, "uq_dump: null output");
+    CK(cudaSetDevice(ctx->device));
+    int rc = dump_to_device(ctx, n);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(host_out, ctx->d_model, (size_t)n * n * n * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GBFK_OK;
+}
+
+int gbfk_set_observations(gbfk_ctx *ctx, int n, const double *t1c, const double *flair, const double *pet,
+                          const int *roi, int nroi)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (n <= 0 || !t1c || !flair || nroi < 0 || (nroi > 0 && !roi))
+        return fail(ctx, GBFK_E_INVALID, "set_observations: bad arguments");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    void *old[] = {ctx->d_t1c, ctx->d_flair, ctx->d_pet, ctx->d_roi};
+    for (void *p : old)
+        if (p) cudaFree(p);
+    ctx->d_t1c = ctx->d_flair = nullptr;
+    ctx->d_pet = nullptr;
+    ctx->d_roi = nullptr;
+    const size_t N = (size_t)n * n * n;
+    std::vector<unsigned char> a(N), b(N);
+    for (size_t i = 0; i < N; i++) {
+        a[i] = t1c[i] == 1 ? 1 : 0;
+        b[i] = flair[i] == 1 ? 1 : 0;
+    }
+    CK(cudaMalloc(&ctx->d_t1c, N));
+    CK(cudaMalloc(&ctx->d_flair, N));
+    CK(cudaMemcpy(ctx->d_t1c, a.data(), N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_flair, b.data(), N, cudaMemcpyHostToDevice));
+    if (pet) {
+        CK(cudaMalloc(&ctx->d_pet, N * sizeof(double)));
+        CK(cudaMemcpy(ctx->d_pet, pet, N * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (roi && nroi > 0) {
+        for (int i = 0; i < 3 * nroi; i++)
+            if (roi[i] < 0 || roi[i] >= n) return fail(ctx, GBFK_E_INVALID, "set_observations: ROI point out of the grid");
+        CK(cudaMalloc(&ctx->d_roi, (size_t)nroi * 3 * sizeof(int)));
+        CK(cudaMemcpy(ctx->d_roi, roi, (size_t)nroi * 3 * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    ctx->nroi = roi ? nroi : 0;
+    ctx->obs_n = n;
+    return GBFK_OK;
+}
+
+int gbfk_log_likelihood(gbfk_ctx *ctx, const gbfk_likelihood_params *p, double out[4])
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!p || !out) return fail(ctx, GBFK_E_INVALID, "log_likelihood: null argument");
+    if (!ctx->obs_n) return fail(ctx, GBFK_E_STATE, "log_likelihood: no observations");
+    if (p->step_pet <= 0 || p->step_mri <= 0 || !(p->slope != 0))
+        return fail(ctx, GBFK_E_INVALID, "log_likelihood: bad parameters");
+    CK(cudaSetDevice(ctx->device));
+    int rc = dump_to_device(ctx, ctx->obs_n);
+    if (rc) return rc;
+    const int nparts = 148 * 4;
+    if (!ctx->d_partial) CK(cudaMalloc(&ctx->d_partial, (size_t)nparts * 7 * sizeof(double)));
+    if (!ctx->d_lik) CK(cudaMalloc(&ctx->d_lik, 4 * sizeof(double)));
+    LikelihoodParams lp;
+    lp.pet_sigma2 = p->pet_sigma2;
+    lp.pet_scale = p->pet_scale;
+    lp.t1_uc = p->t1_uc;
+    lp.t2_uc = p->t2_uc;
+    lp.slope = p->slope;
+    lp.step_pet = p->step_pet;
+    lp.step_mri = p->step_mri;
+    CK(launch_likelihood(ctx->d_model, ctx->obs_n, ctx->d_t1c, ctx->d_flair, ctx->d_pet,
+                         ctx->nroi ? ctx->d_roi : nullptr, ctx->nroi, lp, ctx->d_partial, nparts, ctx->d_lik,
+                         ctx->stream));
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(out, ctx->d_lik, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GBFK_OK;
 }
 
 }  // extern "C"

@@ -65,6 +65,21 @@ template <typename Real>
 cudaError_t launch_collapse(int ncollapse, const int *children, const int *parents, Real *phi, Real *pw,
                             Real *pg, cudaStream_t s);
 
+// Finest-uniform dump of phi (double, gpd^3, zeroed first).
+template <typename Real>
+cudaError_t launch_uq_dump(const int *slot, const Real *origin, const Real *hblk, int nblocks, const Real *phi,
+                           int gpd, double *out, cudaStream_t s);
+
+struct LikelihoodParams {
+    double pet_sigma2, pet_scale, t1_uc, t2_uc, slope;
+    int step_pet, step_mri;
+};
+
+// out[0..3] = L_PET, L_T1c, L_FLAIR, their sum; partial holds nparts * 7 doubles.
+cudaError_t launch_likelihood(const double *model, int n, const unsigned char *t1c, const unsigned char *flair,
+                              const double *pet, const int *roi, int nroi, const LikelihoodParams &p,
+                              double *partial, int nparts, double *out, cudaStream_t s);
+
 template <typename Real>
 cudaError_t launch_dense_scatter(const Real *dense, Real *pool, int n, bool to_pool, cudaStream_t s);
 

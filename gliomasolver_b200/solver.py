@@ -169,6 +169,31 @@ class BlockPool:
         self._check(self.lib.gbfk_collapse(self.ctx, p.size, _ptr(c), _ptr(p)))
 
 
+    # -- UQ -----------------------------------------------------------------
+    def uq_dump(self, n: int) -> np.ndarray:
+        """phi on the n^3 grid of the initial resolution (_dumpUQoutput)."""
+        out = np.empty((n, n, n), dtype=np.float64)
+        self._check(self.lib.gbfk_uq_dump(self.ctx, int(n), _ptr(out)))
+        return out
+
+    def set_observations(self, t1c, flair, pet=None, roi=None):
+        t1 = np.ascontiguousarray(t1c, dtype=np.float64)
+        fl = np.ascontiguousarray(flair, dtype=np.float64)
+        pe = None if pet is None else np.ascontiguousarray(pet, dtype=np.float64)
+        ro = None if roi is None else np.ascontiguousarray(roi, dtype=np.int32).reshape(-1, 3)
+        self._check(self.lib.gbfk_set_observations(
+            self.ctx, t1.shape[0], _ptr(t1), _ptr(fl), None if pe is None else _ptr(pe),
+            None if ro is None else _ptr(ro), 0 if ro is None else ro.shape[0]))
+
+    def log_likelihood(self, pet_sigma2=0.000361, pet_scale=0.85, t1_uc=0.7, t2_uc=0.25, slope=2.0, step_pet=1,
+                       step_mri=1) -> np.ndarray:
+        """[L_PET, L_T1c, L_FLAIR, sum] of the current phi (HGG_Likelihood::run)."""
+        p = _lib.LikelihoodParams(pet_sigma2, pet_scale, t1_uc, t2_uc, slope, step_pet, step_mri)
+        out = np.empty(4, dtype=np.float64)
+        self._check(self.lib.gbfk_log_likelihood(self.ctx, ctypes.byref(p), _ptr(out)))
+        return out
+
+
 # ---------------------------------------------------------------- operators
 class ReactionDiffusionOperator:
     """Tag for ReactionDiffusionOperator<3> (ReactionDiffusionOperator.h:21-43):

@@ -156,6 +156,30 @@ int gbfk_split(gbfk_ctx *ctx, int nsplit, const int *parents, const int *childre
  * 22-84).  children[8*i + c] as for gbfk_split; parents[i] is a slot. */
 int gbfk_collapse(gbfk_ctx *ctx, int ncollapse, const int *children, const int *parents);
 
+/* --- UQ: finest-uniform dump and likelihood ---------------------------- */
+/* Parameters of the likelihood (LikelihoodInput.txt and the -stepPET /
+ * -stepMRI flags of tools/pi4u_lite/Inference/Likelihood/source/HGG_Likelihood.cpp:11-36). */
+typedef struct {
+    double pet_sigma2, pet_scale; /* PET Gaussian: variance, signal scale */
+    double t1_uc, t2_uc, slope;   /* T1c / FLAIR thresholds, sigmoid slope */
+    int step_pet, step_mri;       /* sub-sampling steps */
+} gbfk_likelihood_params;
+/* Observations on the n^3 dump grid (x fastest): T1c and FLAIR masks (a voxel
+ * counts as 1 where the value equals 1), the PET signal (NULL: no PET term),
+ * and the ROI voxel list of -bROI 1 (nroi (x,y,z) triples; NULL: every voxel;
+ * HGG_Likelihood.cpp:97-124). */
+int gbfk_set_observations(gbfk_ctx *ctx, int n, const double *t1c, const double *flair, const double *pet,
+                          const int *roi, int nroi);
+/* Glioma_ReactionDiffusion::_dumpUQoutput (Glioma_ReactionDiffusion.cpp:208-262):
+ * phi written onto the n^3 grid of the initial resolution (n = 8 * initial
+ * blocks per direction), as doubles, x fastest, to host memory. */
+int gbfk_uq_dump(gbfk_ctx *ctx, int n, double *host_out);
+/* The log-likelihood of the current phi against the observations
+ * (HGG_Likelihood::run, HGG_Likelihood.cpp:176-192): out[0] = PET,
+ * out[1] = T1c, out[2] = FLAIR, out[3] = their sum (the reference writes
+ * -out[3] to Likelihood.txt).  Sums are FP64 with compensation. */
+int gbfk_log_likelihood(gbfk_ctx *ctx, const gbfk_likelihood_params *params, double out[4]);
+
 /* --- allocation-free step -------------------------------------------- */
 /* No counterpart in the reference.  One fused RD step (the operator and the
  * update of gbfk_rd_step) on a uniform periodic bpd^3 grid, for callers that

@@ -71,6 +71,9 @@ def _declare(L):
     L.orc_split_block_f32.argtypes = [P, P, P]
     L.orc_collapse_blocks_f64.argtypes = [P, P]
     L.orc_collapse_blocks_f32.argtypes = [P, P]
+    L.orc_uq_dump_f64.argtypes = [I, P, P, P, P, I, P]
+    L.orc_uq_dump_f32.argtypes = [I, P, P, P, P, I, P]
+    L.orc_log_likelihood.argtypes = [I, P, P, P, P, P, I, D, D, D, D, D, I, I, P]
 
 
 def _p(a: np.ndarray):
@@ -146,6 +149,32 @@ def collapse_blocks(children):
     return out
 
 
+def uq_dump(levels, indices, h, phi_pool, gpd):
+    """_dumpUQoutput of blocks (level, index (3,), h in Real) with phi in block order."""
+    R = phi_pool.dtype.type
+    lv = np.ascontiguousarray(levels, dtype=np.int32)
+    ix = np.ascontiguousarray(indices, dtype=np.int32).reshape(-1)
+    hh = np.ascontiguousarray(h, dtype=R)
+    out = np.empty((gpd, gpd, gpd), dtype=np.float64)
+    getattr(lib(), "orc_uq_dump_" + _sfx(R))(lv.size, _p(lv), _p(ix), _p(hh),
+                                              _p(np.ascontiguousarray(phi_pool)), gpd, _p(out))
+    return out
+
+
+def log_likelihood(model, t1c, flair, pet=None, roi=None, pet_sigma2=0.000361, pet_scale=0.85, t1_uc=0.7,
+                   t2_uc=0.25, slope=2.0, step_pet=1, step_mri=1):
+    """HGG_Likelihood in long double; returns [L_PET, L_T1c, L_FLAIR] as float64."""
+    n = model.shape[0]
+    out = (ctypes.c_longdouble * 3)()
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (model, t1c, flair)]
+    pe = None if pet is None else np.ascontiguousarray(pet, dtype=np.float64)
+    ro = None if roi is None else np.ascontiguousarray(roi, dtype=np.int32).reshape(-1)
+    lib().orc_log_likelihood(n, _p(a[0]), _p(a[1]), _p(a[2]), None if pe is None else _p(pe),
+                             None if ro is None else _p(ro), 0 if ro is None else ro.size // 3,
+                             pet_sigma2, pet_scale, t1_uc, t2_uc, slope, step_pet, step_mri, out)
+    return np.array([float(out[0]), float(out[1]), float(out[2])])
+
+
 # ------------------------------------------------- the reference's own code
 def ref_available(precision: str = "f64") -> bool:
     return (REF_DIR / f"ref_harness_{precision}").exists()
@@ -201,3 +230,43 @@ def ref_time(pw, pg, phi, Dw, Dg, rho, dt, nsteps, precision="f32", threads=None
                             _fmt(Dw), _fmt(Dg), _fmt(rho), _fmt(dt), str(int(nsteps)), str(int(warmup))],
                            check=True, env=env, capture_output=True, text=True)
         return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def write_matrix3d(path, a):
+    """The reference's Matrix .dat layout (Glioma/Matrix.h:609-631):
+    int32 {1234, 3, nx, ny, nz}, int32 type id (0 = double), data x fastest."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    nz, ny, nx = a.shape
+    with open(path, "wb") as f:
+        f.write(np.array([1234, 3, nx, ny, nz, 0], dtype=np.int32).tobytes())
+        f.write(a.tobytes())
+
+
+def write_matrix2d(path, points):
+    """Matrix::D2D layout with nx = number of points and ny = 3, so that
+    element (i, j) = coordinate j of point i (HGG_Likelihood.cpp:108-115)."""
+    a = np.ascontiguousarray(points, dtype=np.float64)
+    npts, ncoord = a.shape
+    with open(path, "wb") as f:
+        f.write(np.array([1234, 2, npts, ncoord, 0], dtype=np.int32).tobytes())
+        f.write(np.ascontiguousarray(a.T).tobytes())
+
+
+def ref_likelihood(model, t1c, flair, pet, roi=None, pet_sigma2=0.000361, pet_scale=0.85, t1_uc=0.7, t2_uc=0.25,
+                   slope=2.0, step_pet=1, step_mri=1):
+    """Run the reference's likelihood program; returns -log-likelihood as
+    written to Likelihood.txt (printed with %Lf, 6 decimals) and its stdout."""
+    exe = REF_DIR / "likelihood"
+    with tempfile.TemporaryDirectory() as td:
+        write_matrix3d(os.path.join(td, "HGG_data.dat"), model)
+        write_matrix3d(os.path.join(td, "tumT1c.dat"), t1c)
+        write_matrix3d(os.path.join(td, "tumFLAIR.dat"), flair)
+        write_matrix3d(os.path.join(td, "tumPET.dat"), pet)
+        if roi is not None:
+            write_matrix2d(os.path.join(td, "ROI.dat"), np.asarray(roi, dtype=np.float64).reshape(-1, 3))
+        with open(os.path.join(td, "LikelihoodInput.txt"), "w") as f:
+            f.write(f"{pet_sigma2!r}\n{pet_scale!r}\n{t1_uc!r}\n{t2_uc!r}\n{slope!r}\n")
+        args = [str(exe), "-stepPET", str(step_pet), "-stepMRI", str(step_mri), "-bROI", "1" if roi is not None else "0"]
+        r = subprocess.run(args, cwd=td, check=True, capture_output=True, text=True)
+        with open(os.path.join(td, "Likelihood.txt")) as f:
+            return float(f.read().split()[0]), r.stdout

@@ -317,3 +317,98 @@ DEFINE_FWT(f32, float)
 
 DEFINE_SPLIT(f64, double)
 DEFINE_SPLIT(f32, float)
+
+/* ------------------------------------------------------------------------ */
+/* _dumpUQoutput (Glioma_ReactionDiffusion.cpp:208-262). */
+#define DEFINE_UQ_DUMP(SFX, REAL)                                                       \
+    void orc_uq_dump_##SFX(int nblocks, const int *level, const int *index, const REAL *h, \
+                           const REAL *phi, int gpd, double *out)                        \
+    {                                                                                   \
+        const double hf = 1. / gpd;                                                     \
+        const double eps = hf * 0.5;                                                    \
+        memset(out, 0, sizeof(double) * (size_t)gpd * gpd * gpd);                       \
+        for (int b = 0; b < nblocks; b++) {                                             \
+            const double dilate = ldexp(1.0, -level[b]);                                \
+            const REAL origin[3] = {(REAL)(index[3 * b] * dilate), (REAL)(index[3 * b + 1] * dilate), \
+                                    (REAL)(index[3 * b + 2] * dilate)};                 \
+            const REAL hb = h[b];                                                       \
+            const double hd = hb;                                                       \
+            for (int iz = 0; iz < BS; iz++)                                             \
+                for (int iy = 0; iy < BS; iy++)                                         \
+                    for (int ix = 0; ix < BS; ix++) {                                   \
+                        const double x0 = origin[0] + hb * ix;                          \
+                        const double x1 = origin[1] + hb * iy;                          \
+                        const double x2 = origin[2] + hb * iz;                          \
+                        const int mx = (int)floor(x0 / hf), my = (int)floor(x1 / hf),   \
+                                  mz = (int)floor(x2 / hf);                              \
+                        const double v = phi[(int64_t)b * BS3 + ix + BS * (iy + BS * iz)]; \
+                        int c;                                                          \
+                        if (hd < hf + eps) c = 1;                                       \
+                        else if (hd < 2. * hf + eps) c = 2;                             \
+                        else if (hd < 3. * hf + eps) c = 3;                             \
+                        else c = 4;                                                     \
+                        for (int cz = 0; cz < c; cz++)                                  \
+                            for (int cy = 0; cy < c; cy++)                              \
+                                for (int cx = 0; cx < c; cx++)                          \
+                                    out[(mx + cx) + (size_t)gpd * ((my + cy) + (size_t)gpd * (mz + cz))] = v; \
+                    }                                                                   \
+        }                                                                               \
+    }
+
+DEFINE_UQ_DUMP(f64, double)
+DEFINE_UQ_DUMP(f32, float)
+
+/* HGG_Likelihood::_computeLogBernoulli (HGG_Likelihood.cpp:136-163). */
+static long double log_bernoulli(double u, double y, double uc, double slope)
+{
+    const double is2 = 1. / slope;
+    const double diff = u - uc;
+    const long double omega2 = (diff > 0.) ? 1. : diff * diff;
+    const int sgn = (diff < -0.0) ? -1 : (diff > 0.0);
+    const long double alpha = 0.5 + 0.5 * sgn * (1. - expl(-omega2 * is2));
+    return (y == 1) ? logl(alpha) : logl(1. - alpha);
+}
+
+void orc_log_likelihood(int n, const double *model, const double *t1c, const double *flair, const double *pet,
+                        const int *roi, int nroi, double pet_sigma2, double pet_scale, double t1uc,
+                        double t2uc, double slope, int step_pet, int step_mri, long double out[3])
+{
+    /* PET (HGG_Likelihood.cpp:40-75) */
+    out[0] = 0;
+    if (pet) {
+        int N = 0;
+        long double sum = 0.;
+        for (int iz = 0; iz < n; iz++)
+            for (int iy = 0; iy < n; iy++)
+                for (int ix = 0; ix < n; ix++) {
+                    if ((ix % step_pet == 0) && (iy % step_pet == 0) && (iz % step_pet == 0)) {
+                        const size_t g = ix + (size_t)n * (iy + (size_t)n * iz);
+                        if (pet[g] > 0.) {
+                            sum += (model[g] - pet_scale * pet[g]) * (model[g] - pet_scale * pet[g]);
+                            N++;
+                        }
+                    }
+                }
+        const long double p1 = -0.5 * N * log(2. * M_PI * pet_sigma2);
+        const long double p2 = -0.5 * (1. / pet_sigma2) * sum;
+        out[0] = p1 + p2;
+    }
+    /* T1c, FLAIR (:77-128) */
+    for (int ti = 1; ti <= 2; ti++) {
+        const double *data = ti == 1 ? t1c : flair;
+        const double uc = ti == 1 ? t1uc : t2uc;
+        long double sum = 0.;
+        if (!roi) {
+            for (size_t g = 0; g < (size_t)n * n * n; g++) sum += log_bernoulli(model[g], data[g], uc, slope);
+        } else {
+            for (int i = 0; i < nroi; i++) {
+                const int ix = roi[3 * i], iy = roi[3 * i + 1], iz = roi[3 * i + 2];
+                if ((ix % step_mri == 0) && (iy % step_mri == 0) && (iz % step_mri == 0)) {
+                    const size_t g = ix + (size_t)n * (iy + (size_t)n * iz);
+                    sum += log_bernoulli(model[g], data[g], uc, slope);
+                }
+            }
+        }
+        out[ti] = sum;
+    }
+}

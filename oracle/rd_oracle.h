@@ -96,6 +96,26 @@ void orc_split_block_f32(const float *parent, const float *gparent, float *child
 void orc_collapse_blocks_f64(const double *children, double *parent);
 void orc_collapse_blocks_f32(const float *children, float *parent);
 
+/* _dumpUQoutput (Glioma/Glioma_ReactionDiffusion.cpp:208-262): phi of every
+ * block written onto the gpd^3 grid of the initial resolution, x fastest.
+ * Block b has level[b], index[3*b..], spacing h[b] (Real); cells at
+ * x = origin + h*i with origin = index * 2^-level.  Cells of blocks as fine
+ * as the dump grid or finer write their voxel (the last cell in loop order
+ * wins); coarser blocks write c^3 copies, c = 2, 3 or 4 by h (as the
+ * reference).  out must hold gpd^3 doubles and is zeroed first. */
+void orc_uq_dump_f64(int nblocks, const int *level, const int *index, const double *h, const double *phi,
+                     int gpd, double *out);
+void orc_uq_dump_f32(int nblocks, const int *level, const int *index, const float *h, const float *phi,
+                     int gpd, double *out);
+
+/* HGG_Likelihood (tools/pi4u_lite/Inference/Likelihood/source/HGG_Likelihood.cpp:
+ * 40-156) in long double: out[0] = PET log-likelihood (or 0 if pet is NULL),
+ * out[1] = T1c, out[2] = FLAIR; roi (npoints triples) selects voxels for the
+ * MRI terms (-bROI 1), NULL = every voxel. */
+void orc_log_likelihood(int n, const double *model, const double *t1c, const double *flair, const double *pet,
+                        const int *roi, int nroi, double pet_sigma2, double pet_scale, double t1uc,
+                        double t2uc, double slope, int step_pet, int step_mri, long double out[3]);
+
 #ifdef __cplusplus
 }
 #endif
