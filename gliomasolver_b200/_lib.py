@@ -34,6 +34,9 @@ EXPORTS = (
     "gbfk_rd_step", "gbfk_rd_rhs", "gbfk_fwt_details", "gbfk_split", "gbfk_collapse",
     "gbfk_rd_step_static",
     "gbfk_set_observations", "gbfk_uq_dump", "gbfk_log_likelihood",
+    "gbfk_batch_create", "gbfk_batch_destroy", "gbfk_batch_last_error", "gbfk_batch_launch_count",
+    "gbfk_batch_set_anatomy", "gbfk_batch_set_samples", "gbfk_batch_run", "gbfk_batch_samples_per_cta",
+    "gbfk_batch_download",
 )
 
 
@@ -70,6 +73,19 @@ class LikelihoodParams(ctypes.Structure):
         ("slope", ctypes.c_double),
         ("step_pet", ctypes.c_int),
         ("step_mri", ctypes.c_int),
+    ]
+
+
+class Sample(ctypes.Structure):
+    _fields_ = [
+        ("Dw", ctypes.c_double),
+        ("Dg", ctypes.c_double),
+        ("rho", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("nsteps", ctypes.c_int),
+        ("anatomy", ctypes.c_int),
+        ("x0", ctypes.c_double * 3),
+        ("sigma", ctypes.c_double),
     ]
 
 
@@ -121,6 +137,15 @@ def load(path: Path | str | None = None):
         "gbfk_set_observations": (I, [P, I, P, P, P, P, I]),
         "gbfk_uq_dump": (I, [P, I, P]),
         "gbfk_log_likelihood": (I, [P, ctypes.POINTER(LikelihoodParams), P]),
+        "gbfk_batch_create": (I, [ctypes.POINTER(Config), I, I, I, ctypes.POINTER(P)]),
+        "gbfk_batch_destroy": (I, [P]),
+        "gbfk_batch_last_error": (ctypes.c_char_p, [P]),
+        "gbfk_batch_launch_count": (I64, [P]),
+        "gbfk_batch_set_anatomy": (I, [P, I, P, P]),
+        "gbfk_batch_set_samples": (I, [P, I, ctypes.POINTER(Sample)]),
+        "gbfk_batch_run": (I, [P, I]),
+        "gbfk_batch_samples_per_cta": (I, [P]),
+        "gbfk_batch_download": (I, [P, I, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1,0 +1,411 @@
+// Batched TMCMC-stage forward solves.
+//
+// The reference evaluates a TMCMC stage as independent tasks
+// (tools/pi4u_lite/Inference/engine_tmcmc.c:597-624), each forking a process
+// that runs the whole solver on one parameter sample
+// (tools/pi4u_lite/Inference/fitfun_glioma.c:46-245, runAll.sh: brain -UQ 1).
+// Here all samples of a stage live in GPU memory and advance together: one
+// launch per time step covers every sample that has not reached its own
+// horizon.  Samples are sorted by step count (longest first), so the active
+// samples of step k are a prefix and retired samples cost nothing.
+#include "gbfk.h"
+#include "gbfk_exact.cuh"
+#include "gbfk_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <numeric>
+#include <string>
+#include <vector>
+
+using namespace gbfk;
+
+namespace gbfk {
+cudaError_t upload_ghost_table();
+}
+
+struct gbfk_batch {
+    int precision = GBFK_F32;
+    size_t rsize = 4;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int bpd = 0, n = 0, nblocks = 0;
+    int max_samples = 0, max_anatomies = 0;
+    int log2_bpd = -1;
+    int *d_nbr = nullptr;
+    double *d_ih2 = nullptr;
+    // per anatomy
+    std::vector<void *> pw, pg;
+    std::vector<unsigned short *> meta;
+    std::vector<unsigned char *> btype;
+    std::vector<bool> anatomy_set;
+    // per sample (in the caller's order)
+    int nsamples = 0;
+    std::vector<gbfk_sample> params;
+    std::vector<void *> phi0, phi1, H;
+    std::vector<int> order;  // position -> caller's sample index (longest horizon first)
+    void *d_views = nullptr;
+    unsigned *d_nan = nullptr;
+    double *d_scratch_h = nullptr;  // unused placeholder for alignment of future scratch
+    int chosen_spc = 0;
+    int64_t launches = 0;
+    std::string err;
+};
+
+namespace {
+
+int bfail(gbfk_batch *b, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (b) b->err = buf;
+    return code;
+}
+
+#define BK(call)                                                                                          \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess)                                                                            \
+            return bfail(b, e_ == cudaErrorMemoryAllocation ? GBFK_E_OOM : GBFK_E_CUDA, "%s: %s (%s:%d)", \
+                         #call, cudaGetErrorString(e_), __FILE__, __LINE__);                              \
+    } while (0)
+
+template <typename Real>
+PoolView<Real> batch_pool(gbfk_batch *b)
+{
+    PoolView<Real> v;
+    v.slot = nullptr;
+    v.nbr = b->d_nbr;
+    v.hblk = nullptr;
+    v.gpw = v.gpg = v.gphi = nullptr;
+    v.pw = v.pg = nullptr;
+    v.btype = nullptr;
+    v.nblocks = b->nblocks;
+    v.identity_slots = 1;
+    v.log2_bpd = b->log2_bpd;
+    return v;
+}
+
+// Tumour initial condition of a sample on the device: c0 = exp(-|x-x0|^2 /
+// (2 sigma^2)) where p_w + p_g > 0, else 0, in Real, at vertex positions
+// x = i / n (MRAG BlockInfo::pos); block-pool order.
+template <typename Real>
+__global__ void ic_kernel(int n, int bpd, const Real *__restrict__ pw, const Real *__restrict__ pg, double x0,
+                          double y0, double z0, double sigma, Real *__restrict__ out)
+{
+    const int64_t N = (int64_t)n * n * n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = i >> 9;
+        const int c = (int)(i & 511);
+        const int bx = (int)(b % bpd), by = (int)((b / bpd) % bpd), bz = (int)(b / ((int64_t)bpd * bpd));
+        const double x = (double)(bx * 8 + (c & 7)) / n, y = (double)(by * 8 + ((c >> 3) & 7)) / n,
+                     z = (double)(bz * 8 + (c >> 6)) / n;
+        const double r2 = (x - x0) * (x - x0) + (y - y0) * (y - y0) + (z - z0) * (z - z0);
+        const double v = exp(-r2 / (2. * sigma * sigma));
+        out[i] = (pw[i] + pg[i] > (Real)0) ? (Real)v : (Real)0;
+    }
+}
+
+template <typename Real>
+int batch_prepare(gbfk_batch *b)
+{
+    // face coefficients and meta words of every sample's (anatomy, Dw, Dg)
+    for (int s = 0; s < b->nsamples; s++) {
+        const gbfk_sample &p = b->params[s];
+        PoolView<Real> v = batch_pool<Real>(b);
+        v.pw = (const Real *)b->pw[p.anatomy];
+        v.pg = (const Real *)b->pg[p.anatomy];
+        v.btype = b->btype[p.anatomy];
+        BK(launch_faces<Real>(v, (Real)p.Dw, (Real)p.Dg, (Real *)b->H[s], b->meta[p.anatomy], b->btype[p.anatomy],
+                              b->stream));
+        int64_t nb = ((int64_t)b->nblocks * kBS3 + 255) / 256;
+        if (nb > 148 * 32) nb = 148 * 32;
+        ic_kernel<Real><<<(int)nb, 256, 0, b->stream>>>(b->n, b->bpd, v.pw, v.pg, p.x0[0], p.x0[1], p.x0[2],
+                                                         p.sigma, (Real *)b->phi0[s]);
+        BK(cudaGetLastError());
+        b->launches += 2;
+    }
+    // views sorted by horizon
+    b->order.resize(b->nsamples);
+    std::iota(b->order.begin(), b->order.end(), 0);
+    std::stable_sort(b->order.begin(), b->order.end(),
+                     [&](int i, int j) { return b->params[i].nsteps > b->params[j].nsteps; });
+    std::vector<SampleView<Real>> views(b->nsamples);
+    for (int k = 0; k < b->nsamples; k++) {
+        const int s = b->order[k];
+        const gbfk_sample &p = b->params[s];
+        SampleView<Real> &sv = views[k];
+        sv.pw = (const Real *)b->pw[p.anatomy];
+        sv.pg = (const Real *)b->pg[p.anatomy];
+        sv.btype = b->btype[p.anatomy];
+        sv.meta = b->meta[p.anatomy];
+        sv.H = (const Real *)b->H[s];
+        sv.phi0 = (Real *)b->phi0[s];
+        sv.phi1 = (Real *)b->phi1[s];
+        sv.rho = (Real)p.rho;
+        sv.dt = p.dt;
+        sv.nsteps = p.nsteps;
+    }
+    BK(cudaMemcpyAsync(b->d_views, views.data(), views.size() * sizeof(SampleView<Real>), cudaMemcpyHostToDevice,
+                       b->stream));
+    BK(cudaMemsetAsync(b->d_nan, 0, b->max_samples * sizeof(unsigned), b->stream));
+    BK(cudaStreamSynchronize(b->stream));
+    return GBFK_OK;
+}
+
+template <typename Real>
+int batch_run(gbfk_batch *b, int spc)
+{
+    int rc = batch_prepare<Real>(b);
+    if (rc) return rc;
+    BatchView<Real> bv;
+    bv.pool = batch_pool<Real>(b);
+    bv.samples = (const SampleView<Real> *)b->d_views;
+    bv.ih2 = b->d_ih2;
+    bv.nan_flags = b->d_nan;
+    const int maxsteps = b->nsamples ? b->params[b->order[0]].nsteps : 0;
+    // active samples of step k: a prefix of the sorted list
+    std::vector<int> sorted_steps(b->nsamples);
+    for (int k = 0; k < b->nsamples; k++) sorted_steps[k] = b->params[b->order[k]].nsteps;
+    int nactive = b->nsamples;
+    auto active_at = [&](int step) {
+        while (nactive > 0 && sorted_steps[nactive - 1] <= step) nactive--;
+        return nactive;
+    };
+    int step = 0;
+    // autotuner: samples per CTA in {1, 2, 4}, timed on real steps (the
+    // results do not depend on the choice), 3 steps each after 1 warm-up
+    if (spc == 0) {
+        const int cands[3] = {1, 2, 4};
+        float best = 1e30f;
+        int best_spc = 1;
+        cudaEvent_t e0, e1;
+        BK(cudaEventCreate(&e0));
+        BK(cudaEventCreate(&e1));
+        for (int ci = 0; ci < 3 && step + 4 <= maxsteps; ci++) {
+            BK(launch_rd_batch_step<Real>(bv, active_at(step), step, cands[ci], b->stream));
+            step++;
+            BK(cudaEventRecord(e0, b->stream));
+            for (int r = 0; r < 3; r++, step++) BK(launch_rd_batch_step<Real>(bv, active_at(step), step, cands[ci], b->stream));
+            BK(cudaEventRecord(e1, b->stream));
+            BK(cudaEventSynchronize(e1));
+            float ms = 0;
+            BK(cudaEventElapsedTime(&ms, e0, e1));
+            b->launches += 4;
+            if (ms < best) {
+                best = ms;
+                best_spc = cands[ci];
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        spc = best_spc;
+    }
+    b->chosen_spc = spc;
+    for (; step < maxsteps; step++) {
+        BK(launch_rd_batch_step<Real>(bv, active_at(step), step, spc, b->stream));
+        b->launches++;
+    }
+    BK(cudaStreamSynchronize(b->stream));
+    std::vector<unsigned> flags(b->nsamples);
+    BK(cudaMemcpy(flags.data(), b->d_nan, b->nsamples * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < b->nsamples; k++)
+        if (flags[k]) return bfail(b, GBFK_E_NAN, "sample %d became NaN", b->order[k]);
+    return GBFK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gbfk_batch_create(const gbfk_config *cfg, int bpd, int max_samples, int max_anatomies, gbfk_batch **out)
+{
+    if (!cfg || !out || bpd <= 0 || max_samples <= 0 || max_anatomies <= 0) return GBFK_E_INVALID;
+    if (cfg->precision != GBFK_F64 && cfg->precision != GBFK_F32) return GBFK_E_INVALID;
+    *out = nullptr;
+    gbfk_batch *b = new gbfk_batch();
+    b->precision = cfg->precision;
+    b->rsize = cfg->precision == GBFK_F64 ? 8 : 4;
+    b->device = cfg->device;
+    b->bpd = bpd;
+    b->n = 8 * bpd;
+    b->nblocks = bpd * bpd * bpd;
+    b->max_samples = max_samples;
+    b->max_anatomies = max_anatomies;
+    auto bail = [&](int rc) {
+        gbfk_batch_destroy(b);
+        return rc;
+    };
+    if (cudaSetDevice(cfg->device) != cudaSuccess) return bail(GBFK_E_CUDA);
+    if (upload_ghost_table() != cudaSuccess) return bail(GBFK_E_CUDA);
+    if (cfg->stream) b->stream = (cudaStream_t)cfg->stream;
+    else {
+        if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GBFK_E_CUDA);
+        b->own_stream = true;
+    }
+    if ((bpd & (bpd - 1)) == 0) {
+        int L = 0;
+        while ((1 << L) < bpd) L++;
+        b->log2_bpd = L;
+    }
+    const int nb = b->nblocks;
+    std::vector<int> nbr((size_t)nb * 6);
+    for (int bz = 0; bz < bpd; bz++)
+        for (int by = 0; by < bpd; by++)
+            for (int bx = 0; bx < bpd; bx++) {
+                auto id = [&](int x, int y, int z) {
+                    x = (x + bpd) % bpd; y = (y + bpd) % bpd; z = (z + bpd) % bpd;
+                    return x + bpd * (y + bpd * z);
+                };
+                int *q = &nbr[(size_t)(bx + bpd * (by + bpd * bz)) * 6];
+                q[0] = id(bx - 1, by, bz); q[1] = id(bx + 1, by, bz);
+                q[2] = id(bx, by - 1, bz); q[3] = id(bx, by + 1, bz);
+                q[4] = id(bx, by, bz - 1); q[5] = id(bx, by, bz + 1);
+            }
+    const double h = b->precision == GBFK_F64 ? 1.0 / (8.0 * bpd) : (double)(float)(1.0 / (8.0 * bpd));
+    std::vector<double> ih2(nb, 1. / (h * h));
+    const size_t field = (size_t)nb * kBS3 * b->rsize;
+    if (cudaMalloc(&b->d_nbr, nbr.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_ih2, nb * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&b->d_views, (size_t)max_samples * sizeof(SampleView<double>)) != cudaSuccess ||
+        cudaMalloc(&b->d_nan, (size_t)max_samples * sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(GBFK_E_OOM);
+    }
+    cudaMemcpy(b->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->d_ih2, ih2.data(), nb * sizeof(double), cudaMemcpyHostToDevice);
+    b->pw.assign(max_anatomies, nullptr);
+    b->pg.assign(max_anatomies, nullptr);
+    b->meta.assign(max_anatomies, nullptr);
+    b->btype.assign(max_anatomies, nullptr);
+    b->anatomy_set.assign(max_anatomies, false);
+    for (int a = 0; a < max_anatomies; a++) {
+        if (cudaMalloc(&b->pw[a], field) != cudaSuccess || cudaMalloc(&b->pg[a], field) != cudaSuccess ||
+            cudaMalloc(&b->meta[a], (size_t)nb * kBS3 * sizeof(unsigned short)) != cudaSuccess ||
+            cudaMalloc(&b->btype[a], (size_t)nb) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(GBFK_E_OOM);
+        }
+    }
+    b->phi0.assign(max_samples, nullptr);
+    b->phi1.assign(max_samples, nullptr);
+    b->H.assign(max_samples, nullptr);
+    for (int s = 0; s < max_samples; s++) {
+        if (cudaMalloc(&b->phi0[s], field) != cudaSuccess || cudaMalloc(&b->phi1[s], field) != cudaSuccess ||
+            cudaMalloc(&b->H[s], (size_t)nb * kFacesPerBlock * b->rsize) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(GBFK_E_OOM);
+        }
+    }
+    *out = b;
+    return GBFK_OK;
+}
+
+int gbfk_batch_destroy(gbfk_batch *b)
+{
+    if (!b) return GBFK_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto *v : {&b->pw, &b->pg, &b->phi0, &b->phi1, &b->H})
+        for (void *p : *v)
+            if (p) cudaFree(p);
+    for (auto p : b->meta)
+        if (p) cudaFree(p);
+    for (auto p : b->btype)
+        if (p) cudaFree(p);
+    void *ptrs[] = {b->d_nbr, b->d_ih2, b->d_views, b->d_nan};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return GBFK_OK;
+}
+
+const char *gbfk_batch_last_error(const gbfk_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int64_t gbfk_batch_launch_count(const gbfk_batch *b) { return b ? b->launches : 0; }
+
+int gbfk_batch_set_anatomy(gbfk_batch *b, int anatomy, const void *pw_dense, const void *pg_dense)
+{
+    if (!b) return GBFK_E_INVALID;
+    if (anatomy < 0 || anatomy >= b->max_anatomies || !pw_dense || !pg_dense)
+        return bfail(b, GBFK_E_INVALID, "set_anatomy: bad anatomy index or null field");
+    BK(cudaSetDevice(b->device));
+    const size_t bytes = (size_t)b->n * b->n * b->n * b->rsize;
+    void *stage = nullptr;
+    BK(cudaMalloc(&stage, bytes));
+    const void *src[2] = {pw_dense, pg_dense};
+    void *dst[2] = {b->pw[anatomy], b->pg[anatomy]};
+    for (int f = 0; f < 2; f++) {
+        cudaError_t e = cudaMemcpyAsync(stage, src[f], bytes, cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess)
+            e = b->precision == GBFK_F64
+                    ? launch_dense_scatter<double>((const double *)stage, (double *)dst[f], b->n, true, b->stream)
+                    : launch_dense_scatter<float>((const float *)stage, (float *)dst[f], b->n, true, b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) {
+            cudaFree(stage);
+            BK(e);
+        }
+        b->launches++;
+    }
+    cudaFree(stage);
+    b->anatomy_set[anatomy] = true;
+    return GBFK_OK;
+}
+
+int gbfk_batch_set_samples(gbfk_batch *b, int nsamples, const gbfk_sample *samples)
+{
+    if (!b) return GBFK_E_INVALID;
+    if (nsamples < 0 || nsamples > b->max_samples || (nsamples && !samples))
+        return bfail(b, GBFK_E_INVALID, "set_samples: %d samples for %d slots", nsamples, b->max_samples);
+    for (int s = 0; s < nsamples; s++) {
+        const gbfk_sample &p = samples[s];
+        if (p.anatomy < 0 || p.anatomy >= b->max_anatomies || !b->anatomy_set[p.anatomy])
+            return bfail(b, GBFK_E_STATE, "sample %d: anatomy %d not set", s, p.anatomy);
+        if (p.nsteps < 0 || !(p.sigma > 0)) return bfail(b, GBFK_E_INVALID, "sample %d: bad nsteps or sigma", s);
+    }
+    b->nsamples = nsamples;
+    b->params.assign(samples, samples + nsamples);
+    return GBFK_OK;
+}
+
+int gbfk_batch_run(gbfk_batch *b, int samples_per_cta)
+{
+    if (!b) return GBFK_E_INVALID;
+    if (samples_per_cta != 0 && samples_per_cta != 1 && samples_per_cta != 2 && samples_per_cta != 4)
+        return bfail(b, GBFK_E_INVALID, "samples_per_cta must be 0 (autotune), 1, 2 or 4");
+    BK(cudaSetDevice(b->device));
+    return b->precision == GBFK_F64 ? batch_run<double>(b, samples_per_cta) : batch_run<float>(b, samples_per_cta);
+}
+
+int gbfk_batch_samples_per_cta(const gbfk_batch *b) { return b ? b->chosen_spc : 0; }
+
+int gbfk_batch_download(gbfk_batch *b, int sample, void *dense_out)
+{
+    if (!b) return GBFK_E_INVALID;
+    if (sample < 0 || sample >= b->nsamples || !dense_out) return bfail(b, GBFK_E_INVALID, "download: bad sample");
+    BK(cudaSetDevice(b->device));
+    const size_t bytes = (size_t)b->n * b->n * b->n * b->rsize;
+    void *stage = nullptr;
+    BK(cudaMalloc(&stage, bytes));
+    const void *src = (b->params[sample].nsteps & 1) ? b->phi1[sample] : b->phi0[sample];
+    cudaError_t e = b->precision == GBFK_F64
+                        ? launch_dense_scatter<double>((const double *)src, (double *)stage, b->n, false, b->stream)
+                        : launch_dense_scatter<float>((const float *)src, (float *)stage, b->n, false, b->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dense_out, stage, bytes, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    cudaFree(stage);
+    BK(e);
+    b->launches++;
+    return GBFK_OK;
+}
+
+}  // extern "C"

@@ -10,6 +10,13 @@ namespace gbfk {
 // -1 for the interior.  Filled by init_ghost_table() at library load.
 __constant__ short c_ghost_id[kLab3];
 
+// Pool slot of topology block blk.
+template <typename Real>
+__device__ __forceinline__ int64_t slot_of(const PoolView<Real> &v, int blk)
+{
+    return v.identity_slots ? (int64_t)blk : (int64_t)v.slot[blk];
+}
+
 __host__ __device__ inline int lab_index(int x, int y, int z)
 {
     return (x + 1) + kLab * ((y + 1) + kLab * (z + 1));
@@ -81,7 +88,7 @@ face_kernel(PoolView<Real> v, Real Dw, Real Dg, Real *__restrict__ H, unsigned s
     FaceSmem<Real> &S = *reinterpret_cast<FaceSmem<Real> *>(smem_raw);
     const int blk = blockIdx.x;
     const int t = threadIdx.x;
-    const int64_t base = (int64_t)v.slot[blk] * kBS3;
+    const int64_t base = slot_of(v, blk) * kBS3;
     for (int c = t; c < kBS3; c += 256) {
         const int l = lab_index(c & 7, (c >> 3) & 7, c >> 6);
         S.pw[l] = v.pw[base + c];
@@ -256,16 +263,18 @@ __device__ __forceinline__ int face_neighbour(const PoolView<Real> &v, int blk, 
 #define GBFK_STEP_MIN_BLOCKS_F64 5
 #endif
 
+// The step for one block `blk` (all 128 threads of the CTA call it together;
+// it synchronises the CTA).  v.pw/v.pg/v.btype and meta describe the anatomy,
+// H the face coefficients of the coefficient pair, phi_in/phi_out the field.
 template <typename Real, bool kWriteRhs>
-__global__ void __launch_bounds__(128, sizeof(Real) == 4 ? GBFK_STEP_MIN_BLOCKS_F32 : GBFK_STEP_MIN_BLOCKS_F64)
-rd_step_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
-               const double *__restrict__ ih2blk, const Real *__restrict__ phi_in, Real *__restrict__ phi_out,
-               Real *__restrict__ dphidt_out, Real rho, double dt, int dt_finite, unsigned *nan_flag)
+__device__ __forceinline__ void step_block(const PoolView<Real> &v, int blk, Real *__restrict__ ph,
+                                           const Real *__restrict__ H, const unsigned short *__restrict__ meta,
+                                           const double *__restrict__ ih2blk, const Real *__restrict__ phi_in,
+                                           Real *__restrict__ phi_out, Real *__restrict__ dphidt_out, Real rho,
+                                           double dt, int dt_finite, unsigned *nan_flag)
 {
-    __shared__ __align__(16) Real ph[kStepLab];
-    const int blk = blockIdx.x;
     const int t = threadIdx.x;
-    const int64_t base = (int64_t)(v.identity_slots ? blk : v.slot[blk]) * kBS3;
+    const int64_t base = slot_of(v, blk) * kBS3;
     const int x4 = (t & 1) * 4, y = (t >> 1) & 7, z = t >> 4;
     const int c0 = x4 + kBS * (y + kBS * z);
     const int l0 = lab_p(x4, y, z);
@@ -407,6 +416,60 @@ rd_step_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned shor
     if (!kWriteRhs && bad) atomicOr(nan_flag, 1u);
 }
 
+template <typename Real, bool kWriteRhs>
+__global__ void __launch_bounds__(128, sizeof(Real) == 4 ? GBFK_STEP_MIN_BLOCKS_F32 : GBFK_STEP_MIN_BLOCKS_F64)
+rd_step_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
+               const double *__restrict__ ih2blk, const Real *__restrict__ phi_in, Real *__restrict__ phi_out,
+               Real *__restrict__ dphidt_out, Real rho, double dt, int dt_finite, unsigned *nan_flag)
+{
+    __shared__ __align__(16) Real ph[kStepLab];
+    step_block<Real, kWriteRhs>(v, blockIdx.x, ph, H, meta, ih2blk, phi_in, phi_out, dphidt_out, rho, dt, dt_finite,
+                                nan_flag);
+}
+
+// Batched step: every sample of the batch has its own phi buffers, face
+// coefficients (its own Dw, Dg), rho and dt, and may have its own anatomy.
+// blockIdx.x = block, blockIdx.y = group of kSamples consecutive active
+// samples; a sample whose horizon is reached (step >= nsteps) is skipped.
+template <typename Real, int kSamples>
+__global__ void __launch_bounds__(128, sizeof(Real) == 4 ? GBFK_STEP_MIN_BLOCKS_F32 : GBFK_STEP_MIN_BLOCKS_F64)
+rd_batch_step_kernel(BatchView<Real> b, int nactive, int step)
+{
+    __shared__ __align__(16) Real ph[kStepLab];
+    const int blk = blockIdx.x;
+#pragma unroll 1
+    for (int k = 0; k < kSamples; k++) {
+        const int s = blockIdx.y * kSamples + k;
+        if (s >= nactive) return;
+        const SampleView<Real> &sv = b.samples[s];
+        if (step >= sv.nsteps) continue;
+        PoolView<Real> v = b.pool;
+        v.pw = sv.pw;
+        v.pg = sv.pg;
+        v.btype = sv.btype;
+        const int par = step & 1;
+        step_block<Real, false>(v, blk, ph, sv.H, sv.meta, b.ih2, par ? sv.phi1 : sv.phi0, par ? sv.phi0 : sv.phi1,
+                                nullptr, sv.rho, sv.dt, 1, b.nan_flags + s);
+        __syncthreads();
+    }
+}
+
+template <typename Real>
+cudaError_t launch_rd_batch_step(const BatchView<Real> &b, int nactive, int step, int samples_per_cta,
+                                 cudaStream_t s)
+{
+    if (nactive <= 0 || b.pool.nblocks <= 0) return cudaSuccess;
+    const int groups = (nactive + samples_per_cta - 1) / samples_per_cta;
+    const dim3 grid(b.pool.nblocks, groups);
+    switch (samples_per_cta) {
+    case 1: rd_batch_step_kernel<Real, 1><<<grid, 128, 0, s>>>(b, nactive, step); break;
+    case 2: rd_batch_step_kernel<Real, 2><<<grid, 128, 0, s>>>(b, nactive, step); break;
+    case 4: rd_batch_step_kernel<Real, 4><<<grid, 128, 0, s>>>(b, nactive, step); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 template <typename Real>
 cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigned short *meta, const double *ih2,
                            const Real *phi_in, Real *phi_out, Real *dphidt_out, Real rho, double dt,
@@ -487,7 +550,7 @@ __global__ void __launch_bounds__(256) fwt_details_kernel(PoolView<Real> v, cons
     __shared__ double det[7][64];
     __shared__ double codemax[7];
     const int blk = blockIdx.x, t = threadIdx.x;
-    const int64_t base = (int64_t)v.slot[blk] * kBS3;
+    const int64_t base = slot_of(v, blk) * kBS3;
     for (int c = t; c < kBS3; c += 256) lab[lab_index(c & 7, (c >> 3) & 7, c >> 6)] = phi[base + c];
     // ghosts on the + side only: lab range [0, 9)^3
     for (int q = t; q < 9 * 9 * 9; q += 256) {
@@ -542,7 +605,7 @@ __global__ void __launch_bounds__(256) split_kernel(PoolView<Real> v, const int 
     __shared__ Real lab[3][kLab3];
     const int i = blockIdx.x, t = threadIdx.x;
     const int pblk = parents[i];
-    const int64_t base = (int64_t)v.slot[pblk] * kBS3;
+    const int64_t base = slot_of(v, pblk) * kBS3;
     Real *fields[3] = {phi, pw, pg};
     const Real *ghosts[3] = {v.gphi, v.gpw, v.gpg};
     for (int f = 0; f < 3; f++) {
@@ -680,6 +743,7 @@ cudaError_t upload_ghost_table()
                                               unsigned *, cudaStream_t);                                      \
     template cudaError_t launch_faces<Real>(const PoolView<Real> &, Real, Real, Real *, unsigned short *,       \
                                             unsigned char *, cudaStream_t);                                   \
+    template cudaError_t launch_rd_batch_step<Real>(const BatchView<Real> &, int, int, int, cudaStream_t);      \
     template cudaError_t launch_fill_ghosts<Real>(const int *, int64_t, const int64_t *, const int *,         \
                                                   const Real *, const Real *, Real *, cudaStream_t);          \
     template cudaError_t launch_fwt_details<Real>(const PoolView<Real> &, const Real *, double *, cudaStream_t); \

@@ -38,6 +38,33 @@ struct PoolView {
 // are read (kBlockMixed).
 constexpr unsigned char kBlockEmpty = 0, kBlockTissue = 1, kBlockMixed = 2;
 
+// One sample of a batch (device pointers).
+template <typename Real>
+struct SampleView {
+    const Real *pw, *pg;           // anatomy (pool order)
+    const unsigned char *btype;    // block types of that anatomy
+    const unsigned short *meta;    // meta words of that anatomy
+    const Real *H;                 // face coefficients of (anatomy, Dw, Dg)
+    Real *phi0, *phi1;             // ping-pong fields; step k reads phi[k & 1]
+    Real rho;
+    double dt;
+    int nsteps;
+};
+
+// A batch: one uniform topology, per-sample views (sorted by horizon,
+// longest first, so the active samples of a step are a prefix).
+template <typename Real>
+struct BatchView {
+    PoolView<Real> pool;           // topology (slot/nbr/log2_bpd/identity) shared by the samples
+    const SampleView<Real> *samples;
+    const double *ih2;
+    unsigned *nan_flags;           // one per sample
+};
+
+template <typename Real>
+cudaError_t launch_rd_batch_step(const BatchView<Real> &b, int nactive, int step, int samples_per_cta,
+                                 cudaStream_t s);
+
 // Harmonic means of all faces of every block for (Dw, Dg): H[nblocks * 1728],
 // and the per-cell meta words (class + neighbour class masks, pool-indexed).
 template <typename Real>

@@ -156,6 +156,40 @@ int gbfk_split(gbfk_ctx *ctx, int nsplit, const int *parents, const int *childre
  * 22-84).  children[8*i + c] as for gbfk_split; parents[i] is a slot. */
 int gbfk_collapse(gbfk_ctx *ctx, int ncollapse, const int *children, const int *parents);
 
+/* --- batched TMCMC-stage forward solves --------------------------------- */
+/* The reference evaluates the samples of a TMCMC stage as independent tasks
+ * (tools/pi4u_lite/Inference/engine_tmcmc.c:597-624), each a separate solver
+ * process (tools/pi4u_lite/Inference/fitfun_glioma.c:46-245).  A batch keeps
+ * every sample of a stage in GPU memory and advances all samples that have
+ * not reached their own horizon with one launch per time step. */
+typedef struct gbfk_batch gbfk_batch;
+typedef struct {
+    double Dw, Dg, rho; /* rescaled Real coefficients, as for gbfk_rd_step */
+    double dt;          /* time step */
+    int nsteps;         /* steps to this sample's horizon */
+    int anatomy;        /* which anatomy (gbfk_batch_set_anatomy) */
+    double x0[3];       /* tumour origin in the unit cube */
+    double sigma;       /* initial condition: c0 = exp(-|x-x0|^2/(2 sigma^2)) where p_w+p_g > 0 */
+} gbfk_sample;
+/* A batch on a uniform periodic bpd^3 grid with room for max_samples samples
+ * and max_anatomies anatomies (2 phi buffers + face coefficients per sample). */
+int gbfk_batch_create(const gbfk_config *cfg, int bpd, int max_samples, int max_anatomies, gbfk_batch **out);
+int gbfk_batch_destroy(gbfk_batch *b);
+const char *gbfk_batch_last_error(const gbfk_batch *b);
+int64_t gbfk_batch_launch_count(const gbfk_batch *b);
+/* p_w, p_g of one anatomy: dense n^3 Real volumes (x fastest, n = 8*bpd). */
+int gbfk_batch_set_anatomy(gbfk_batch *b, int anatomy, const void *pw_dense, const void *pg_dense);
+int gbfk_batch_set_samples(gbfk_batch *b, int nsamples, const gbfk_sample *samples);
+/* Build every sample's initial condition and face coefficients, then run all
+ * samples to their horizons.  samples_per_cta: 1, 2 or 4 samples per CTA, or
+ * 0 to let the autotuner time the three on the first steps and keep the
+ * fastest (the results do not depend on it).  GBFK_E_NAN if a sample became NaN. */
+int gbfk_batch_run(gbfk_batch *b, int samples_per_cta);
+/* The samples-per-CTA the last run used. */
+int gbfk_batch_samples_per_cta(const gbfk_batch *b);
+/* phi of one sample after the run, dense n^3 Real. */
+int gbfk_batch_download(gbfk_batch *b, int sample, void *dense_out);
+
 /* --- UQ: finest-uniform dump and likelihood ---------------------------- */
 /* Parameters of the likelihood (LikelihoodInput.txt and the -stepPET /
  * -stepMRI flags of tools/pi4u_lite/Inference/Likelihood/source/HGG_Likelihood.cpp:11-36). */
