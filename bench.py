@@ -176,6 +176,70 @@ def reference_arm(args):
     return 0
 
 
+def batched_stage(args, stream, local, nsamples=512, bpd=16, seed=1):
+    """Config 3: a TMCMC stage of 512 forward solves on 128^3 (FP32, one
+    seeded anatomy, Dw log-U[0.02,0.3], rho log-U[0.002,0.2], T U[30,300] d,
+    x0 a white-matter voxel), batched vs the same 512 solves one after the
+    other through gbfk_rd_step on one BlockPool.  Returns the JSON record."""
+    import torch
+
+    from gliomasolver_b200 import BlockPool
+    from gliomasolver_b200.anatomy import make_anatomy, tumor_ic
+    from gliomasolver_b200.tmcmc import Batch, sample_stage, to_gbfk_samples
+
+    n = 8 * bpd
+    p_w, p_g, _ = make_anatomy(n, SEED)
+    pw32, pg32 = p_w.astype(np.float32), p_g.astype(np.float32)
+    stage = sample_stage(nsamples, p_w, seed=seed)
+    samples, scheds = to_gbfk_samples(stage, bpd, "f32", L_CM)
+    steps = np.array([sc.nsteps for sc in scheds])
+    cells = n ** 3
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    with Batch(bpd, nsamples, "f32", device=local, stream=stream.cuda_stream) as b:
+        b.set_anatomy(0, pw32, pg32)
+        b.set_samples(samples)
+        l0 = b.launches
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        b.run(0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_batch = e0.elapsed_time(e1) / 1e3
+        batch_launches = b.launches - l0
+        spc = b.samples_per_cta
+
+    with BlockPool(bpd ** 3, "f32", device=local, stream=stream.cuda_stream) as pool:
+        pool.set_uniform(bpd)
+        pool.upload_dense("p_w", pw32)
+        pool.upload_dense("p_g", pg32)
+        ics = [tumor_ic(n, st.x0, p_w, p_g).astype(np.float32) for st in stage]
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        for ic, sc in zip(ics, scheds):
+            pool.upload_dense("phi", ic)
+            pool.rd_step(sc.Dw, sc.Dg, sc.rho, sc.dt, sc.nsteps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_seq = e0.elapsed_time(e1) / 1e3
+
+    return {
+        "workload": f"{nsamples} TMCMC samples, {n}^3 uniform, FP32, one seeded anatomy; Dw log-U[0.02,0.3], "
+                    "rho log-U[0.002,0.2], T U[30,300] d, x0 in white matter",
+        "samples": nsamples, "steps_total": int(steps.sum()), "steps_min": int(steps.min()),
+        "steps_max": int(steps.max()),
+        "batched_s": t_batch, "batched_samples_per_s": nsamples / t_batch,
+        "batched_cell_updates_per_s": float(steps.sum()) * cells / t_batch,
+        "sequential_s": t_seq, "sequential_samples_per_s": nsamples / t_seq,
+        "speedup_vs_sequential": t_seq / t_batch,
+        "samples_per_cta": spc, "batched_launches": batch_launches,
+        "timing": "CUDA events on the stream: batched = face coefficients + initial conditions + all steps; "
+                  "sequential = per sample an H2D of c0, face coefficients and its steps",
+    }
+
+
 def gpu_arm(args):
     import torch
     import torch.distributed as dist
@@ -282,6 +346,10 @@ def gpu_arm(args):
            "steps": e2e_steps,
            "api": "BlockPool.upload_dense x3 + rd_step + gbfk_download_dense (pinned host buffers)"}
 
+    batch = None
+    if not args.no_batch:
+        batch = batched_stage(args, stream, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rec, kind, cores, n_s, st = cpu_reference_run(0, 2, CPU_SAMPLE_N, prec, target_s=15.0)
@@ -296,6 +364,7 @@ def gpu_arm(args):
             "vs_baseline": None, "dtype": prec, "data": "synthetic", "config": workload_config(n, prec),
             "parallelism": "replicas" if world > 1 else "single",
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+            "batched_stage": batch,
         }
         print(json.dumps(line), flush=True)
     pool.close()
@@ -314,6 +383,7 @@ def main():
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--n", type=int, default=N_GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched TMCMC-stage measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
