@@ -37,6 +37,7 @@ EXPORTS = (
     "gbfk_batch_create", "gbfk_batch_destroy", "gbfk_batch_last_error", "gbfk_batch_launch_count",
     "gbfk_batch_set_anatomy", "gbfk_batch_set_samples", "gbfk_batch_run", "gbfk_batch_samples_per_cta",
     "gbfk_batch_download",
+    "gbfk_forward_adjoint",
 )
 
 
@@ -86,6 +87,22 @@ class Sample(ctypes.Structure):
         ("anatomy", ctypes.c_int),
         ("x0", ctypes.c_double * 3),
         ("sigma", ctypes.c_double),
+    ]
+
+
+class AdjointParams(ctypes.Structure):
+    _fields_ = [
+        ("Dw", ctypes.c_double), ("Dg", ctypes.c_double), ("rho", ctypes.c_double), ("dt", ctypes.c_double),
+        ("nsteps", ctypes.c_int), ("nsnapshots", ctypes.c_int),
+        ("x0", ctypes.c_double * 3), ("sigma", ctypes.c_double),
+        ("t1_uc", ctypes.c_double), ("t2_uc", ctypes.c_double), ("slope", ctypes.c_double),
+    ]
+
+
+class AdjointResult(ctypes.Structure):
+    _fields_ = [
+        ("loss", ctypes.c_double), ("dDw", ctypes.c_double), ("drho", ctypes.c_double),
+        ("dx0", ctypes.c_double * 3), ("forward_steps", ctypes.c_int64), ("adjoint_steps", ctypes.c_int64),
     ]
 
 
@@ -146,6 +163,7 @@ def load(path: Path | str | None = None):
         "gbfk_batch_run": (I, [P, I]),
         "gbfk_batch_samples_per_cta": (I, [P]),
         "gbfk_batch_download": (I, [P, I, P]),
+        "gbfk_forward_adjoint": (I, [P, ctypes.POINTER(AdjointParams), ctypes.POINTER(AdjointResult), P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -944,3 +944,249 @@ int gbfk_log_likelihood(gbfk_ctx *ctx, const gbfk_likelihood_params *p, double o
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Forward + discrete adjoint with binomial checkpointing.
+namespace {
+
+template <typename Real>
+struct Adjoint {
+    gbfk_ctx *ctx;
+    PoolView<Real> v;
+    size_t fbytes;
+    Real *T0, *T1, *T2, *LAM, *MU;
+    unsigned char *FL;
+    std::vector<Real *> slots;
+    double *grad_acc;
+    Real rho;
+    double dt, Dw;
+    int64_t fsteps = 0, asteps = 0;
+    cudaError_t err = cudaSuccess;
+
+    void step(const Real *in, Real *out)
+    {
+        if (err != cudaSuccess) return;
+        err = launch_rd_step<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, in, out, nullptr, rho, dt,
+                                   ctx->d_nan, ctx->stream);
+        fsteps++;
+        ctx->launches++;
+    }
+    // k forward steps from src into dst; intermediate states alternate
+    // between T0 and T1 (src and dst are never T0/T1 and never equal)
+    void advance(const Real *src, Real *dst, int k)
+    {
+        if (err != cudaSuccess) return;
+        if (k == 0) {
+            if (src != dst) err = cudaMemcpyAsync(dst, src, fbytes, cudaMemcpyDeviceToDevice, ctx->stream);
+            return;
+        }
+        const Real *cur = src;
+        for (int s = 0; s < k; s++) {
+            Real *out = (s == k - 1) ? dst : (cur == T0 ? T1 : T0);
+            step(cur, out);
+            cur = out;
+        }
+    }
+    void adjoint_step(const Real *phi_k)
+    {
+        if (err != cudaSuccess) return;
+        err = launch_adjoint_step<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, phi_k, LAM, MU, FL, rho,
+                                        dt, Dw, grad_acc, ctx->stream);
+        asteps++;
+        ctx->launches += 2;
+    }
+    static double beta(int c, int r)  // C(c + r, c), capped
+    {
+        double b = 1;
+        for (int i = 1; i <= c; i++) {
+            b = b * (r + i) / i;
+            if (b > 1e18) return 1e18;
+        }
+        return b;
+    }
+    // X holds phi_a; LAM holds dL/dphi_b on entry and dL/dphi_a on exit;
+    // slots[0..c) are free.
+    void reverse(int a, int b, int c, Real *X)
+    {
+        const int l = b - a;
+        if (l <= 0 || err != cudaSuccess) return;
+        if (l == 1) {
+            adjoint_step(X);
+            return;
+        }
+        if (c == 0) {
+            for (int k = b - 1; k > a; k--) {
+                advance(X, T2, k - a);
+                adjoint_step(T2);
+            }
+            adjoint_step(X);
+            return;
+        }
+        int r = 0;
+        while (beta(c, r) < l) r++;
+        int l1 = (int)std::max(1.0, l - beta(c - 1, r));
+        if (l1 >= l) l1 = l - 1;
+        Real *S = slots[c - 1];
+        advance(X, S, l1);
+        reverse(a + l1, b, c - 1, S);
+        reverse(a, a + l1, c, X);
+    }
+};
+
+template <typename Real>
+int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoint_result *res, void *grad_c0)
+{
+    int rc = prepare_static<Real>(ctx, p->Dw, p->Dg);
+    if (rc) return rc;
+    const int nb = ctx->nblocks, bpd = ctx->bpd, n = 8 * bpd;
+    Adjoint<Real> A;
+    A.ctx = ctx;
+    A.v = view<Real>(ctx);
+    A.fbytes = (size_t)nb * kBS3 * sizeof(Real);
+    A.rho = (Real)p->rho;
+    A.dt = p->dt;
+    A.Dw = (double)(Real)p->Dw;
+    std::vector<void *> owned;
+    auto alloc = [&](size_t bytes, void **out) {
+        cudaError_t e = cudaMalloc(out, bytes);
+        if (e == cudaSuccess) owned.push_back(*out);
+        return e;
+    };
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(ctx->stream);
+        for (void *q : owned) cudaFree(q);
+    };
+    Real *X0 = nullptr, *F = nullptr;
+    double *xpart = nullptr;
+    const int xparts = 148 * 4;
+    cudaError_t e = cudaSuccess;
+    void **bufs[] = {(void **)&X0, (void **)&F, (void **)&A.T0, (void **)&A.T1, (void **)&A.T2, (void **)&A.LAM,
+                     (void **)&A.MU};
+    for (void **b : bufs)
+        if (e == cudaSuccess) e = alloc(A.fbytes, b);
+    if (e == cudaSuccess) e = alloc((size_t)nb * kBS3, (void **)&A.FL);
+    if (e == cudaSuccess) e = alloc((size_t)nb * kGradSlots * sizeof(double), (void **)&A.grad_acc);
+    if (e == cudaSuccess) e = alloc((size_t)xparts * 6 * sizeof(double), (void **)&xpart);
+    A.slots.assign(p->nsnapshots, nullptr);
+    for (int i = 0; i < p->nsnapshots && e == cudaSuccess; i++) e = alloc(A.fbytes, (void **)&A.slots[i]);
+    if (e != cudaSuccess) {
+        cleanup();
+        cudaGetLastError();
+        return fail(ctx, GBFK_E_OOM, "forward_adjoint: %s", cudaGetErrorString(e));
+    }
+    e = cudaMemsetAsync(A.grad_acc, 0, (size_t)nb * kGradSlots * sizeof(double), ctx->stream);
+    // initial condition
+    if (e == cudaSuccess) {
+        if (p->sigma > 0) {
+            e = launch_gaussian_ic<Real>(bpd, (const Real *)ctx->pw, (const Real *)ctx->pg, p->x0, p->sigma, X0,
+                                         ctx->stream);
+            ctx->launches++;
+        } else {
+            e = cudaMemcpyAsync(X0, ctx->phi[ctx->cur], A.fbytes, cudaMemcpyDeviceToDevice, ctx->stream);
+        }
+    }
+    // forward to the horizon, loss and its gradient
+    if (e == cudaSuccess) {
+        A.advance(X0, F, p->nsteps);
+        e = A.err;
+    }
+    double lik[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) {
+        if (!ctx->d_partial) e = cudaMalloc(&ctx->d_partial, (size_t)148 * 4 * 7 * sizeof(double));
+        if (e == cudaSuccess && !ctx->d_lik) e = cudaMalloc(&ctx->d_lik, 4 * sizeof(double));
+        if (e == cudaSuccess && ctx->model_bytes < (size_t)n * n * n * sizeof(double)) {
+            if (ctx->d_model) cudaFree(ctx->d_model);
+            ctx->d_model = nullptr;
+            ctx->model_bytes = 0;
+            e = cudaMalloc(&ctx->d_model, (size_t)n * n * n * sizeof(double));
+            if (e == cudaSuccess) ctx->model_bytes = (size_t)n * n * n * sizeof(double);
+        }
+    }
+    if (e == cudaSuccess)
+        e = launch_uq_dump<Real>(ctx->d_slot, (const Real *)ctx->d_origin, (const Real *)ctx->d_h, nb, F, n,
+                                 ctx->d_model, ctx->stream);
+    if (e == cudaSuccess) {
+        LikelihoodParams lp;
+        lp.pet_sigma2 = 1;
+        lp.pet_scale = 1;
+        lp.t1_uc = p->t1_uc;
+        lp.t2_uc = p->t2_uc;
+        lp.slope = p->slope;
+        lp.step_pet = 1;
+        lp.step_mri = 1;
+        e = launch_likelihood(ctx->d_model, n, ctx->d_t1c, ctx->d_flair, nullptr, nullptr, 0, lp, ctx->d_partial,
+                              148 * 4, ctx->d_lik, ctx->stream);
+        ctx->launches += 3;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(lik, ctx->d_lik, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) {
+        e = launch_loss_grad<Real>(bpd, F, ctx->d_t1c, ctx->d_flair, p->t1_uc, p->t2_uc, p->slope, A.LAM, ctx->stream);
+        ctx->launches++;
+    }
+    // reverse sweep
+    if (e == cudaSuccess) {
+        A.reverse(0, p->nsteps, p->nsnapshots, X0);
+        e = A.err;
+    }
+    // parameter gradients
+    std::vector<double> acc((size_t)nb * kGradSlots);
+    std::vector<double> xp((size_t)xparts * 6, 0.0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(acc.data(), A.grad_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && p->sigma > 0) {
+        e = launch_x0_grad<Real>(bpd, X0, A.LAM, p->x0, p->sigma, xpart, xparts, ctx->stream);
+        ctx->launches++;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(xp.data(), xpart, xp.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    }
+    if (e == cudaSuccess && grad_c0) {
+        if (ctx->stage_bytes < A.fbytes) {
+            if (ctx->d_stage) cudaFree(ctx->d_stage);
+            ctx->d_stage = nullptr;
+            ctx->stage_bytes = 0;
+            e = cudaMalloc(&ctx->d_stage, A.fbytes);
+            if (e == cudaSuccess) ctx->stage_bytes = A.fbytes;
+        }
+        if (e == cudaSuccess) e = launch_dense_scatter<Real>(A.LAM, (Real *)ctx->d_stage, n, false, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(grad_c0, ctx->d_stage, A.fbytes, cudaMemcpyDeviceToHost, ctx->stream);
+        ctx->launches++;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cleanup();
+    if (e != cudaSuccess) return fail(ctx, GBFK_E_CUDA, "forward_adjoint: %s", cudaGetErrorString(e));
+    auto nsum = [](const double *v, size_t stride, size_t count) {
+        double s = 0, c = 0;
+        for (size_t i = 0; i < count; i++)
+            for (int k = 0; k < 2; k++) {
+                const double x = v[i * stride + k];
+                const double t = s + x;
+                if (fabs(s) >= fabs(x)) c += (s - t) + x;
+                else c += (x - t) + s;
+                s = t;
+            }
+        return s + c;
+    };
+    res->loss = -(lik[1] + lik[2]);
+    res->drho = nsum(acc.data(), kGradSlots, nb);
+    res->dDw = nsum(acc.data() + 2, kGradSlots, nb);
+    for (int d = 0; d < 3; d++) res->dx0[d] = p->sigma > 0 ? nsum(xp.data() + 2 * d, 6, xparts) : 0.0;
+    res->forward_steps = A.fsteps;
+    res->adjoint_steps = A.asteps;
+    return GBFK_OK;
+}
+
+}  // namespace
+
+extern "C" int gbfk_forward_adjoint(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoint_result *out,
+                                    void *grad_c0)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!p || !out) return fail(ctx, GBFK_E_INVALID, "forward_adjoint: null argument");
+    if (!ctx->uniform || !ctx->d_origin) return fail(ctx, GBFK_E_STATE, "forward_adjoint: needs a uniform power-of-two grid");
+    if (ctx->obs_n != 8 * ctx->bpd || ctx->nroi) return fail(ctx, GBFK_E_STATE, "forward_adjoint: observations must cover the grid (no ROI)");
+    if (p->nsteps < 0 || p->nsnapshots < 1 || !(p->slope != 0) || !(p->Dw > 0))
+        return fail(ctx, GBFK_E_INVALID, "forward_adjoint: bad parameters");
+    CK(cudaSetDevice(ctx->device));
+    return ctx->precision == GBFK_F64 ? forward_adjoint_impl<double>(ctx, p, out, grad_c0)
+                                      : forward_adjoint_impl<float>(ctx, p, out, grad_c0);
+}

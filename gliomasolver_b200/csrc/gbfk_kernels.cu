@@ -487,6 +487,352 @@ cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigne
 }
 
 // ---------------------------------------------------------------------------
+// Discrete adjoint of the fused step (uniform grids).  The forward step is
+//   pre_i = phi_i + dt * r_i(phi),  phi'_i = clamp(pre_i)
+//   r_i   = dom_i * ( ih2 * sum_k H~_ik phi_k - ih2 * (sum_k H~_ik) phi_i + rho phi_i (1 - phi_i) )
+// with H~_ik the face coefficient toward neighbour k, doubled by the no-flux
+// switch.  The switches (dom, the doubling, the clamp) are piecewise constant
+// in phi and are held fixed (their derivative is taken as 0), and rounding is
+// treated as exact.  Given lambda' = dL/dphi', one adjoint step forms
+//   mu_i     = lambda'_i * [0 < pre_i <= 1]                      (adj_mu)
+//   lambda_j = mu_j + dt * ( dom_j mu_j (-ih2 sum_k H~_jk + rho (1 - 2 phi_j))
+//                           + ih2 sum_{i nbr j} dom_i mu_i H~_ij )  (adj_lambda)
+// and accumulates dL/drho += sum_i mu_i dt dom_i phi_i (1 - phi_i) and
+// dL/dDw += sum_i mu_i dt dom_i (diffusive part of r_i) / Dw (the face
+// coefficients are homogeneous of degree 1 in (Dw, Dg = 0.1 Dw)).
+// adj_mu recomputes the forward step of its block exactly like step_block and
+// records per cell: bit 0 = dom, bit 1+k = coefficient k doubled.
+
+__device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
+{
+    const double t = s + x;
+    if (fabs(s) >= fabs(x)) c += (s - t) + x;
+    else c += (x - t) + s;
+    s = t;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(128)
+adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
+              const double *__restrict__ ih2blk, const Real *__restrict__ phi, const Real *__restrict__ lam_next,
+              Real *__restrict__ mu, unsigned char *__restrict__ flags, Real rho, double dt, double inv_Dw,
+              double *__restrict__ grad_acc)
+{
+    __shared__ __align__(16) Real ph[kStepLab];
+    __shared__ double red[4][128];
+    const int blk = blockIdx.x, t = threadIdx.x;
+    const int64_t base = slot_of(v, blk) * kBS3;
+    const int x4 = (t & 1) * 4, y = (t >> 1) & 7, z = t >> 4;
+    const int c0 = x4 + kBS * (y + kBS * z);
+    const int l0 = lab_p(x4, y, z);
+    Vec4<Real> p;
+    p.load(phi + base + c0);
+    p.store(ph + l0);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const int q = t + 128 * i;
+        const int f = q >> 6, pc = q & 63;
+        int lx, ly, lz, sc;
+        face_cell(f, pc, lx, ly, lz, sc);
+        const int nb = face_neighbour(v, blk, f);
+        ph[lab_p(lx, ly, lz)] = phi[(int64_t)nb * kBS3 + sc];
+    }
+    const unsigned char bt = v.btype[blk];
+    unsigned mw[4];
+    if (bt == kBlockMixed) {
+        for (int i = 0; i < 4; i++) mw[i] = meta[base + c0 + i];
+    } else {
+        const unsigned m = bt == kBlockEmpty ? kMetaAllEmpty : kMetaAllTissue;
+        mw[0] = mw[1] = mw[2] = mw[3] = m;
+    }
+    __syncthreads();
+    const Real *Hb = H + (int64_t)blk * kFacesPerBlock;
+    const double ih2 = ih2blk[blk];
+    const Real eps = (Real)0.1;
+    double grho = 0, grho_c = 0, gdw = 0, gdw_c = 0;
+    Vec4<Real> lam;
+    lam.load(lam_next + base + c0);
+    Vec4<Real> out;
+    unsigned char fl[4];
+#pragma unroll 1
+    for (int i = 0; i < 4; i++) {
+        const int x = x4 + i;
+        const Real ph0 = p.v[i];
+        const unsigned cls = mw[i] & 3u;
+        bool dom;
+        if (cls == kTissue && ph0 >= (Real)0) dom = true;
+        else if (cls == kEmpty) dom = ph0 > (Real)0;
+        else {
+            Real pw, pg;
+            lab_pwpg(v, blk, base, x, y, z, pw, pg);
+            dom = in_domain(pw, pg, ph0);
+        }
+        unsigned char f = dom ? 1 : 0;
+        Real dphidt = (Real)0.;
+        double flux_diff = 0;
+        if (dom) {
+            const int l = l0 + i;
+            Real phn[6] = {ph[l - 1], ph[l + 1], ph[l - kPitch], ph[l + kPitch], ph[l - kPlane], ph[l + kPlane]};
+            bool low[6];
+            for (int k = 0; k < 6; k++) {
+                bool slow;
+                if ((mw[i] >> (2 + k)) & 1u) {
+                    low[k] = phn[k] < eps;
+                    slow = false;
+                } else {
+                    low[k] = false;
+                    slow = ((mw[i] >> (8 + k)) & 1u) || !(phn[k] >= (Real)0);
+                }
+                if (slow) {
+                    const int nx = x + (k == 0 ? -1 : k == 1 ? 1 : 0);
+                    const int ny = y + (k == 2 ? -1 : k == 3 ? 1 : 0);
+                    const int nz = z + (k == 4 ? -1 : k == 5 ? 1 : 0);
+                    Real pw, pg;
+                    lab_pwpg(v, blk, base, nx, ny, nz, pw, pg);
+                    low[k] = domain_chf(phn[k], pw, pg) < eps;
+                }
+            }
+            const int rx = (z * 8 + y) * 9 + x, ry = 576 + (z * 9 + y) * 8 + x, rz = 1152 + (z * 8 + y) * 8 + x;
+            Real df[6] = {Hb[rx], Hb[rx + 1], Hb[ry], Hb[ry + 8], Hb[rz], Hb[rz + 64]};
+            // _applyNoFluxBC: neighbour k below 0.1 doubles the opposite coefficient k^1
+            for (int k = 0; k < 6; k++)
+                if (low[k]) {
+                    df[k ^ 1] = rmul(df[k ^ 1], (Real)2.0);
+                    f |= (unsigned char)(1u << (1 + (k ^ 1)));
+                }
+            Real sin_ = rmul(df[0], phn[0]);
+            for (int k = 1; k < 6; k++) sin_ = radd(sin_, rmul(df[k], phn[k]));
+            const double fluxIn = __dmul_rn(ih2, (double)sin_);
+            const Real sdf = radd(radd(radd(radd(radd(df[0], df[1]), df[2]), df[3]), df[4]), df[5]);
+            const double fluxOut = -__dmul_rn((double)rmul(sdf, ph0), ih2);
+            const double reaction = __dmul_rn((double)rmul(rho, ph0), __dadd_rn(1., -(double)ph0));
+            dphidt = to_real<Real>(__dadd_rn(__dadd_rn(fluxOut, fluxIn), reaction));
+            flux_diff = fluxOut + fluxIn;
+        }
+        const Real pre = to_real<Real>(__dadd_rn((double)ph0, __dmul_rn(dt, (double)dphidt)));
+        const bool pass = pre > (Real)0 && pre <= (Real)1;
+        const Real m = pass ? lam.v[i] : (Real)0;
+        out.v[i] = m;
+        fl[i] = f;
+        if (dom && pass) {
+            neumaier_add(grho, grho_c, (double)m * dt * (double)ph0 * (1. - (double)ph0));
+            neumaier_add(gdw, gdw_c, (double)m * dt * flux_diff * inv_Dw);
+        }
+    }
+    out.store(mu + base + c0);
+    *reinterpret_cast<uchar4 *>(flags + base + c0) = make_uchar4(fl[0], fl[1], fl[2], fl[3]);
+    // CTA partials, accumulated into this CTA's own slot (deterministic: one
+    // writer per slot and launches are ordered on the stream)
+    red[0][t] = grho; red[1][t] = grho_c; red[2][t] = gdw; red[3][t] = gdw_c;
+    __syncthreads();
+    for (int w = 64; w > 0; w >>= 1) {
+        if (t < w) {
+            neumaier_add(red[0][t], red[1][t], red[0][t + w]);
+            neumaier_add(red[0][t], red[1][t], red[1][t + w]);
+            neumaier_add(red[2][t], red[3][t], red[2][t + w]);
+            neumaier_add(red[2][t], red[3][t], red[3][t + w]);
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        double *acc = grad_acc + (int64_t)blk * kGradSlots;
+        neumaier_add(acc[0], acc[1], red[0][0]);
+        neumaier_add(acc[0], acc[1], red[1][0]);
+        neumaier_add(acc[2], acc[3], red[2][0]);
+        neumaier_add(acc[2], acc[3], red[3][0]);
+    }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(128)
+adj_lambda_kernel(PoolView<Real> v, const Real *__restrict__ H, const double *__restrict__ ih2blk,
+                  const Real *__restrict__ phi, const Real *__restrict__ mu, const unsigned char *__restrict__ flags,
+                  Real *__restrict__ lam, Real rho, double dt)
+{
+    __shared__ __align__(16) Real smu[kStepLab];
+    __shared__ unsigned char sfl[kStepLab];
+    const int blk = blockIdx.x, t = threadIdx.x;
+    const int64_t base = slot_of(v, blk) * kBS3;
+    const int x4 = (t & 1) * 4, y = (t >> 1) & 7, z = t >> 4;
+    const int c0 = x4 + kBS * (y + kBS * z);
+    const int l0 = lab_p(x4, y, z);
+    Vec4<Real> m;
+    m.load(mu + base + c0);
+    m.store(smu + l0);
+    const uchar4 f4 = *reinterpret_cast<const uchar4 *>(flags + base + c0);
+    sfl[l0] = f4.x; sfl[l0 + 1] = f4.y; sfl[l0 + 2] = f4.z; sfl[l0 + 3] = f4.w;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const int q = t + 128 * i;
+        const int f = q >> 6, pc = q & 63;
+        int lx, ly, lz, sc;
+        face_cell(f, pc, lx, ly, lz, sc);
+        const int nb = face_neighbour(v, blk, f);
+        const int l = lab_p(lx, ly, lz);
+        smu[l] = mu[(int64_t)nb * kBS3 + sc];
+        sfl[l] = flags[(int64_t)nb * kBS3 + sc];
+    }
+    Vec4<Real> p;
+    p.load(phi + base + c0);
+    __syncthreads();
+    const Real *Hb = H + (int64_t)blk * kFacesPerBlock;
+    const double ih2 = ih2blk[blk];
+    Vec4<Real> out;
+#pragma unroll 1
+    for (int i = 0; i < 4; i++) {
+        const int x = x4 + i;
+        const int l = l0 + i;
+        const int rx = (z * 8 + y) * 9 + x, ry = 576 + (z * 9 + y) * 8 + x, rz = 1152 + (z * 8 + y) * 8 + x;
+        const double hf[6] = {(double)Hb[rx], (double)Hb[rx + 1], (double)Hb[ry], (double)Hb[ry + 8],
+                              (double)Hb[rz], (double)Hb[rz + 64]};
+        const int ln[6] = {l - 1, l + 1, l - kPitch, l + kPitch, l - kPlane, l + kPlane};
+        const unsigned fj = sfl[l];
+        const double muj = (double)smu[l];
+        double acc = 0;
+        if (fj & 1u) {
+            double sdf = 0;
+            for (int k = 0; k < 6; k++) sdf += ((fj >> (1 + k)) & 1u) ? 2. * hf[k] : hf[k];
+            const double ph0 = (double)p.v[i];
+            acc += muj * (-ih2 * sdf + (double)rho * (1. - 2. * ph0));
+        }
+        for (int k = 0; k < 6; k++) {
+            const unsigned fi = sfl[ln[k]];
+            if (!(fi & 1u)) continue;
+            // neighbour i sees this cell in direction k^1
+            const double hik = ((fi >> (1 + (k ^ 1))) & 1u) ? 2. * hf[k] : hf[k];
+            acc += ih2 * hik * (double)smu[ln[k]];
+        }
+        out.v[i] = (Real)(muj + dt * acc);
+    }
+    out.store(lam + base + c0);
+}
+
+template <typename Real>
+cudaError_t launch_adjoint_step(const PoolView<Real> &v, const Real *H, const unsigned short *meta, const double *ih2,
+                                const Real *phi, Real *lam, Real *mu, unsigned char *flags, Real rho, double dt,
+                                double Dw, double *grad_acc, cudaStream_t s)
+{
+    if (v.nblocks <= 0) return cudaSuccess;
+    adj_mu_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, meta, ih2, phi, lam, mu, flags, rho, dt, 1. / Dw, grad_acc);
+    adj_lambda_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, ih2, phi, mu, flags, lam, rho, dt);
+    return cudaGetLastError();
+}
+
+// dL/du of loss = -(L_T1c + L_FLAIR) (HGG_Likelihood.cpp:136-156) on a
+// uniform grid, written in pool order; the dump of a uniform grid is the
+// identity.  For d = u - uc > 0 the term is constant in u; for d < 0,
+// d log(alpha)/du = -2 d/slope and d log(1-alpha)/du = e d/slope / (1 - e/2),
+// e = exp(-d^2/slope); at d = 0 both are 0.
+__device__ __forceinline__ double bernoulli_dlog(double u, double uc, double is2, bool y)
+{
+    const double d = u - uc;
+    if (!(d < -0.0)) return 0.;
+    const double e = exp(-d * d * is2);
+    return y ? -2. * d * is2 : e * d * is2 / (1. - 0.5 * e);
+}
+
+template <typename Real>
+__global__ void loss_grad_kernel(int bpd, const Real *__restrict__ phi, const unsigned char *__restrict__ t1c,
+                                 const unsigned char *__restrict__ flair, double t1uc, double t2uc, double is2,
+                                 Real *__restrict__ lam)
+{
+    const int n = 8 * bpd;
+    const int64_t N = (int64_t)n * n * n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = i >> 9;
+        const int c = (int)(i & 511);
+        const int bx = (int)(b % bpd), by = (int)((b / bpd) % bpd), bz = (int)(b / ((int64_t)bpd * bpd));
+        const int64_t g = (bx * 8 + (c & 7)) + (int64_t)n * ((by * 8 + ((c >> 3) & 7)) + (int64_t)n * (bz * 8 + (c >> 6)));
+        const double u = (double)phi[i];
+        lam[i] = (Real)(-(bernoulli_dlog(u, t1uc, is2, t1c[g] != 0) + bernoulli_dlog(u, t2uc, is2, flair[g] != 0)));
+    }
+}
+
+template <typename Real>
+cudaError_t launch_loss_grad(int bpd, const Real *phi, const unsigned char *t1c, const unsigned char *flair,
+                             double t1uc, double t2uc, double slope, Real *lam, cudaStream_t s)
+{
+    const int64_t N = (int64_t)512 * bpd * bpd * bpd;
+    int64_t nb = (N + 255) / 256;
+    if (nb > 148 * 32) nb = 148 * 32;
+    loss_grad_kernel<Real><<<(int)nb, 256, 0, s>>>(bpd, phi, t1c, flair, t1uc, t2uc, 1. / slope, lam);
+    return cudaGetLastError();
+}
+
+// Initial condition c0 = exp(-|x-x0|^2/(2 sigma^2)) where p_w + p_g > 0 (x =
+// vertex positions of a uniform bpd^3 grid, pool order), and the reduction
+// of dL/dx0 = sum_i lambda0_i c0_i (x_i - x0) / sigma^2 (per CTA partials).
+template <typename Real>
+__global__ void gaussian_ic_kernel(int bpd, const Real *__restrict__ pw, const Real *__restrict__ pg, double x0,
+                                   double y0, double z0, double sigma, Real *__restrict__ out)
+{
+    const int n = 8 * bpd;
+    const int64_t N = (int64_t)n * n * n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = i >> 9;
+        const int c = (int)(i & 511);
+        const int bx = (int)(b % bpd), by = (int)((b / bpd) % bpd), bz = (int)(b / ((int64_t)bpd * bpd));
+        const double x = (double)(bx * 8 + (c & 7)) / n, y = (double)(by * 8 + ((c >> 3) & 7)) / n,
+                     z = (double)(bz * 8 + (c >> 6)) / n;
+        const double r2 = (x - x0) * (x - x0) + (y - y0) * (y - y0) + (z - z0) * (z - z0);
+        out[i] = (pw[i] + pg[i] > (Real)0) ? (Real)exp(-r2 / (2. * sigma * sigma)) : (Real)0;
+    }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(256)
+x0_grad_kernel(int bpd, const Real *__restrict__ c0, const Real *__restrict__ lam0, double x0, double y0, double z0,
+               double sigma, double *__restrict__ partial)
+{
+    const int n = 8 * bpd;
+    const int64_t N = (int64_t)n * n * n;
+    double s[3] = {0, 0, 0}, cc[3] = {0, 0, 0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = i >> 9;
+        const int c = (int)(i & 511);
+        const int bx = (int)(b % bpd), by = (int)((b / bpd) % bpd), bz = (int)(b / ((int64_t)bpd * bpd));
+        const double xs[3] = {(double)(bx * 8 + (c & 7)) / n, (double)(by * 8 + ((c >> 3) & 7)) / n,
+                              (double)(bz * 8 + (c >> 6)) / n};
+        const double w = (double)lam0[i] * (double)c0[i] / (sigma * sigma);
+        neumaier_add(s[0], cc[0], w * (xs[0] - x0));
+        neumaier_add(s[1], cc[1], w * (xs[1] - y0));
+        neumaier_add(s[2], cc[2], w * (xs[2] - z0));
+    }
+    __shared__ double red[6][256];
+    const int t = threadIdx.x;
+    for (int d = 0; d < 3; d++) { red[2 * d][t] = s[d]; red[2 * d + 1][t] = cc[d]; }
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (t < w)
+            for (int d = 0; d < 3; d++) {
+                neumaier_add(red[2 * d][t], red[2 * d + 1][t], red[2 * d][t + w]);
+                neumaier_add(red[2 * d][t], red[2 * d + 1][t], red[2 * d + 1][t + w]);
+            }
+        __syncthreads();
+    }
+    if (t < 6) partial[blockIdx.x * 6 + t] = red[t][0];
+}
+
+template <typename Real>
+cudaError_t launch_gaussian_ic(int bpd, const Real *pw, const Real *pg, const double x0[3], double sigma, Real *out,
+                               cudaStream_t s)
+{
+    const int64_t N = (int64_t)512 * bpd * bpd * bpd;
+    int64_t nb = (N + 255) / 256;
+    if (nb > 148 * 32) nb = 148 * 32;
+    gaussian_ic_kernel<Real><<<(int)nb, 256, 0, s>>>(bpd, pw, pg, x0[0], x0[1], x0[2], sigma, out);
+    return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_x0_grad(int bpd, const Real *c0, const Real *lam0, const double x0[3], double sigma,
+                           double *partial, int nparts, cudaStream_t s)
+{
+    x0_grad_kernel<Real><<<nparts, 256, 0, s>>>(bpd, c0, lam0, x0[0], x0[1], x0[2], sigma, partial);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Ghost fill: BlockLab::load step 3 (MRAGBlockLab.h:277-293) for a list of
 // rows, ghost = 0; ghost += v * w in Real, entries in list order.
 template <typename Real>
@@ -744,6 +1090,15 @@ cudaError_t upload_ghost_table()
     template cudaError_t launch_faces<Real>(const PoolView<Real> &, Real, Real, Real *, unsigned short *,       \
                                             unsigned char *, cudaStream_t);                                   \
     template cudaError_t launch_rd_batch_step<Real>(const BatchView<Real> &, int, int, int, cudaStream_t);      \
+    template cudaError_t launch_adjoint_step<Real>(const PoolView<Real> &, const Real *, const unsigned short *,  \
+                                                   const double *, const Real *, Real *, Real *, unsigned char *, \
+                                                   Real, double, double, double *, cudaStream_t);            \
+    template cudaError_t launch_loss_grad<Real>(int, const Real *, const unsigned char *, const unsigned char *, \
+                                                double, double, double, Real *, cudaStream_t);               \
+    template cudaError_t launch_gaussian_ic<Real>(int, const Real *, const Real *, const double *, double, Real *, \
+                                                  cudaStream_t);                                             \
+    template cudaError_t launch_x0_grad<Real>(int, const Real *, const Real *, const double *, double, double *, \
+                                              int, cudaStream_t);                                            \
     template cudaError_t launch_fill_ghosts<Real>(const int *, int64_t, const int64_t *, const int *,         \
                                                   const Real *, const Real *, Real *, cudaStream_t);          \
     template cudaError_t launch_fwt_details<Real>(const PoolView<Real> &, const Real *, double *, cudaStream_t); \

@@ -12,6 +12,7 @@ constexpr int kLab3 = 1000;
 constexpr int kLabGhosts = 488;
 constexpr int kFaceCells = 64;
 constexpr int kFacesPerBlock = 3 * 576;  // x, y, z faces of a block incl. its boundary faces
+constexpr int kGradSlots = 4;            // adjoint gradient partials per block: rho (sum, comp), Dw (sum, comp)
 
 // cell classes for the step's exact shortcuts (see cell_class)
 constexpr unsigned char kEmpty = 0, kTissue = 1, kOther = 2;
@@ -106,6 +107,23 @@ struct LikelihoodParams {
 cudaError_t launch_likelihood(const double *model, int n, const unsigned char *t1c, const unsigned char *flair,
                               const double *pet, const int *roi, int nroi, const LikelihoodParams &p,
                               double *partial, int nparts, double *out, cudaStream_t s);
+
+// Discrete adjoint (uniform grids): one adjoint step through the step that
+// maps phi (input state) to the next state; lam holds dL/dphi' on entry and
+// dL/dphi on exit; grad_acc: nblocks * 4 doubles (rho sum/comp, Dw sum/comp).
+template <typename Real>
+cudaError_t launch_adjoint_step(const PoolView<Real> &v, const Real *H, const unsigned short *meta, const double *ih2,
+                                const Real *phi, Real *lam, Real *mu, unsigned char *flags, Real rho, double dt,
+                                double Dw, double *grad_acc, cudaStream_t s);
+template <typename Real>
+cudaError_t launch_loss_grad(int bpd, const Real *phi, const unsigned char *t1c, const unsigned char *flair,
+                             double t1uc, double t2uc, double slope, Real *lam, cudaStream_t s);
+template <typename Real>
+cudaError_t launch_gaussian_ic(int bpd, const Real *pw, const Real *pg, const double x0[3], double sigma, Real *out,
+                               cudaStream_t s);
+template <typename Real>
+cudaError_t launch_x0_grad(int bpd, const Real *c0, const Real *lam0, const double x0[3], double sigma,
+                           double *partial, int nparts, cudaStream_t s);
 
 template <typename Real>
 cudaError_t launch_dense_scatter(const Real *dense, Real *pool, int n, bool to_pool, cudaStream_t s);

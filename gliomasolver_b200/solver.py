@@ -194,6 +194,25 @@ class BlockPool:
         return out
 
 
+    # -- discrete adjoint ---------------------------------------------------
+    def forward_adjoint(self, Dw, Dg, rho, dt, nsteps, x0=(0.0, 0.0, 0.0), sigma=0.0, nsnapshots=64, t1_uc=0.7,
+                        t2_uc=0.25, slope=2.0, grad_c0=False):
+        """Loss -(L_T1c + L_FLAIR) at the horizon and its gradients (gbfk_forward_adjoint).
+        Returns a dict; with grad_c0 the dense d loss / d c0 is included."""
+        p = _lib.AdjointParams(float(Dw), float(Dg), float(rho), float(dt), int(nsteps), int(nsnapshots),
+                               (ctypes.c_double * 3)(*[float(v) for v in x0]), float(sigma), float(t1_uc),
+                               float(t2_uc), float(slope))
+        r = _lib.AdjointResult()
+        g = np.empty((self.n, self.n, self.n), dtype=self.dtype) if grad_c0 else None
+        self._check(self.lib.gbfk_forward_adjoint(self.ctx, ctypes.byref(p), ctypes.byref(r),
+                                                  None if g is None else _ptr(g)))
+        out = {"loss": r.loss, "dDw": r.dDw, "drho": r.drho, "dx0": np.array(list(r.dx0)),
+               "forward_steps": int(r.forward_steps), "adjoint_steps": int(r.adjoint_steps)}
+        if g is not None:
+            out["grad_c0"] = g
+        return out
+
+
 # ---------------------------------------------------------------- operators
 class ReactionDiffusionOperator:
     """Tag for ReactionDiffusionOperator<3> (ReactionDiffusionOperator.h:21-43):

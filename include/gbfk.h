@@ -214,6 +214,35 @@ int gbfk_uq_dump(gbfk_ctx *ctx, int n, double *host_out);
  * -out[3] to Likelihood.txt).  Sums are FP64 with compensation. */
 int gbfk_log_likelihood(gbfk_ctx *ctx, const gbfk_likelihood_params *params, double out[4]);
 
+/* --- discrete adjoint ------------------------------------------------- */
+/* No counterpart in the reference (which samples with TMCMC and never
+ * differentiates).  Forward solve plus the hand-written discrete adjoint of
+ * the fused step on the context's uniform grid, for the loss
+ *   loss = -(L_T1c + L_FLAIR)        (HGG_Likelihood.cpp:77-156)
+ * of the state at the horizon against the observations (gbfk_set_observations,
+ * without ROI).  dt and the step count are held fixed; the piecewise-constant
+ * switches of the step (domain test, no-flux doubling, clamp) are held fixed.
+ * States are kept with binomial checkpointing in nsnapshots device buffers. */
+typedef struct {
+    double Dw, Dg, rho, dt; /* rescaled Real coefficients and the time step */
+    int nsteps;             /* steps to the horizon */
+    int nsnapshots;         /* checkpoint buffers (>= 1) */
+    double x0[3];           /* tumour origin, used when sigma > 0 */
+    double sigma;           /* > 0: c0 = exp(-|x-x0|^2/(2 sigma^2)) where p_w+p_g > 0;
+                               <= 0: c0 = the context's current phi */
+    double t1_uc, t2_uc, slope; /* Bernoulli loss parameters */
+} gbfk_adjoint_params;
+typedef struct {
+    double loss;            /* -(L_T1c + L_FLAIR) at the horizon */
+    double dDw, drho;       /* d loss / d Dw (with Dg = 0.1 Dw), d loss / d rho */
+    double dx0[3];          /* d loss / d x0 (0 when sigma <= 0) */
+    int64_t forward_steps;  /* forward steps run, recomputation included */
+    int64_t adjoint_steps;
+} gbfk_adjoint_result;
+/* grad_c0_dense: NULL, or n^3 Real (x fastest) receiving d loss / d c0. */
+int gbfk_forward_adjoint(gbfk_ctx *ctx, const gbfk_adjoint_params *params, gbfk_adjoint_result *out,
+                         void *grad_c0_dense);
+
 /* --- allocation-free step -------------------------------------------- */
 /* No counterpart in the reference.  One fused RD step (the operator and the
  * update of gbfk_rd_step) on a uniform periodic bpd^3 grid, for callers that
