@@ -240,6 +240,68 @@ def batched_stage(args, stream, local, nsamples=512, bpd=16, seed=1):
     }
 
 
+def adjoint_sample(stream, local, bpd=16, nsnap=64):
+    """Config 4: forward + discrete adjoint at 128^3, FP32 state, FP64 loss and
+    gradient sums, 64 checkpoint buffers, about 10^4 steps (Dw = 0.2, T = 300 d);
+    observations from a seeded ground-truth run (rho = 0.012) thresholded at
+    0.7 / 0.25 with 2% label noise; gradients taken at Dw = 0.18, rho = 0.014.
+    rho*T ~ 4 keeps a tumour front: with rho*T >> 1 the tumour saturates the
+    brain (every cell exactly 0 or 1), the loss is locally constant and all
+    gradients are 0.  Timed against one plain forward solve of the same steps."""
+    import torch
+
+    from gliomasolver_b200 import BlockPool
+    from gliomasolver_b200.anatomy import make_anatomy, pick_origin, tumor_ic
+
+    n = 8 * bpd
+    p_w, p_g, _ = make_anatomy(n, SEED)
+    s = make_schedule(0.2, 0.012, 300.0, L_CM, bpd, "f32")
+    x_gt = pick_origin(p_w, SEED)[0]
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    with BlockPool(bpd ** 3, "f32", device=local, stream=stream.cuda_stream) as pool:
+        pool.set_uniform(bpd)
+        pool.upload_dense("p_w", p_w.astype(np.float32))
+        pool.upload_dense("p_g", p_g.astype(np.float32))
+        pool.upload_dense("phi", tumor_ic(n, x_gt, p_w, p_g).astype(np.float32))
+        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, s.nsteps)
+        u = pool.download_dense("phi").astype(np.float64)
+        rng = np.random.default_rng(SEED + 17)
+        masks = [(u > 0.7).astype(float), (u > 0.25).astype(float)]
+        for m in masks:
+            flip = rng.random(m.shape) < 0.02
+            m[flip] = 1 - m[flip]
+        pool.set_observations(*masks)
+        x0 = np.clip(np.array(x_gt) + 2.0 / n, 0, 1)
+        Dw = float(np.float32(np.float32(0.18) / np.float32(L_CM * L_CM)))
+        Dg = float(np.float32(0.1 * Dw))
+        # warm-up (face coefficients, first allocations)
+        pool.forward_adjoint(Dw, Dg, 0.014, s.dt, 20, x0=x0, sigma=2.0 / n, nsnapshots=nsnap)
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        res = pool.forward_adjoint(Dw, Dg, 0.014, s.dt, s.nsteps, x0=x0, sigma=2.0 / n, nsnapshots=nsnap)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_adj = e0.elapsed_time(e1) / 1e3
+        pool.upload_dense("phi", tumor_ic(n, x0, p_w, p_g).astype(np.float32))
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        pool.rd_step(Dw, Dg, 0.014, s.dt, s.nsteps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_fwd = e0.elapsed_time(e1) / 1e3
+    return {
+        "workload": f"forward + discrete adjoint, {n}^3 uniform, FP32 state, FP64 loss/gradient sums, "
+                    f"{nsnap} checkpoint buffers, {s.nsteps} steps",
+        "steps": s.nsteps, "forward_steps_run": res["forward_steps"], "adjoint_steps": res["adjoint_steps"],
+        "gradient_s": t_adj, "gradient_samples_per_s": 1.0 / t_adj,
+        "plain_forward_s": t_fwd, "plain_forward_samples_per_s": 1.0 / t_fwd,
+        "gradient_cost_in_forward_solves": t_adj / t_fwd,
+        "loss": res["loss"], "dDw": res["dDw"], "drho": res["drho"], "dx0": list(res["dx0"]),
+    }
+
+
 def gpu_arm(args):
     import torch
     import torch.distributed as dist
@@ -347,8 +409,10 @@ def gpu_arm(args):
            "api": "BlockPool.upload_dense x3 + rd_step + gbfk_download_dense (pinned host buffers)"}
 
     batch = None
+    adj = None
     if not args.no_batch:
         batch = batched_stage(args, stream, local)
+        adj = adjoint_sample(stream, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -364,7 +428,7 @@ def gpu_arm(args):
             "vs_baseline": None, "dtype": prec, "data": "synthetic", "config": workload_config(n, prec),
             "parallelism": "replicas" if world > 1 else "single",
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-            "batched_stage": batch,
+            "batched_stage": batch, "forward_adjoint": adj,
         }
         print(json.dumps(line), flush=True)
     pool.close()
