@@ -37,6 +37,9 @@ from gliomasolver_b200.schedule import make_schedule  # noqa: E402
 
 METRIC = "RD cell-updates/s & % HBM roofline"
 UNIT = "cell-updates/s"
+# the step kernel each GBFK_STEP_* choice launches
+KERNEL_NAMES = {"pipelined": "rd_step_tma_kernel<{real}> (persistent, TMA-fed)",
+                "block": "rd_step_kernel<{real},0> (one CTA per block)"}
 N_GRID = 256
 DW, RHO, TEND, L_CM = 0.2, 0.05, 300.0, 25.6
 SEED = 0
@@ -335,6 +338,7 @@ def gpu_arm(args):
     pool = BlockPool((n // 8) ** 3, prec, device=local, stream=stream.cuda_stream)
     assert stream.cuda_stream != 0
     pool.set_uniform(n // 8)
+    pool.step_kernel = args.step_kernel
     pool.upload_dense("p_w", pw)
     pool.upload_dense("p_g", pg)
     pool.upload_dense("phi", c0)
@@ -355,8 +359,7 @@ def gpu_arm(args):
     launches0 = pool.launches
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1)
+    pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
     launches = pool.launches - launches0
@@ -377,7 +380,8 @@ def gpu_arm(args):
     achieved = alg_bytes / kernel_s / 1e9
     peak, peak_kind = measured_peak()
     traffic = profiled_traffic()
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+    roofline = {"kernel": KERNEL_NAMES[pool.step_kernel].format(real="float" if prec == "f32" else "double"),
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "algorithmic_bytes_per_launch": alg_bytes}
 
@@ -448,6 +452,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched TMCMC-stage measurement")
+    ap.add_argument("--step-kernel", default="auto", choices=["auto", "block", "pipelined"],
+                    help="step kernel of the resident solve (auto: pipelined on uniform power-of-two grids)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

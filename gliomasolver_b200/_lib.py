@@ -25,13 +25,16 @@ STATUS = {
 }
 GBFK_F64, GBFK_F32 = 0, 1
 GBFK_PHI, GBFK_PW, GBFK_PG = 0, 1, 2
+# step kernels (gbfk_set_step_kernel)
+STEP_KERNELS = {"auto": 0, "block": 1, "pipelined": 2}
 
 # Every symbol include/gbfk.h declares (checked by the CPU test suite).
 EXPORTS = (
     "gbfk_create", "gbfk_destroy", "gbfk_last_error", "gbfk_sync", "gbfk_launch_count",
     "gbfk_set_uniform", "gbfk_set_topology", "gbfk_num_blocks",
     "gbfk_upload_field", "gbfk_download_field", "gbfk_upload_dense", "gbfk_download_dense",
-    "gbfk_rd_step", "gbfk_rd_rhs", "gbfk_fwt_details", "gbfk_split", "gbfk_collapse",
+    "gbfk_rd_step", "gbfk_set_step_kernel", "gbfk_step_kernel",
+    "gbfk_rd_rhs", "gbfk_fwt_details", "gbfk_split", "gbfk_collapse",
     "gbfk_rd_step_static",
     "gbfk_set_observations", "gbfk_uq_dump", "gbfk_log_likelihood",
     "gbfk_batch_create", "gbfk_batch_destroy", "gbfk_batch_last_error", "gbfk_batch_launch_count",
@@ -146,6 +149,8 @@ def load(path: Path | str | None = None):
         "gbfk_upload_dense": (I, [P, I, P, I]),
         "gbfk_download_dense": (I, [P, I, P, I]),
         "gbfk_rd_step": (I, [P, D, D, D, D, I, I]),
+        "gbfk_set_step_kernel": (I, [P, I]),
+        "gbfk_step_kernel": (I, [P]),
         "gbfk_rd_rhs": (I, [P, D, D, D, P]),
         "gbfk_fwt_details": (I, [P, P]),
         "gbfk_split": (I, [P, I, P, P]),

@@ -10,7 +10,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
-SOURCES = ["csrc/gbfk_kernels.cu", "csrc/gbfk_api.cu", "csrc/gbfk_static.cu", "csrc/gbfk_uq.cu", "csrc/gbfk_batch.cu"]
+SOURCES = ["csrc/gbfk_kernels.cu", "csrc/gbfk_api.cu", "csrc/gbfk_static.cu", "csrc/gbfk_uq.cu", "csrc/gbfk_batch.cu",
+           "csrc/gbfk_step_tma.cu"]
 OUT = HERE / "libgbfk.so"
 
 NVCC_FLAGS = [

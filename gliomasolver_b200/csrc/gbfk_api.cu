@@ -78,8 +78,15 @@ struct gbfk_ctx {
     bool faces_valid = false;
     double faces_Dw = 0, faces_Dg = 0;
 
+    // step kernel: preference (GBFK_STEP_*), the one the last step ran, and
+    // the pipelined step's tensor maps of phi[0] / phi[1]
+    int step_pref = GBFK_STEP_AUTO;
+    int step_used = 0;
+    bool tma_maps_ready = false;
+    CUtensorMap tma_maps[2][3];
+
     // scratch
-    unsigned *d_nan = nullptr;
+    unsigned *d_nan = nullptr;        // [0]: NaN seen in a step, [1]: a pipeline stage wait timed out
     void *d_stage = nullptr;
     size_t stage_bytes = 0;
     double *d_fwt = nullptr;
@@ -212,6 +219,20 @@ int ints_scratch(gbfk_ctx *ctx, size_t n)
     ctx->ints_cap = 0;
     CK(cudaMalloc(&ctx->d_ints, n * sizeof(int)));
     ctx->ints_cap = n;
+    return GBFK_OK;
+}
+
+// The pipelined step's timeout word (d_nan[1]); reading it synchronises the
+// stream.  A timeout is reported once and the word cleared.
+int check_stage_timeout(gbfk_ctx *ctx)
+{
+    unsigned flag = 0;
+    CK(cudaMemcpyAsync(&flag, ctx->d_nan + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (flag) {
+        CK(cudaMemsetAsync(ctx->d_nan + 1, 0, sizeof(unsigned), ctx->stream));
+        return fail(ctx, GBFK_E_CUDA, "rd_step: a pipeline stage's copies did not complete within 1 s");
+    }
     return GBFK_OK;
 }
 
@@ -376,10 +397,32 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
     int rc = prepare_static<Real>(ctx, Dw, Dg);
     if (rc) return rc;
     PoolView<Real> v = view<Real>(ctx);
+    const bool eligible = tma_step_eligible<Real>(v);
+    if (ctx->step_pref == GBFK_STEP_PIPELINED && !eligible)
+        return fail(ctx, GBFK_E_STATE, "rd_step: the pipelined step needs a uniform power-of-two grid (gbfk_set_uniform)");
+    const bool pipelined = eligible && ctx->step_pref != GBFK_STEP_BLOCK;
+    double ih2 = 0;
+    if (pipelined) {
+        if (!ctx->tma_maps_ready) {
+            for (int b = 0; b < 2; b++)
+                CK(make_pool_tensor_maps(ctx->phi[b], ctx->max_blocks, (int)sizeof(Real), ctx->tma_maps[b]));
+            ctx->tma_maps_ready = true;
+        }
+        // uniform grid: one h for every block, as upload_ih2 forms it
+        const double h = sizeof(Real) == 8 ? ctx->h_h[0] : (double)(float)ctx->h_h[0];
+        ih2 = 1. / (h * h);
+    }
     if (check_nan) CK(cudaMemsetAsync(ctx->d_nan, 0, sizeof(unsigned), ctx->stream));
     for (int s = 0; s < nsteps; s++) {
         const Real *in = (const Real *)ctx->phi[ctx->cur];
         Real *out = (Real *)ctx->phi[ctx->cur ^ 1];
+        if (pipelined) {
+            CK(launch_rd_step_tma<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ih2, in, out, (Real)rho, dt,
+                                        ctx->d_nan, ctx->d_nan + 1, ctx->tma_maps[ctx->cur], ctx->stream));
+            ctx->launches++;
+            ctx->cur ^= 1;
+            continue;
+        }
         if (ctx->n_step_rows > 0) {
             CK(launch_fill_ghosts<Real>(ctx->d_step_rows, ctx->n_step_rows, ctx->d_row_ptr, ctx->d_src,
                                         (const Real *)ctx->d_w, in, (Real *)ctx->d_gphi, ctx->stream));
@@ -390,10 +433,13 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
         ctx->launches++;
         ctx->cur ^= 1;
     }
+    if (nsteps > 0) ctx->step_used = pipelined ? GBFK_STEP_PIPELINED : GBFK_STEP_BLOCK;
     if (check_nan) {
         unsigned flag = 0;
         CK(cudaMemcpyAsync(&flag, ctx->d_nan, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        int rc2 = check_stage_timeout(ctx);
+        if (rc2) return rc2;
         if (flag) return fail(ctx, GBFK_E_NAN, "phi became NaN during the step");
     }
     return GBFK_OK;
@@ -547,7 +593,7 @@ int gbfk_create(const gbfk_config *cfg, gbfk_ctx **out)
     const size_t bytes = (size_t)cfg->max_blocks * kBS3 * ctx->rsize;
     if (cudaMalloc(&ctx->phi[0], bytes) != cudaSuccess || cudaMalloc(&ctx->phi[1], bytes) != cudaSuccess ||
         cudaMalloc(&ctx->pw, bytes) != cudaSuccess || cudaMalloc(&ctx->pg, bytes) != cudaSuccess ||
-        cudaMalloc(&ctx->d_nan, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_nan, 2 * sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&ctx->d_meta, (size_t)cfg->max_blocks * kBS3 * sizeof(unsigned short)) != cudaSuccess) {
         cudaGetLastError();
         return bail(GBFK_E_OOM);
@@ -556,7 +602,7 @@ int gbfk_create(const gbfk_config *cfg, gbfk_ctx **out)
     cudaMemset(ctx->phi[1], 0, bytes);
     cudaMemset(ctx->pw, 0, bytes);
     cudaMemset(ctx->pg, 0, bytes);
-    cudaMemset(ctx->d_nan, 0, sizeof(unsigned));
+    cudaMemset(ctx->d_nan, 0, 2 * sizeof(unsigned));
     if (ensure_table(ctx) != GBFK_OK) return bail(GBFK_E_CUDA);
     *out = ctx;
     return GBFK_OK;
@@ -584,8 +630,19 @@ int gbfk_sync(gbfk_ctx *ctx)
     if (!ctx) return GBFK_E_INVALID;
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->stream));
+    return check_stage_timeout(ctx);
+}
+
+int gbfk_set_step_kernel(gbfk_ctx *ctx, int kind)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (kind != GBFK_STEP_AUTO && kind != GBFK_STEP_BLOCK && kind != GBFK_STEP_PIPELINED)
+        return fail(ctx, GBFK_E_INVALID, "set_step_kernel: unknown kernel %d", kind);
+    ctx->step_pref = kind;
     return GBFK_OK;
 }
+
+int gbfk_step_kernel(const gbfk_ctx *ctx) { return ctx ? ctx->step_used : 0; }
 
 int64_t gbfk_launch_count(const gbfk_ctx *ctx) { return ctx ? ctx->launches : 0; }
 

@@ -44,9 +44,6 @@ __device__ __forceinline__ void face_cell(int f, int p, int &lx, int &ly, int &l
 //   kTissue: t = p_w + p_g >= 0.1 in Real.  Rounding is monotone, so for
 //            phi >= 0 both chf >= t >= 0.1 (no doubling) and t + phi > 0 hold;
 //   kOther : evaluated exactly from p_w and p_g.
-// meta words of a cell whose own class and all six neighbour classes are kEmpty / kTissue
-constexpr unsigned kMetaAllEmpty = kEmpty | (0x3fu << 2);
-constexpr unsigned kMetaAllTissue = kTissue;
 
 template <typename Real>
 __device__ __forceinline__ unsigned cell_class(Real pw, Real pg)

@@ -1,6 +1,7 @@
 // Kernel launchers of the gbfk library (declarations shared by the C ABI).
 #pragma once
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace gbfk {
@@ -38,6 +39,9 @@ struct PoolView {
 // (kBlockEmpty) or kTissue (kBlockTissue); otherwise the per-cell meta words
 // are read (kBlockMixed).
 constexpr unsigned char kBlockEmpty = 0, kBlockTissue = 1, kBlockMixed = 2;
+// meta words of a cell whose own class and all six neighbour classes are kEmpty / kTissue
+constexpr unsigned kMetaAllEmpty = kEmpty | (0x3fu << 2);
+constexpr unsigned kMetaAllTissue = kTissue;
 
 // One sample of a batch (device pointers).
 template <typename Real>
@@ -77,6 +81,18 @@ template <typename Real>
 cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigned short *meta, const double *ih2,
                            const Real *phi_in, Real *phi_out, Real *dphidt_out, Real rho, double dt,
                            unsigned *nan_flag, cudaStream_t s);
+
+// The same step as a persistent TMA-fed pipeline (gbfk_step_tma.cu): uniform
+// periodic power-of-two grids with identity slots only (tma_step_eligible).
+// maps: the three face-box tensor maps of phi_in (make_pool_tensor_maps);
+// ih2: the grid's 1/(h*h); err_flag: set when a stage wait timed out.
+template <typename Real>
+bool tma_step_eligible(const PoolView<Real> &v);
+template <typename Real>
+cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const Real *H, const unsigned short *meta, double ih2,
+                               const Real *phi_in, Real *phi_out, Real rho, double dt, unsigned *nan_flag,
+                               unsigned *err_flag, const CUtensorMap *maps, cudaStream_t s);
+cudaError_t make_pool_tensor_maps(void *base, int nslots, int real_bytes, CUtensorMap maps[3]);
 
 template <typename Real>
 cudaError_t launch_fill_ghosts(const int *rows, int64_t nrows, const int64_t *row_ptr, const int *src,

@@ -139,6 +139,18 @@ class BlockPool:
         return out
 
     # -- hot path ---------------------------------------------------------
+    @property
+    def step_kernel(self) -> str:
+        """Kernel of the last rd_step: "pipelined" (persistent TMA pipeline,
+        uniform power-of-two grids), "block" (one CTA per block) or "" before
+        any step.  Assign "auto", "block" or "pipelined" to choose."""
+        k = int(self.lib.gbfk_step_kernel(self.ctx))
+        return {v: n for n, v in _lib.STEP_KERNELS.items()}.get(k, "") if k else ""
+
+    @step_kernel.setter
+    def step_kernel(self, kind: str):
+        self._check(self.lib.gbfk_set_step_kernel(self.ctx, _lib.STEP_KERNELS[kind]))
+
     def rd_step(self, Dw, Dg, rho, dt, nsteps: int = 1, check_nan: bool = False):
         self._check(self.lib.gbfk_rd_step(self.ctx, float(Dw), float(Dg), float(rho), float(dt),
                                           int(nsteps), int(bool(check_nan))))

@@ -135,6 +135,21 @@ int gbfk_download_dense(gbfk_ctx *ctx, int field, void *host, int n);
  * synchronises and returns GBFK_E_NAN when phi became NaN/Inf. */
 int gbfk_rd_step(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int nsteps,
                  int check_nan);
+/* Which kernel runs the step (no counterpart in the reference: the
+ * reference has one CPU operator).  GBFK_STEP_AUTO (the default) runs the
+ * persistent TMA-fed pipeline where it applies -- a uniform periodic
+ * power-of-two grid from gbfk_set_uniform -- and the one-CTA-per-block kernel
+ * elsewhere; both give bit-identical results.  GBFK_STEP_PIPELINED on a grid
+ * it does not apply to makes gbfk_rd_step return GBFK_E_STATE.
+ * gbfk_step_kernel reports the kernel of the last gbfk_rd_step (0 before
+ * any).  A pipeline stage whose copies never complete ends its wait after
+ * about a second; gbfk_rd_step with check_nan, or gbfk_sync, then returns
+ * GBFK_E_CUDA. */
+#define GBFK_STEP_AUTO 0
+#define GBFK_STEP_BLOCK 1
+#define GBFK_STEP_PIPELINED 2
+int gbfk_set_step_kernel(gbfk_ctx *ctx, int kind);
+int gbfk_step_kernel(const gbfk_ctx *ctx);
 /* The operator alone: writes dphidt (Real, pool order, nblocks*512 cells) to
  * host memory; phi is unchanged.  (ReactionDiffusionOperator.h:47-138.) */
 int gbfk_rd_rhs(gbfk_ctx *ctx, double Dw, double Dg, double rho, void *host_dphidt);

@@ -168,3 +168,56 @@ def test_fp32_storage_error_vs_fp64(gbfk_lib):
         x, y = a.download_dense("phi"), b.download_dense("phi").astype(np.float64)
     rel = np.linalg.norm(x - y) / np.linalg.norm(x)
     assert rel <= 1e-5
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("n,seed,steps", [(8, 3, 7), (32, 2, 9), (64, 9, 5)])
+def test_pipelined_step_equals_block_step(gbfk_lib, prec, n, seed, steps):
+    """The persistent TMA-fed step and the one-CTA-per-block step on the same
+    uniform power-of-two grid give bit-identical fields after every step, and
+    both equal the oracle: with tumour outside the anatomy (empty blocks with
+    cells inside the domain), negative values and values above 1."""
+    R = np.float64 if prec == "f64" else np.float32
+    pw, pg, c0, _ = make_case(n, seed)
+    rng = np.random.default_rng(seed + 100)
+    c0 = np.maximum(c0, rng.uniform(0, 1, c0.shape) * (rng.uniform(0, 1, c0.shape) < 0.03))
+    c0[0, 0, :] = 1.7
+    c0[1, :, 2] = -0.3
+    pw[n // 2, :, : n // 3] = 0.0
+    pg[n // 2, :, : n // 3] = 0.0
+    pw, pg, c0 = (a.astype(R) for a in (pw, pg, c0))
+    s = make_schedule(0.3, 0.2, 300.0, 25.6, n // 8, prec)
+    with _pool(n, prec, pw, pg, c0) as a, _pool(n, prec, pw, pg, c0) as b:
+        assert a.step_kernel == ""
+        a.step_kernel = "pipelined"
+        b.step_kernel = "block"
+        for _ in range(steps):
+            a.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1, check_nan=True)
+            b.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1, check_nan=True)
+            assert np.array_equal(a.download_dense("phi"), b.download_dense("phi"))
+        assert a.step_kernel == "pipelined" and b.step_kernel == "block"
+        got = a.download_dense("phi")
+    want = O.rd_steps_dense(pw, pg, c0, s.Dw, s.Dg, s.rho, s.h, s.dt, steps)
+    assert np.array_equal(got, want)
+
+
+def test_pipelined_step_kernel_selection(gbfk_lib):
+    """AUTO picks the pipeline on uniform power-of-two grids and the block
+    kernel elsewhere; forcing the pipeline where it does not apply is an
+    error, and the pool stays usable."""
+    pw, pg, c0, _ = make_case(48, 1)
+    s = make_schedule(0.2, 0.05, 300.0, 25.6, 6, "f32")
+    with _pool(48, "f32", *(a.astype(np.float32) for a in (pw, pg, c0))) as pool:
+        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1)
+        assert pool.step_kernel == "block"
+        pool.step_kernel = "pipelined"
+        with pytest.raises(GbfkError) as e:
+            pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1)
+        assert e.value.code == 6
+        pool.step_kernel = "auto"
+        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1, check_nan=True)
+    pw, pg, c0, _ = make_case(32, 1)
+    with _pool(32, "f64", pw, pg, c0) as pool:
+        pool.rd_step(1e-3, 1e-4, 0.1, 0.5, 2, check_nan=True)
+        assert pool.step_kernel == "pipelined"
+        pool.sync()
