@@ -84,6 +84,13 @@ struct gbfk_ctx {
     int step_used = 0;
     bool tma_maps_ready = false;
     CUtensorMap tma_maps[2][3];
+    // the pipelined step's work lists (heavy blocks, then empty blocks), from d_btype
+    int *d_lists = nullptr;
+    int n_heavy = 0, n_empty = 0;
+    bool lists_valid = false;
+    // phi[cur] is the output of a step: every value +0 <= phi <= 1 or NaN
+    // (set only by rd_step; every other writer of phi clears it)
+    bool phi_clamped = false;
 
     // scratch
     unsigned *d_nan = nullptr;        // [0]: NaN seen in a step, [1]: a pipeline stage wait timed out
@@ -136,7 +143,8 @@ void free_topology(gbfk_ctx *c)
 {
     void **ptrs[] = {(void **)&c->d_slot, (void **)&c->d_nbr, &c->d_h, (void **)&c->d_row_ptr, (void **)&c->d_src,
                      &c->d_w, (void **)&c->d_step_rows, (void **)&c->d_all_rows, &c->d_gpw, &c->d_gpg,
-                     &c->d_gphi, (void **)&c->d_fwt, &c->d_H, (void **)&c->d_ih2, (void **)&c->d_btype, &c->d_origin};
+                     &c->d_gphi, (void **)&c->d_fwt, &c->d_H, (void **)&c->d_ih2, (void **)&c->d_btype, &c->d_origin,
+                     (void **)&c->d_lists};
     for (void **p : ptrs) {
         if (*p) cudaFree(*p);
         *p = nullptr;
@@ -148,6 +156,8 @@ void free_topology(gbfk_ctx *c)
     c->h_h.clear();
     c->static_ghosts_dirty = true;
     c->faces_valid = false;
+    c->lists_valid = false;
+    c->phi_clamped = false;
 }
 
 // Something the face coefficients or classes depend on changed.
@@ -222,8 +232,9 @@ int ints_scratch(gbfk_ctx *ctx, size_t n)
     return GBFK_OK;
 }
 
-// The pipelined step's timeout word (d_nan[1]); reading it synchronises the
-// stream.  A timeout is reported once and the word cleared.
+// The pipelined step's error word (d_nan[1]: bit 0 a wait timed out, bit 1 a
+// work list overflowed); reading it synchronises the stream.  An error is
+// reported once and the word cleared.
 int check_stage_timeout(gbfk_ctx *ctx)
 {
     unsigned flag = 0;
@@ -231,7 +242,8 @@ int check_stage_timeout(gbfk_ctx *ctx)
     CK(cudaStreamSynchronize(ctx->stream));
     if (flag) {
         CK(cudaMemsetAsync(ctx->d_nan + 1, 0, sizeof(unsigned), ctx->stream));
-        return fail(ctx, GBFK_E_CUDA, "rd_step: a pipeline stage's copies did not complete within 1 s");
+        return fail(ctx, GBFK_E_CUDA, (flag & 1u) ? "rd_step: a wait of the pipelined step timed out (1 s)"
+                                                  : "rd_step: a CTA's work list of the pipelined step overflowed");
     }
     return GBFK_OK;
 }
@@ -385,9 +397,39 @@ int prepare_static(gbfk_ctx *ctx, double Dw, double Dg)
                               ctx->stream));
         ctx->launches++;
         ctx->faces_valid = true;
+        ctx->lists_valid = false;  // block types recomputed
         ctx->faces_Dw = kDw;
         ctx->faces_Dg = kDg;
     }
+    return GBFK_OK;
+}
+
+// Work lists of the pipelined step from the block types: heavy blocks
+// (entry block * 4 + type; mixed blocks first, then tissue blocks), then
+// empty blocks (entry: block).  Rebuilt whenever the block types change.
+int build_step_lists(gbfk_ctx *ctx)
+{
+    if (ctx->lists_valid) return GBFK_OK;
+    const int nb = ctx->nblocks;
+    std::vector<unsigned char> bt(nb);
+    CK(cudaMemcpyAsync(bt.data(), ctx->d_btype, nb, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<int> lists;
+    lists.reserve(nb);
+    for (int b = 0; b < nb; b++)
+        if (bt[b] == kBlockMixed) lists.push_back(b * 4 + kBlockMixed);
+    for (int b = 0; b < nb; b++)
+        if (bt[b] == kBlockTissue) lists.push_back(b * 4 + kBlockTissue);
+    const int nh = (int)lists.size();
+    for (int b = 0; b < nb; b++)
+        if (bt[b] == kBlockEmpty) lists.push_back(b);
+    if ((int)lists.size() != nb) return fail(ctx, GBFK_E_CUDA, "rd_step: unknown block type");
+    if (!ctx->d_lists) CK(cudaMalloc(&ctx->d_lists, (size_t)nb * sizeof(int)));
+    CK(cudaMemcpyAsync(ctx->d_lists, lists.data(), (size_t)nb * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->n_heavy = nh;
+    ctx->n_empty = nb - nh;
+    ctx->lists_valid = true;
     return GBFK_OK;
 }
 
@@ -408,6 +450,8 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
                 CK(make_pool_tensor_maps(ctx->phi[b], ctx->max_blocks, (int)sizeof(Real), ctx->tma_maps[b]));
             ctx->tma_maps_ready = true;
         }
+        rc = build_step_lists(ctx);
+        if (rc) return rc;
         // uniform grid: one h for every block, as upload_ih2 forms it
         const double h = sizeof(Real) == 8 ? ctx->h_h[0] : (double)(float)ctx->h_h[0];
         ih2 = 1. / (h * h);
@@ -417,8 +461,10 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
         const Real *in = (const Real *)ctx->phi[ctx->cur];
         Real *out = (Real *)ctx->phi[ctx->cur ^ 1];
         if (pipelined) {
-            CK(launch_rd_step_tma<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ih2, in, out, (Real)rho, dt,
-                                        ctx->d_nan, ctx->d_nan + 1, ctx->tma_maps[ctx->cur], ctx->stream));
+            const BlockLists lists = {ctx->d_lists, ctx->n_heavy, ctx->d_lists + ctx->n_heavy, ctx->n_empty};
+            CK(launch_rd_step_tma<Real>(v, lists, (const Real *)ctx->d_H, ctx->d_meta, ih2, in,
+                                        ctx->phi_clamped || s > 0, out, (Real)rho, dt, ctx->d_nan, ctx->d_nan + 1,
+                                        ctx->tma_maps[ctx->cur], ctx->stream));
             ctx->launches++;
             ctx->cur ^= 1;
             continue;
@@ -433,7 +479,10 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
         ctx->launches++;
         ctx->cur ^= 1;
     }
-    if (nsteps > 0) ctx->step_used = pipelined ? GBFK_STEP_PIPELINED : GBFK_STEP_BLOCK;
+    if (nsteps > 0) {
+        ctx->step_used = pipelined ? GBFK_STEP_PIPELINED : GBFK_STEP_BLOCK;
+        ctx->phi_clamped = true;
+    }
     if (check_nan) {
         unsigned flag = 0;
         CK(cudaMemcpyAsync(&flag, ctx->d_nan, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
@@ -502,6 +551,7 @@ int fwt_impl(gbfk_ctx *ctx, double *out)
 template <typename Real>
 int split_impl(gbfk_ctx *ctx, int nsplit, const int *parents, const int *children)
 {
+    ctx->phi_clamped = false;  // the interpolation may leave [0, 1]
     if (!ctx->have_csr && ctx->uniform) {
         int rc = build_uniform_csr(ctx);
         if (rc) return rc;
@@ -534,6 +584,7 @@ int split_impl(gbfk_ctx *ctx, int nsplit, const int *parents, const int *childre
 template <typename Real>
 int collapse_impl(gbfk_ctx *ctx, int n, const int *children, const int *parents)
 {
+    ctx->phi_clamped = false;
     for (int i = 0; i < n; i++) {
         if (parents[i] < 0 || parents[i] >= ctx->max_blocks)
             return fail(ctx, GBFK_E_INVALID, "collapse: parent slot %d out of range", parents[i]);
@@ -779,6 +830,7 @@ int gbfk_set_topology(gbfk_ctx *ctx, const gbfk_blockinfo *blocks, int nblocks, 
 int gbfk_upload_field(gbfk_ctx *ctx, int field, const void *host, int64_t first, int64_t ncells)
 {
     if (!ctx) return GBFK_E_INVALID;
+    if (field == GBFK_PHI) ctx->phi_clamped = false;
     void *p = field_ptr(ctx, field);
     if (!p || !host || first < 0 || ncells < 0 || first + ncells > (int64_t)ctx->max_blocks * kBS3)
         return fail(ctx, GBFK_E_INVALID, "upload_field: bad field or range");
@@ -840,6 +892,7 @@ static int dense_io(gbfk_ctx *ctx, int field, void *host, int n, bool up)
 
 int gbfk_upload_dense(gbfk_ctx *ctx, int field, const void *host, int n)
 {
+    if (ctx && field == GBFK_PHI) ctx->phi_clamped = false;
     return dense_io(ctx, field, const_cast<void *>(host), n, true);
 }
 
@@ -1238,6 +1291,7 @@ extern "C" int gbfk_forward_adjoint(gbfk_ctx *ctx, const gbfk_adjoint_params *p,
                                     void *grad_c0)
 {
     if (!ctx) return GBFK_E_INVALID;
+    ctx->phi_clamped = false;
     if (!p || !out) return fail(ctx, GBFK_E_INVALID, "forward_adjoint: null argument");
     if (!ctx->uniform || !ctx->d_origin) return fail(ctx, GBFK_E_STATE, "forward_adjoint: needs a uniform power-of-two grid");
     if (ctx->obs_n != 8 * ctx->bpd || ctx->nroi) return fail(ctx, GBFK_E_STATE, "forward_adjoint: observations must cover the grid (no ROI)");

@@ -84,14 +84,26 @@ cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigne
 
 // The same step as a persistent TMA-fed pipeline (gbfk_step_tma.cu): uniform
 // periodic power-of-two grids with identity slots only (tma_step_eligible).
-// maps: the three face-box tensor maps of phi_in (make_pool_tensor_maps);
-// ih2: the grid's 1/(h*h); err_flag: set when a stage wait timed out.
+// lists: the blocks that need halos and face coefficients (heavy: entries
+// block * 4 + block type, mixed blocks first) and the empty ones (entries:
+// block), together every block once; maps: the three face-box tensor maps of
+// phi_in (make_pool_tensor_maps); ih2: the grid's 1/(h*h); clamped: phi_in
+// is the output of a step (every value +0 <= phi <= 1 or NaN), which lets
+// the kernel skip the negativity tests; err_flag: set when a wait of the
+// pipeline timed out.
+struct BlockLists {
+    const int *heavy;
+    int n_heavy;
+    const int *empty;
+    int n_empty;
+};
 template <typename Real>
 bool tma_step_eligible(const PoolView<Real> &v);
 template <typename Real>
-cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const Real *H, const unsigned short *meta, double ih2,
-                               const Real *phi_in, Real *phi_out, Real rho, double dt, unsigned *nan_flag,
-                               unsigned *err_flag, const CUtensorMap *maps, cudaStream_t s);
+cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const BlockLists &lists, const Real *H,
+                               const unsigned short *meta, double ih2, const Real *phi_in, bool clamped,
+                               Real *phi_out, Real rho, double dt, unsigned *nan_flag, unsigned *err_flag,
+                               const CUtensorMap *maps, cudaStream_t s);
 cudaError_t make_pool_tensor_maps(void *base, int nslots, int real_bytes, CUtensorMap maps[3]);
 
 template <typename Real>

@@ -3,28 +3,40 @@
 // solve: gbfk_set_uniform).  Results are bit-identical to rd_step_kernel
 // (gbfk_kernels.cu), which stays the step of every other topology.
 //
-// Each CTA owns every G-th block (G CTAs, all resident).  Thread 0 keeps
-// kStages blocks in flight; the CTA's k-th block lands in stage k % kStages:
-//   - the block's phi (cp.async.bulk, 512 Real);
-//   - unless the block is empty (every cell and face-halo cell kEmpty), its
-//     six face halos as tensor boxes of the neighbouring blocks
-//     (cp.async.bulk.tensor.4d on the pool viewed as [slot][z][y][x]; the
-//     x faces as 4-wide boxes so that the inner extent is 16 bytes, the y and
-//     z faces as a row set / a plane), and its 1728 face coefficients
-//     (cp.async.bulk);
-//   - for mixed blocks, its 512 meta words (cp.async.bulk).
-// Every copy of a stage completes on the stage's mbarrier.  All waits are
-// bounded: a stage that does not complete sets the error word and the CTA
-// stops after letting its copies in flight land (also bounded).  The
-// threads compute the block from shared memory with the arithmetic of
-// step_block and store phi; one CTA barrier per block
-// both frees the previous stage for refilling and keeps the timeout
-// decision uniform across the CTA.  No load uses cluster multicast.
+// Work lists.  The host sorts the blocks into a heavy list (mixed, then
+// tissue blocks: everything that needs halos and face coefficients) and an
+// empty list (every cell and face-halo cell kEmpty: only the clamp of the
+// update applies).  CTA c of G (all resident) takes entries c, c + G, ... of
+// each list, so every CTA gets the same number of blocks of each kind, and
+// runs its heavy and empty blocks merged evenly in time (item order by
+// (2j + 1) / n of each list), so that the compute of heavy blocks overlaps
+// the streaming of empty ones.
+//
+// Two rings of shared memory.  A heavy block lands in a heavy slot: its phi
+// (cp.async.bulk), its six face halos as tensor boxes of the neighbouring
+// blocks (cp.async.bulk.tensor.4d on the pool viewed as [slot][z][y][x]; x
+// faces as 4-wide boxes so that the inner extent is 16 bytes, y and z faces
+// as a row set / a plane), its 1728 face coefficients and, for mixed blocks,
+// its meta words.  An empty block's phi (2 KB in FP32) lands in an empty
+// slot.  Warp kWarps is the producer: its lane 0 issues every item in the
+// merged order, each into its ring's next slot once that slot is released,
+// completing on the slot's `full` mbarrier.
+//
+// Consumers.  All kWarps consumer warps compute a heavy block: consumer
+// thread t owns the column x = t % 8, y = (t / 8) % 8 and kCells consecutive
+// z from (t / 64) * kCells (a warp reads 32 consecutive cells of a z plane --
+// no bank conflicts -- and stores 32 consecutive cells); the slot is free
+// when all of them have released it.  Empty block j is computed by warp
+// j % kWarps alone, in 16-byte vectors, and lives in empty slot
+// j % kEmptySlots; kEmptySlots is a multiple of kWarps, so each empty slot
+// serves one warp, which observes every phase of it in order (parity waits
+// stay exact).  All waits are bounded: a wait that gives up sets the error
+// word; the producer lets its copies in flight land (also bounded) before
+// the CTA exits.  No load uses cluster multicast.
 #include <cuda.h>
 
 #include <cstdio>
 #include <cstdlib>
-#include <cstring>
 #include <mutex>
 
 #include "gbfk_exact.cuh"
@@ -33,7 +45,6 @@
 namespace gbfk {
 namespace {
 
-constexpr int kMaxChunk = 4096;  // blocks per CTA (their block-type bytes are staged in shared memory)
 constexpr unsigned long long kWaitNs = 1000000000ull;  // a stage not complete after 1 s is declared lost
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -49,9 +60,9 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
                  : "memory");
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar, uint32_t count)
 {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
 // One try_wait that may suspend the thread until the phase completes, for
@@ -109,10 +120,10 @@ __device__ __forceinline__ void box_g2s(void *dst, const CUtensorMap *map, int c
         : "memory");
 }
 
-// One stage.  Every member starts on a 128-byte boundary (sizes are
-// multiples of 128 bytes for float and double).
+// One slot of the heavy ring.  Every member starts on a 128-byte boundary
+// (sizes are multiples of 128 bytes for float and double).
 template <typename Real>
-struct alignas(128) Stage {
+struct alignas(128) HeavySlot {
     Real in[512];           // the block, [z][y][x]
     Real xm[256], xp[256];  // x faces: [z][y][4] boxes of the x- (x = 4..7) / x+ (x = 0..3) neighbour
     Real ym[64], yp[64];    // y faces [z][x]: row y = 7 of the y- / y = 0 of the y+ neighbour
@@ -120,12 +131,26 @@ struct alignas(128) Stage {
     Real H[kFacesPerBlock];
     unsigned short meta[512];
 };
-static_assert(sizeof(Stage<float>) % 128 == 0 && sizeof(Stage<double>) % 128 == 0, "stage alignment");
+static_assert(sizeof(HeavySlot<float>) % 128 == 0 && sizeof(HeavySlot<double>) % 128 == 0, "slot alignment");
 
-template <typename Real, int kStages>
-constexpr size_t stage_smem()
+constexpr int kMaxItems = 1024;  // heavy + empty blocks of one CTA (staged in shared memory)
+
+// dynamic shared memory: heavy ring, empty ring, barriers, the CTA's items
+template <typename Real, int kHeavySlots, int kEmptySlots>
+struct SmemLayout {
+    static constexpr size_t heavy = 0;
+    static constexpr size_t empty = heavy + (size_t)kHeavySlots * sizeof(HeavySlot<Real>);
+    static constexpr size_t bars = empty + (size_t)kEmptySlots * kBS3 * sizeof(Real);
+    static constexpr size_t items = bars + (8 * (size_t)(2 * kHeavySlots + 2 * kEmptySlots) + 127) / 128 * 128;
+    static constexpr size_t bytes = items + kMaxItems * sizeof(int);
+};
+
+// Merged item order of a CTA: true when item (jh, je) is the heavy one.
+__device__ __forceinline__ bool heavy_next(int jh, int je, int nh, int ne)
 {
-    return kStages * sizeof(Stage<Real>) + 256 + kMaxChunk;
+    if (jh >= nh) return false;
+    if (je >= ne) return true;
+    return (2 * jh + 1) * ne <= (2 * je + 1) * nh;
 }
 
 // same-level periodic neighbour of block blk across face f on a 2^L grid
@@ -157,16 +182,19 @@ __device__ __forceinline__ void pwpg_at(const PoolView<Real> &v, int blk, int x,
     pg = v.pg[g];
 }
 
-// kCells consecutive Real from shared / to global memory in one access
+// N consecutive Real from shared / to global memory in one 16- or 8-byte access
 template <typename Real, int N>
 __device__ __forceinline__ void vec_lds(const Real *src, Real (&d)[N])
 {
-    if constexpr (N * sizeof(Real) == 16) {
+    if constexpr (sizeof(Real) == 4 && N == 4) {
         const float4 a = *reinterpret_cast<const float4 *>(src);
-        memcpy(d, &a, 16);
-    } else if constexpr (N * sizeof(Real) == 8) {
+        d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w;
+    } else if constexpr (sizeof(Real) == 4 && N == 2) {
         const float2 a = *reinterpret_cast<const float2 *>(src);
-        memcpy(d, &a, 8);
+        d[0] = a.x; d[1] = a.y;
+    } else if constexpr (sizeof(Real) == 8 && N == 2) {
+        const double2 a = *reinterpret_cast<const double2 *>(src);
+        d[0] = a.x; d[1] = a.y;
     } else {
 #pragma unroll
         for (int i = 0; i < N; i++) d[i] = src[i];
@@ -176,14 +204,12 @@ __device__ __forceinline__ void vec_lds(const Real *src, Real (&d)[N])
 template <typename Real, int N>
 __device__ __forceinline__ void vec_stg(Real *dst, const Real (&d)[N])
 {
-    if constexpr (N * sizeof(Real) == 16) {
-        float4 a;
-        memcpy(&a, d, 16);
-        *reinterpret_cast<float4 *>(dst) = a;
-    } else if constexpr (N * sizeof(Real) == 8) {
-        float2 a;
-        memcpy(&a, d, 8);
-        *reinterpret_cast<float2 *>(dst) = a;
+    if constexpr (sizeof(Real) == 4 && N == 4) {
+        *reinterpret_cast<float4 *>(dst) = make_float4(d[0], d[1], d[2], d[3]);
+    } else if constexpr (sizeof(Real) == 4 && N == 2) {
+        *reinterpret_cast<float2 *>(dst) = make_float2(d[0], d[1]);
+    } else if constexpr (sizeof(Real) == 8 && N == 2) {
+        *reinterpret_cast<double2 *>(dst) = make_double2(d[0], d[1]);
     } else {
 #pragma unroll
         for (int i = 0; i < N; i++) dst[i] = d[i];
@@ -193,7 +219,10 @@ __device__ __forceinline__ void vec_stg(Real *dst, const Real (&d)[N])
 // The no-flux tests of a cell's six neighbours (x-, x+, y-, y+, z-, z+):
 // low[k] = chf of neighbour k < 0.1, from its class bits in the meta word
 // (kMixed) or, in a tissue block, knowing that every neighbour is kTissue.
-template <typename Real, bool kMixed>
+// A kTissue neighbour with phi >= 0 has chf >= 0.1; so has one whose phi is
+// NaN (the comparison is false), so with kClamped (phi_in holds the output
+// of a step: +0 <= phi <= 1 or NaN) its test needs no evaluation.
+template <typename Real, bool kMixed, bool kClamped>
 __device__ __forceinline__ void neighbour_low(const PoolView<Real> &v, int blk, int x, int y, int z, unsigned mw,
                                               const Real (&phn)[6], bool (&low)[6])
 {
@@ -206,7 +235,7 @@ __device__ __forceinline__ void neighbour_low(const PoolView<Real> &v, int blk, 
             slow = false;
         } else {
             low[kk] = false;
-            slow = (kMixed && ((mw >> (8 + kk)) & 1u)) || !(phn[kk] >= (Real)0);
+            slow = (kMixed && ((mw >> (8 + kk)) & 1u)) || (!kClamped && !(phn[kk] >= (Real)0));
         }
         if (slow) {
             const int nx = x + (kk == 0 ? -1 : kk == 1 ? 1 : 0);
@@ -221,16 +250,19 @@ __device__ __forceinline__ void neighbour_low(const PoolView<Real> &v, int blk, 
 
 // The cells of one thread in a tissue (kMixed = false) or mixed block: its
 // column (x, y) at z = z0 .. z0 + kCells - 1, everything from the stage.
-template <typename Real, int kCells, bool kMixed>
-__device__ __forceinline__ void column_cells(const PoolView<Real> &v, const Stage<Real> &S, int blk, int x, int y,
-                                             int z0, int c0, Real rho, double ih2, double dt, int dt_finite,
+// With kClamped a kTissue cell is inside the domain without a test (phi >= 0;
+// a NaN phi yields NaN either way).
+template <typename Real, int kCells, bool kMixed, bool kClamped>
+__device__ __forceinline__ void column_cells(const PoolView<Real> &v, const HeavySlot<Real> &S, int blk, int x,
+                                             int y, int z0, int c0, Real rho, double ih2, double dt, int dt_finite,
                                              Real (&out)[kCells])
 {
+    const Real *in = S.in;
     Real p[kCells];
     unsigned mw[kCells];
 #pragma unroll
     for (int i = 0; i < kCells; i++) {
-        p[i] = S.in[c0 + 64 * i];
+        p[i] = in[c0 + 64 * i];
         mw[i] = kMixed ? (unsigned)S.meta[c0 + 64 * i] : kMetaAllTissue;
     }
 #pragma unroll
@@ -239,7 +271,7 @@ __device__ __forceinline__ void column_cells(const PoolView<Real> &v, const Stag
         const int z = z0 + i, c = c0 + 64 * i;
         const unsigned cls = mw[i] & 3u;
         bool dom;
-        if (cls == kTissue && phi >= (Real)0) dom = true;
+        if (cls == kTissue && (kClamped || phi >= (Real)0)) dom = true;
         else if (cls == kEmpty) dom = phi > (Real)0;
         else {
             Real pw, pg;
@@ -252,15 +284,22 @@ __device__ __forceinline__ void column_cells(const PoolView<Real> &v, const Stag
         }
         // one shared load per neighbour: interior or face halo by address
         Real phn[6];
-        phn[0] = *(x > 0 ? &S.in[c - 1] : &S.xm[(z * 8 + y) * 4 + 3]);
-        phn[1] = *(x < 7 ? &S.in[c + 1] : &S.xp[(z * 8 + y) * 4]);
-        phn[2] = *(y > 0 ? &S.in[c - 8] : &S.ym[z * 8 + x]);
-        phn[3] = *(y < 7 ? &S.in[c + 8] : &S.yp[z * 8 + x]);
-        phn[4] = i > 0 ? p[i - 1] : *(z > 0 ? &S.in[c - 64] : &S.zm[y * 8 + x]);
-        phn[5] = i < kCells - 1 ? p[i + 1] : *(z < 7 ? &S.in[c + 64] : &S.zp[y * 8 + x]);
-        bool low[6];
-        neighbour_low<Real, kMixed>(v, blk, x, y, z, mw[i], phn, low);
+        phn[0] = *(x > 0 ? &in[c - 1] : &S.xm[(z * 8 + y) * 4 + 3]);
+        phn[1] = *(x < 7 ? &in[c + 1] : &S.xp[(z * 8 + y) * 4]);
+        phn[2] = *(y > 0 ? &in[c - 8] : &S.ym[z * 8 + x]);
+        phn[3] = *(y < 7 ? &in[c + 8] : &S.yp[z * 8 + x]);
+        phn[4] = i > 0 ? p[i - 1] : *(z > 0 ? &in[c - 64] : &S.zm[y * 8 + x]);
+        phn[5] = i < kCells - 1 ? p[i + 1] : *(z < 7 ? &in[c + 64] : &S.zp[y * 8 + x]);
         const int rx = (z * 8 + y) * 9 + x, ry = 576 + (z * 9 + y) * 8 + x, rz = 1152 + (z * 8 + y) * 8 + x;
+        bool low[6];
+        if (!kMixed && (kClamped || (phn[0] >= (Real)0 && phn[1] >= (Real)0 && phn[2] >= (Real)0 &&
+                                     phn[3] >= (Real)0 && phn[4] >= (Real)0 && phn[5] >= (Real)0))) {
+            // kTissue neighbours with phi >= 0: chf >= 0.1, no doubling
+#pragma unroll
+            for (int kk = 0; kk < 6; kk++) low[kk] = false;
+        } else {
+            neighbour_low<Real, kMixed, kClamped>(v, blk, x, y, z, mw[i], phn, low);
+        }
         const Real dphidt = cell_rhs_flags<Real>(S.H[rx], S.H[rx + 1], S.H[ry], S.H[ry + 8], S.H[rz], S.H[rz + 64],
                                                  low, phn, phi, rho, ih2);
         out[i] = cell_update(phi, dphidt, dt);
@@ -295,40 +334,56 @@ __device__ __noinline__ Real empty_cell(const PoolView<Real> &v, int blk, int c,
     return cell_update(phi, dphidt, dt);
 }
 
-// CTA c of G handles blocks c, c + G, c + 2G, ... (interleaved, so that the
-// tissue blocks of the anatomy spread evenly over the CTAs).  Warp kWarps is
-// the producer: its lane 0 refills a stage once every consumer warp has
-// released it (the stage's `empty` barrier) and puts the next block in
-// flight (its `full` barrier).  The kWarps consumer warps never wait for one
-// another: consumer thread t owns the column x = t % 8, y = (t / 8) % 8 and
-// kCells consecutive z from (t / 64) * kCells of every block, waits for the
-// block's stage, computes and stores its cells and releases the stage.  A
-// warp reads 32 consecutive cells of a z plane from shared memory (no bank
-// conflicts) and stores 32 consecutive cells.
-template <typename Real, int kWarps, int kStages>
+// OR of the bit patterns: zero exactly when every value is +0.0
+__device__ __forceinline__ unsigned bits_or(float a) { return __float_as_uint(a); }
+__device__ __forceinline__ unsigned bits_or(double a)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(a);
+    return (unsigned)b | (unsigned)(b >> 32);
+}
+
+template <typename Real, int kWarps, int kHeavySlots, int kEmptySlots, bool kClamped>
 __global__ void __launch_bounds__((kWarps + 1) * 32)
-rd_step_tma_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta, double ih2,
-                   const Real *__restrict__ phi_in, Real *__restrict__ phi_out, Real rho, double dt, int dt_finite,
-                   unsigned *nan_flag, unsigned *err_flag, const __grid_constant__ CUtensorMap map_x,
+rd_step_tma_kernel(PoolView<Real> v, BlockLists lists, const Real *__restrict__ H,
+                   const unsigned short *__restrict__ meta, double ih2, const Real *__restrict__ phi_in,
+                   Real *__restrict__ phi_out, Real rho, double dt, int dt_finite, unsigned *nan_flag,
+                   unsigned *err_flag, const __grid_constant__ CUtensorMap map_x,
                    const __grid_constant__ CUtensorMap map_y, const __grid_constant__ CUtensorMap map_z)
 {
+    using Lay = SmemLayout<Real, kHeavySlots, kEmptySlots>;
     constexpr int kThreads = kWarps * 32;  // consumer threads
     constexpr int kCells = kBS3 / kThreads;
     static_assert(kCells * kThreads == kBS3 && kCells >= 1 && kCells <= 8, "consumer warps per block");
+    static_assert(kEmptySlots % kWarps == 0, "an empty slot must serve one warp");
+    constexpr int kVec = 16 / sizeof(Real);       // cells per 16-byte vector
+    constexpr int kOwnVecs = kBS3 / (32 * kVec);  // vectors per lane of an empty block's warp
     extern __shared__ __align__(128) unsigned char smem[];
-    Stage<Real> *st = reinterpret_cast<Stage<Real> *>(smem);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + kStages * sizeof(Stage<Real>));
-    uint64_t *empty = full + kStages;
-    unsigned char *sbt = smem + kStages * sizeof(Stage<Real>) + 256;
+    HeavySlot<Real> *heavy = reinterpret_cast<HeavySlot<Real> *>(smem + Lay::heavy);
+    Real *empties = reinterpret_cast<Real *>(smem + Lay::empty);
+    uint64_t *hfull = reinterpret_cast<uint64_t *>(smem + Lay::bars);
+    uint64_t *hfree = hfull + kHeavySlots;
+    uint64_t *efull = hfree + kHeavySlots;
+    uint64_t *efree = efull + kEmptySlots;
+    int *items = reinterpret_cast<int *>(smem + Lay::items);
     const int t = threadIdx.x;
-    const int G = gridDim.x;
-    const int nmine = v.nblocks > (int)blockIdx.x ? (v.nblocks - 1 - (int)blockIdx.x) / G + 1 : 0;
-    if (nmine <= 0) return;  // uniform across the CTA
-    for (int i = t; i < nmine; i += blockDim.x) sbt[i] = v.btype[blockIdx.x + i * G];
+    const int c = blockIdx.x, G = gridDim.x;
+    const int nh = lists.n_heavy > c ? (lists.n_heavy - 1 - c) / G + 1 : 0;
+    const int ne = lists.n_empty > c ? (lists.n_empty - 1 - c) / G + 1 : 0;
+    if (nh + ne == 0) return;  // uniform across the CTA
+    if (nh + ne > kMaxItems) {  // the launcher keeps nh + ne in range
+        if (t == 0) atomicOr(err_flag, 2u);
+        return;
+    }
+    for (int i = t; i < nh; i += blockDim.x) items[i] = lists.heavy[c + i * G];
+    for (int i = t; i < ne; i += blockDim.x) items[nh + i] = lists.empty[c + i * G];
     if (t == 0) {
-        for (int s = 0; s < kStages; s++) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], kWarps);
+        for (int i = 0; i < kHeavySlots; i++) {
+            mbar_init(&hfull[i], 1);
+            mbar_init(&hfree[i], kWarps);
+        }
+        for (int i = 0; i < kEmptySlots; i++) {
+            mbar_init(&efull[i], 1);
+            mbar_init(&efree[i], 1);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -338,24 +393,24 @@ rd_step_tma_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned 
     if (t >= kThreads) {
         // producer warp
         if (t != kThreads) return;
-        int issued = 0;
-        for (; issued < nmine; issued++) {
-            const int k = issued, s = k % kStages;
-            if (k >= kStages && !mbar_wait(&empty[s], ((k / kStages) - 1) & 1)) {
-                atomicOr(err_flag, 1u);
-                break;
-            }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            const int blk = blockIdx.x + k * G;
-            Stage<Real> &S = st[s];
-            uint64_t *bar = &full[s];
-            const unsigned char bt = sbt[k];
-            uint32_t bytes = 512 * sizeof(Real);
-            if (bt != kBlockEmpty) bytes += (2 * 256 + 4 * 64 + kFacesPerBlock) * sizeof(Real);
-            if (bt == kBlockMixed) bytes += 512 * sizeof(unsigned short);
-            mbar_arrive_expect_tx(bar, bytes);
-            bulk_g2s(S.in, phi_in + (int64_t)blk * kBS3, 512 * sizeof(Real), bar);
-            if (bt != kBlockEmpty) {
+        int jh = 0, je = 0;  // heavy / empty items put in flight
+        bool ok = true;
+        while (ok && (jh < nh || je < ne)) {
+            if (heavy_next(jh, je, nh, ne)) {
+                const int s = jh % kHeavySlots;
+                if (jh >= kHeavySlots && !mbar_wait(&hfree[s], ((jh / kHeavySlots) - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const int it = items[jh];
+                const int blk = it >> 2, bt = it & 3;
+                HeavySlot<Real> &S = heavy[s];
+                uint64_t *bar = &hfull[s];
+                uint32_t bytes = (kBS3 + 2 * 256 + 4 * 64 + kFacesPerBlock) * sizeof(Real);
+                if (bt == kBlockMixed) bytes += kBS3 * sizeof(unsigned short);
+                mbar_arrive_expect_tx(bar, bytes);
+                bulk_g2s(S.in, phi_in + (int64_t)blk * kBS3, kBS3 * sizeof(Real), bar);
                 box_g2s(S.xm, &map_x, 4, 0, 0, nb_of(blk, L, 0), bar);
                 box_g2s(S.xp, &map_x, 0, 0, 0, nb_of(blk, L, 1), bar);
                 box_g2s(S.ym, &map_y, 0, 7, 0, nb_of(blk, L, 2), bar);
@@ -363,66 +418,120 @@ rd_step_tma_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned 
                 box_g2s(S.zm, &map_z, 0, 0, 7, nb_of(blk, L, 4), bar);
                 box_g2s(S.zp, &map_z, 0, 0, 0, nb_of(blk, L, 5), bar);
                 bulk_g2s(S.H, H + (int64_t)blk * kFacesPerBlock, kFacesPerBlock * sizeof(Real), bar);
+                if (bt == kBlockMixed)
+                    bulk_g2s(S.meta, meta + (int64_t)blk * kBS3, kBS3 * sizeof(unsigned short), bar);
+                jh++;
+            } else {
+                const int s = je % kEmptySlots;
+                if (je >= kEmptySlots && !mbar_wait(&efree[s], ((je / kEmptySlots) - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const int blk = items[nh + je];
+                mbar_arrive_expect_tx(&efull[s], kBS3 * sizeof(Real));
+                bulk_g2s(empties + s * kBS3, phi_in + (int64_t)blk * kBS3, kBS3 * sizeof(Real), &efull[s]);
+                je++;
             }
-            if (bt == kBlockMixed) bulk_g2s(S.meta, meta + (int64_t)blk * kBS3, 512 * sizeof(unsigned short), bar);
         }
+        if (!ok) atomicOr(err_flag, 1u);
         // the CTA's shared memory must outlive every copy in flight (bounded)
-        for (int j = issued - kStages > 0 ? issued - kStages : 0; j < issued; j++)
-            mbar_wait(&full[j % kStages], (j / kStages) & 1);
+        for (int j = jh - kHeavySlots > 0 ? jh - kHeavySlots : 0; j < jh; j++)
+            mbar_wait(&hfull[j % kHeavySlots], (j / kHeavySlots) & 1);
+        for (int j = je - kEmptySlots > 0 ? je - kEmptySlots : 0; j < je; j++)
+            mbar_wait(&efull[j % kEmptySlots], (j / kEmptySlots) & 1);
         return;
     }
 
-    const int lane = t & 31;
+    const int warp = t >> 5, lane = t & 31;
     const int x = t & 7, y = (t >> 3) & 7, z0 = (t >> 6) * kCells;
     const int c0 = x + kBS * (y + kBS * z0);
-    const int ce = t * kCells;  // empty blocks: kCells consecutive cells
     bool bad = false;
-    for (int k = 0; k < nmine; k++) {
-        const int s = k % kStages;
-        if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (k / kStages) & 1))) {
+    int jh = 0, je = warp;  // next heavy item; next empty item of this warp (j % kWarps == warp)
+    while (jh < nh || je < ne) {
+        if (heavy_next(jh, je, nh, ne)) {
+            const int s = jh % kHeavySlots;
+            if (!__all_sync(0xffffffffu, mbar_wait(&hfull[s], (jh / kHeavySlots) & 1))) {
+                if (lane == 0) atomicOr(err_flag, 1u);
+                break;
+            }
+            const int it = items[jh];
+            const int blk = it >> 2;
+            Real out[kCells];
+            if ((it & 3) == kBlockTissue)
+                column_cells<Real, kCells, false, kClamped>(v, heavy[s], blk, x, y, z0, c0, rho, ih2, dt, dt_finite,
+                                                            out);
+            else
+                column_cells<Real, kCells, true, kClamped>(v, heavy[s], blk, x, y, z0, c0, rho, ih2, dt, dt_finite,
+                                                           out);
+            // every shared read of this warp is done: release the slot
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&hfree[s], 1);
+            Real *ob = phi_out + (int64_t)blk * kBS3;
+#pragma unroll
+            for (int i = 0; i < kCells; i++) {
+                bad |= (out[i] != out[i]);
+                ob[c0 + 64 * i] = out[i];
+            }
+            jh++;
+            continue;
+        }
+        const int j = je;
+        je += kWarps;
+        const int s = j % kEmptySlots;
+        if (!__all_sync(0xffffffffu, mbar_wait(&efull[s], (j / kEmptySlots) & 1))) {
             if (lane == 0) atomicOr(err_flag, 1u);
             break;
         }
-        const Stage<Real> &S = st[s];
-        const int blk = blockIdx.x + k * G;
-        const unsigned char bt = sbt[k];
+        const Real *in = empties + s * kBS3;
+        const int blk = items[nh + j];
         Real *ob = phi_out + (int64_t)blk * kBS3;
-        if (bt == kBlockEmpty) {
-            Real p[kCells], out[kCells];
-            vec_lds<Real, kCells>(S.in + ce, p);
-            bool any = false;
+        Real p[kOwnVecs][kVec];
+        unsigned bits = 0;
 #pragma unroll
-            for (int i = 0; i < kCells; i++) any |= p[i] > (Real)0;  // the domain test of a kEmpty cell
-            if (!any) {
+        for (int q = 0; q < kOwnVecs; q++) {
+            vec_lds<Real, kVec>(in + (q * 32 + lane) * kVec, p[q]);
 #pragma unroll
-                for (int i = 0; i < kCells; i++)
-                    out[i] = dt_finite ? clamp01(p[i]) : cell_update(p[i], (Real)0., dt);
-            } else {
-                // tumour outside the anatomy: the stage holds no halo or
-                // coefficients of an empty block, read them from global memory
-#pragma unroll
-                for (int i = 0; i < kCells; i++)
-                    out[i] = empty_cell(v, blk, ce + i, p[i], H, phi_in, rho, ih2, dt, dt_finite);
-            }
+            for (int i = 0; i < kVec; i++) bits |= bits_or(p[q][i]);
+        }
+        if (bits == 0) {
+            // every cell +0.0: outside the domain, and the clamp leaves +0.0
             __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[s]);
+            if (lane == 0) mbar_arrive(&efree[s], 1);
 #pragma unroll
-            for (int i = 0; i < kCells; i++) bad |= (out[i] != out[i]);
-            vec_stg<Real, kCells>(ob + ce, out);
+            for (int q = 0; q < kOwnVecs; q++) vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, p[q]);
             continue;
         }
-        Real out[kCells];
-        if (bt == kBlockTissue)
-            column_cells<Real, kCells, false>(v, S, blk, x, y, z0, c0, rho, ih2, dt, dt_finite, out);
-        else
-            column_cells<Real, kCells, true>(v, S, blk, x, y, z0, c0, rho, ih2, dt, dt_finite, out);
-        // every shared read of this warp is done: release the stage
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
+        bool any = false;
 #pragma unroll
-        for (int i = 0; i < kCells; i++) {
-            bad |= (out[i] != out[i]);
-            ob[c0 + 64 * i] = out[i];
+        for (int q = 0; q < kOwnVecs; q++)
+#pragma unroll
+            for (int i = 0; i < kVec; i++) any |= p[q][i] > (Real)0;  // the domain test of a kEmpty cell
+        if (any) {
+            // tumour outside the anatomy: an empty block's slot holds no halo
+            // or coefficients, read them from global memory (rare)
+#pragma unroll 1
+            for (int q = 0; q < kOwnVecs * kVec; q++) {
+                const int cc = ((q / kVec) * 32 + lane) * kVec + q % kVec;
+                const Real o = empty_cell(v, blk, cc, in[cc], H, phi_in, rho, ih2, dt, dt_finite);
+                bad |= (o != o);
+                ob[cc] = o;
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&efree[s], 1);
+            continue;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&efree[s], 1);
+#pragma unroll
+        for (int q = 0; q < kOwnVecs; q++) {
+            Real o[kVec];
+#pragma unroll
+            for (int i = 0; i < kVec; i++) {
+                o[i] = dt_finite ? clamp01(p[q][i]) : cell_update(p[q][i], (Real)0., dt);
+                bad |= (o[i] != o[i]);
+            }
+            vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, o);
         }
     }
     if (bad) atomicOr(nan_flag, 1u);
@@ -445,6 +554,95 @@ EncodeTiled encode_fn()
             fn = reinterpret_cast<EncodeTiled>(p);
     });
     return fn;
+}
+
+// One launch shape: consumer warps per CTA and slots of the two rings.
+template <typename Real, int kWarps, int kHeavySlots, int kEmptySlots>
+struct Shape {
+    static constexpr int kThreads = (kWarps + 1) * 32;
+    static constexpr size_t kSmem = SmemLayout<Real, kHeavySlots, kEmptySlots>::bytes;
+
+    // resident CTAs on this part, taken once per process
+    static cudaError_t grid(int &g)
+    {
+        static int cached = 0;
+        static std::mutex mu;
+        std::lock_guard<std::mutex> lk(mu);
+        if (!cached) {
+            auto k = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false>;
+            auto kc = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true>;
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+            if (e != cudaSuccess) return e;
+            e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+            if (e != cudaSuccess) return e;
+            int dev = 0, sms = 0, per_sm = 0;
+            if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, kSmem)) != cudaSuccess)
+                return e;
+            cached = sms * (per_sm > 0 ? per_sm : 1);
+        }
+        g = cached;
+        return cudaSuccess;
+    }
+
+    static cudaError_t launch(const PoolView<Real> &v, const BlockLists &lists, const Real *H,
+                              const unsigned short *meta, double ih2, const Real *phi_in, bool clamped,
+                              Real *phi_out, Real rho, double dt, unsigned *nan_flag, unsigned *err_flag,
+                              const CUtensorMap *maps, cudaStream_t s)
+    {
+        int g = 0;
+        cudaError_t e = grid(g);
+        if (e != cudaSuccess) return e;
+        const int n = lists.n_heavy + lists.n_empty;
+        const int nctas = n < g ? n : g;
+        if ((lists.n_heavy + nctas - 1) / nctas + (lists.n_empty + nctas - 1) / nctas > kMaxItems)
+            return cudaErrorInvalidValue;
+        auto k = clamped ? rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true>
+                         : rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false>;
+        k<<<nctas, kThreads, kSmem, s>>>(v, lists, H, meta, ih2, phi_in, phi_out, rho, dt, isfinite(dt) ? 1 : 0,
+                                         nan_flag, err_flag, maps[0], maps[1], maps[2]);
+        return cudaGetLastError();
+    }
+};
+
+// launch shape from GBFK_TMA_SHAPE="consumer warps,heavy slots,empty slots"
+// (a tuning knob), else -1: the default of the Real type (8 warps and 8
+// empty slots; 2 heavy slots in FP32, 1 in FP64: fastest at 256^3)
+int tma_shape_code()
+{
+    static int code = -1;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        if (const char *e = getenv("GBFK_TMA_SHAPE")) {
+            int w = 0, hv = 0, em = 0;
+            if (sscanf(e, "%d,%d,%d", &w, &hv, &em) == 3) code = (w * 10 + hv) * 100 + em;
+        }
+    });
+    return code;
+}
+
+#define GBFK_TMA_SHAPES(X) \
+    X(8, 2, 8)             \
+    X(8, 3, 8)             \
+    X(8, 2, 16)            \
+    X(8, 1, 8)             \
+    X(4, 2, 8)             \
+    X(4, 3, 8)             \
+    X(16, 2, 16)
+
+template <typename Real, typename F>
+cudaError_t with_shape(F &&f)
+{
+#define GBFK_TMA_CASE(W, HV, EM) \
+    case (W * 10 + HV) * 100 + EM: return f(Shape<Real, W, HV, EM>());
+    switch (tma_shape_code()) {
+        GBFK_TMA_SHAPES(GBFK_TMA_CASE)
+    default:
+        if constexpr (sizeof(Real) == 4) return f(Shape<Real, 8, 2, 8>());
+        else return f(Shape<Real, 8, 1, 8>());
+    }
+#undef GBFK_TMA_CASE
 }
 
 }  // namespace
@@ -472,98 +670,39 @@ cudaError_t make_pool_tensor_maps(void *base, int nslots, int real_bytes, CUtens
 }
 
 // Whether the pipelined step applies to a view: uniform periodic 2^L grid,
-// identity slots, and per-CTA block counts that fit the kernel's block-type
-// buffer.
+// identity slots, and at most kMaxItems blocks per CTA whatever the split
+// into heavy and empty blocks.
 template <typename Real>
 bool tma_step_eligible(const PoolView<Real> &v)
 {
-    return v.log2_bpd >= 0 && v.identity_slots && v.nblocks > 0 && v.nblocks <= 148 * kMaxChunk;
+    if (v.log2_bpd < 0 || !v.identity_slots || v.nblocks <= 0) return false;
+    int g = 0;
+    if (with_shape<Real>([&](auto sh) { return decltype(sh)::grid(g); }) != cudaSuccess) return false;
+    return (int64_t)v.nblocks <= (int64_t)g * (kMaxItems - 2);
 }
-
-namespace {
-
-// One launch shape: consumer warps per CTA and stages in flight, with its grid
-// (resident CTAs on this part) taken once per process.
-template <typename Real, int kWarps, int kStages>
-cudaError_t launch_shape(const PoolView<Real> &v, const Real *H, const unsigned short *meta, double ih2,
-                         const Real *phi_in, Real *phi_out, Real rho, double dt, unsigned *nan_flag,
-                         unsigned *err_flag, const CUtensorMap *maps, cudaStream_t s)
-{
-    static int grid = 0;
-    static std::mutex mu;
-    constexpr int kThreads = (kWarps + 1) * 32;
-    auto k = rd_step_tma_kernel<Real, kWarps, kStages>;
-    constexpr size_t smem = stage_smem<Real, kStages>();
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (!grid) {
-            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            int dev = 0, sms = 0, per_sm = 0;
-            if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem)) != cudaSuccess)
-                return e;
-            grid = sms * (per_sm > 0 ? per_sm : 1);
-        }
-    }
-    const int nctas = v.nblocks < grid ? v.nblocks : grid;
-    if ((v.nblocks + nctas - 1) / nctas > kMaxChunk) return cudaErrorInvalidValue;
-    k<<<nctas, kThreads, smem, s>>>(v, H, meta, ih2, phi_in, phi_out, rho, dt, isfinite(dt) ? 1 : 0, nan_flag,
-                                     err_flag, maps[0], maps[1], maps[2]);
-    return cudaGetLastError();
-}
-
-// launch shape from GBFK_TMA_SHAPE="consumer warps,stages" (a tuning knob), else the default
-int tma_shape_code()
-{
-    static int code = -1;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        code = 8 * 10 + 4;
-        if (const char *e = getenv("GBFK_TMA_SHAPE")) {
-            int th = 0, stg = 0;
-            if (sscanf(e, "%d,%d", &th, &stg) == 2) code = th * 10 + stg;
-        }
-    });
-    return code;
-}
-
-}  // namespace
 
 template <typename Real>
-cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const Real *H, const unsigned short *meta, double ih2,
-                               const Real *phi_in, Real *phi_out, Real rho, double dt, unsigned *nan_flag,
-                               unsigned *err_flag, const CUtensorMap *maps, cudaStream_t s)
+cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const BlockLists &lists, const Real *H,
+                               const unsigned short *meta, double ih2, const Real *phi_in, bool clamped,
+                               Real *phi_out, Real rho, double dt, unsigned *nan_flag, unsigned *err_flag,
+                               const CUtensorMap *maps, cudaStream_t s)
 {
-    if (v.nblocks <= 0) return cudaSuccess;
-    if (!tma_step_eligible(v)) return cudaErrorInvalidValue;
-#define GBFK_TMA_SHAPE(TH, ST)                                                                                   \
-    case TH * 10 + ST:                                                                                           \
-        return launch_shape<Real, TH, ST>(v, H, meta, ih2, phi_in, phi_out, rho, dt, nan_flag, err_flag, maps, s);
-    switch (tma_shape_code()) {
-        GBFK_TMA_SHAPE(4, 2)
-        GBFK_TMA_SHAPE(4, 3)
-        GBFK_TMA_SHAPE(4, 4)
-        GBFK_TMA_SHAPE(8, 2)
-        GBFK_TMA_SHAPE(8, 3)
-        GBFK_TMA_SHAPE(8, 6)
-        GBFK_TMA_SHAPE(16, 2)
-        GBFK_TMA_SHAPE(16, 3)
-        GBFK_TMA_SHAPE(16, 4)
-    default:
-        return launch_shape<Real, 8, 4>(v, H, meta, ih2, phi_in, phi_out, rho, dt, nan_flag, err_flag, maps, s);
-    }
-#undef GBFK_TMA_SHAPE
+    if (lists.n_heavy + lists.n_empty <= 0) return cudaSuccess;
+    if (!tma_step_eligible(v) || lists.n_heavy + lists.n_empty != v.nblocks) return cudaErrorInvalidValue;
+    return with_shape<Real>([&](auto sh) {
+        return decltype(sh)::launch(v, lists, H, meta, ih2, phi_in, clamped, phi_out, rho, dt, nan_flag, err_flag,
+                                    maps, s);
+    });
 }
 
 template bool tma_step_eligible<float>(const PoolView<float> &);
 template bool tma_step_eligible<double>(const PoolView<double> &);
-template cudaError_t launch_rd_step_tma<float>(const PoolView<float> &, const float *, const unsigned short *, double,
-                                               const float *, float *, float, double, unsigned *, unsigned *,
-                                               const CUtensorMap *, cudaStream_t);
-template cudaError_t launch_rd_step_tma<double>(const PoolView<double> &, const double *, const unsigned short *,
-                                                double, const double *, double *, double, double, unsigned *,
-                                                unsigned *, const CUtensorMap *, cudaStream_t);
+template cudaError_t launch_rd_step_tma<float>(const PoolView<float> &, const BlockLists &, const float *,
+                                               const unsigned short *, double, const float *, bool, float *, float,
+                                               double, unsigned *, unsigned *, const CUtensorMap *, cudaStream_t);
+template cudaError_t launch_rd_step_tma<double>(const PoolView<double> &, const BlockLists &, const double *,
+                                                const unsigned short *, double, const double *, bool, double *,
+                                                double, double, unsigned *, unsigned *, const CUtensorMap *,
+                                                cudaStream_t);
 
 }  // namespace gbfk

@@ -197,6 +197,12 @@ def test_pipelined_step_equals_block_step(gbfk_lib, prec, n, seed, steps):
             assert np.array_equal(a.download_dense("phi"), b.download_dense("phi"))
         assert a.step_kernel == "pipelined" and b.step_kernel == "block"
         got = a.download_dense("phi")
+        # a field uploaded after steps (negative values again) takes the
+        # pipeline's unclamped path once more
+        for q in (a, b):
+            q.upload_dense("phi", c0)
+            q.rd_step(s.Dw, s.Dg, s.rho, s.dt, 2)
+        assert np.array_equal(a.download_dense("phi"), b.download_dense("phi"))
     want = O.rd_steps_dense(pw, pg, c0, s.Dw, s.Dg, s.rho, s.h, s.dt, steps)
     assert np.array_equal(got, want)
 
