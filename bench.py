@@ -67,11 +67,12 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """dram bytes per launch of the fused kernel from the committed ncu summary."""
+def profiled_traffic(kind):
+    """dram bytes per launch of the step kernel `kind` ("pipelined" / "block")
+    at the default workload, from the committed ncu summary."""
     if not PROFILE_SUMMARY.exists():
         return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", PROFILE_SUMMARY.read_text())
+    m = re.search(r"dram_bytes_per_launch\[%s\]:\s*([0-9.eE+]+)" % kind, PROFILE_SUMMARY.read_text())
     return float(m.group(1)) if m else None
 
 
@@ -379,11 +380,14 @@ def gpu_arm(args):
     kernel_s = (ms / 1e3) / max(launches, 1) if launches == args.steps else (ms / 1e3) / args.steps
     achieved = alg_bytes / kernel_s / 1e9
     peak, peak_kind = measured_peak()
-    traffic = profiled_traffic()
+    traffic = profiled_traffic(pool.step_kernel) if (n, prec) == (N_GRID, "f32") else None
     roofline = {"kernel": KERNEL_NAMES[pool.step_kernel].format(real="float" if prec == "f32" else "double"),
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "algorithmic_bytes_per_launch": alg_bytes}
+                "algorithmic_bytes_per_launch": alg_bytes,
+                # DRAM bytes actually moved (ncu, one launch) over the same launch time:
+                # below the algorithmic bytes because empty blocks read no p_w/p_g
+                "traffic_frac": (traffic / kernel_s / 1e9 / peak) if traffic else None}
 
     # ---- end to end through the public API with host buffers -------------
     e2e_steps = max(1, min(args.steps, 50))
