@@ -184,23 +184,32 @@ def batched_stage(args, stream, local, nsamples=512, bpd=16, seed=1):
     """Config 3: a TMCMC stage of 512 forward solves on 128^3 (FP32, one
     seeded anatomy, Dw log-U[0.02,0.3], rho log-U[0.002,0.2], T U[30,300] d,
     x0 a white-matter voxel), batched vs the same 512 solves one after the
-    other through gbfk_rd_step on one BlockPool.  Returns the JSON record."""
+    other through gbfk_rd_step on one BlockPool.  With several ranks each
+    runs its share of the samples (shard.stage_shards, balanced by steps) and
+    the times are the max over ranks.  Returns the JSON record."""
     import torch
 
     from gliomasolver_b200 import BlockPool
     from gliomasolver_b200.anatomy import make_anatomy, tumor_ic
+    from gliomasolver_b200.shard import max_over_ranks, stage_shards
     from gliomasolver_b200.tmcmc import Batch, sample_stage, to_gbfk_samples
 
     n = 8 * bpd
     p_w, p_g, _ = make_anatomy(n, SEED)
     pw32, pg32 = p_w.astype(np.float32), p_g.astype(np.float32)
-    stage = sample_stage(nsamples, p_w, seed=seed)
+    full = sample_stage(nsamples, p_w, seed=seed)
+    _, full_scheds = to_gbfk_samples(full, bpd, "f32", L_CM)
+    all_steps = np.array([sc.nsteps for sc in full_scheds])
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    mine = stage_shards(all_steps, world)[rank]
+    stage = [full[i] for i in mine]
     samples, scheds = to_gbfk_samples(stage, bpd, "f32", L_CM)
-    steps = np.array([sc.nsteps for sc in scheds])
+    steps = all_steps
     cells = n ** 3
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
 
-    with Batch(bpd, nsamples, "f32", device=local, stream=stream.cuda_stream) as b:
+    with Batch(bpd, max(len(stage), 1), "f32", device=local, stream=stream.cuda_stream) as b:
         b.set_anatomy(0, pw32, pg32)
         b.set_samples(samples)
         l0 = b.launches
@@ -210,7 +219,7 @@ def batched_stage(args, stream, local, nsamples=512, bpd=16, seed=1):
         b.run(0)
         e1.record(stream)
         torch.cuda.synchronize()
-        t_batch = e0.elapsed_time(e1) / 1e3
+        t_batch = max_over_ranks(e0.elapsed_time(e1) / 1e3)
         batch_launches = b.launches - l0
         spc = b.samples_per_cta
 
@@ -227,7 +236,7 @@ def batched_stage(args, stream, local, nsamples=512, bpd=16, seed=1):
             pool.rd_step(sc.Dw, sc.Dg, sc.rho, sc.dt, sc.nsteps)
         e1.record(stream)
         torch.cuda.synchronize()
-        t_seq = e0.elapsed_time(e1) / 1e3
+        t_seq = max_over_ranks(e0.elapsed_time(e1) / 1e3)
 
     return {
         "workload": f"{nsamples} TMCMC samples, {n}^3 uniform, FP32, one seeded anatomy; Dw log-U[0.02,0.3], "
@@ -238,7 +247,7 @@ def batched_stage(args, stream, local, nsamples=512, bpd=16, seed=1):
         "batched_cell_updates_per_s": float(steps.sum()) * cells / t_batch,
         "sequential_s": t_seq, "sequential_samples_per_s": nsamples / t_seq,
         "speedup_vs_sequential": t_seq / t_batch,
-        "samples_per_cta": spc, "batched_launches": batch_launches,
+        "samples_per_cta": spc, "batched_launches": batch_launches, "ranks": world,
         "timing": "CUDA events on the stream: batched = face coefficients + initial conditions + all steps; "
                   "sequential = per sample an H2D of c0, face coefficients and its steps",
     }
@@ -312,6 +321,7 @@ def gpu_arm(args):
 
     from gliomasolver_b200 import BlockPool
     from gliomasolver_b200.build import build_library
+    from gliomasolver_b200.shard import max_over_ranks
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -366,11 +376,7 @@ def gpu_arm(args):
     launches = pool.launches - launches0
     clk = clocks.stop()
     barrier()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1))
     ms_per_step = ms / args.steps
     value = world * cells * args.steps / (ms / 1e3)
 
@@ -406,11 +412,7 @@ def gpu_arm(args):
         pool._check(pool.lib.gbfk_download_dense(pool.ctx, 0, hout.ctypes.data, n))
     e3.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e2.elapsed_time(e3)
-    if world > 1:
-        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3))
     e2e = {"value": world * cells * e2e_steps / (ms_e2e / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": 3 * word * cells, "d2h_bytes_per_step": word * cells,
            "steps": e2e_steps,
