@@ -18,9 +18,11 @@
  * own splitter, no resampling).
  *   ref: each step is the reference's pipeline_process + process
  *        (:176-187, threaded TBB stand-in);
- *   gpu: between adaptations the leaves stay on the device: one upload of
- *        the topology and fields (gbfk_mrag::Device), gbfk_rd_step(every),
- *        one download of phi back into the grid.
+ *   gpu: the leaves stay on the device while the grid does not change: an
+ *        upload of the topology and fields (gbfk_mrag::Device) after each
+ *        refinement, gbfk_rd_step(every), then the wavelet details on the
+ *        device (gbfk_fwt_details); phi goes back to the host grid only when
+ *        some block qualifies for refinement (and at the end).
  * Coefficients: Dw = 0.2 cm^2/day on L = 25.6 cm, Dg = Dw/10, rho = 0.05/day,
  * dt = the reference's CFL formula (:304-307) with h of the finest level.
  *
@@ -170,7 +172,9 @@ int main(int argc, char **argv)
     hashes.push_back(leaves_hash(grid, nb0));
     nblocks.push_back(nb0);
 
-    gbfk_mrag::Device *dev = NULL;
+    /* room for every leaf the finest level allows; created before the
+     * timed loop (context creation is not stepping) */
+    gbfk_mrag::Device *dev = mode == "gpu" ? new gbfk_mrag::Device((1 << (3 * maxLevel)) + 64) : NULL;
     BlockProcessing ref;
     double t_step = 0;
     long long cell_updates = 0;
@@ -178,19 +182,27 @@ int main(int argc, char **argv)
         const int k = std::min(every, nsteps - done);
         std::vector<BlockInfo> vInfo = grid.getBlocksInfo();
         const double t0 = now();
+        bool refine = true;
         if (mode == "ref") {
             for (int s = 0; s < k; s++) ref_step(grid, ref, Dw, Dg, rho, dt);
         } else {
-            /* room for every leaf the finest level allows */
-            if (!dev) dev = new gbfk_mrag::Device((1 << (3 * maxLevel)) + 64);
-            dev->upload(vInfo, grid.getBlockCollection(), grid.getBoundaryInfo());
+            if (!dev->same_leaves(vInfo)) dev->upload(vInfo, grid.getBlockCollection(), grid.getBoundaryInfo());
             gbfk_mrag::check(dev->ctx, gbfk_rd_step(dev->ctx, Dw, Dg, rho, dt, k, 1), "gbfk_rd_step");
-            dev->download_phi(vInfo, grid.getBlockCollection());
+            /* AutomaticRefinement refines the blocks below maxlevel whose
+             * detail is >= the tolerance (MRAGScienceCore.h:59-84); with
+             * the details computed on the device (bit-identical), the
+             * host grid needs phi back only when some block qualifies */
+            std::vector<double> det(vInfo.size());
+            gbfk_mrag::check(dev->ctx, gbfk_fwt_details(dev->ctx, &det[0]), "gbfk_fwt_details");
+            refine = false;
+            for (size_t i = 0; i < vInfo.size(); i++)
+                if (vInfo[i].level < maxLevel && det[i] >= rtol) refine = true;
+            if (refine || done + k >= nsteps) dev->download_phi(vInfo, grid.getBlockCollection());
         }
         t_step += now() - t0;
         cell_updates += (long long)k * (long long)vInfo.size() * 512;
         done += k;
-        Science::AutomaticRefinement<0, 0>(grid, blockfwt, rtol, maxLevel, 1, NULL);
+        if (refine) Science::AutomaticRefinement<0, 0>(grid, blockfwt, rtol, maxLevel, 1, NULL);
         int nb = 0;
         hashes.push_back(leaves_hash(grid, nb));
         nblocks.push_back(nb);

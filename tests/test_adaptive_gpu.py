@@ -64,10 +64,13 @@ def test_block_lists_and_fields_match_the_reference(gbfk_lib, dense_input, tmp_p
 def test_fp32_storage_against_the_fp64_oracle(gbfk_lib, dense_input, tmp_path):
     """FP32 storage on the GPU vs the reference's FP64 run, same schedule:
     the block lists agree and the relative L2 error of phi stays below 1e-5."""
-    ref, a = _run("f64", "ref", dense_input, 400, tmp_path)
-    gpu, b = _run("f32", "gpu", dense_input, 400, tmp_path)
-    assert gpu["blocks"] == ref["blocks"] and gpu["hashes"] == ref["hashes"]
+    ref, a = _run("f64", "ref", dense_input, 2000, tmp_path)
+    gpu, b = _run("f32", "gpu", dense_input, 2000, tmp_path)
+    gpu64, c = _run("f64", "gpu", dense_input, 2000, tmp_path)
     rel = np.linalg.norm(b - a) / np.linalg.norm(a)
-    print(json.dumps({"fp32_vs_fp64_rel_l2": rel, "blocks": ref["blocks"][-1],
-                      "ref_step_s": ref["step_seconds"], "gpu_step_s": gpu["step_seconds"]}))
+    print(json.dumps({"fp32_vs_fp64_rel_l2": rel, "blocks": ref["blocks"], "lists_match": gpu["hashes"] == ref["hashes"],
+                      "ref_f64_step_s": ref["step_seconds"], "gpu_f32_step_s": gpu["step_seconds"],
+                      "gpu_f64_step_s": gpu64["step_seconds"], "cell_updates": ref["cell_updates"]}))
+    assert gpu64["hashes"] == ref["hashes"] and np.array_equal(c, a)
+    assert gpu["hashes"] == ref["hashes"]
     assert rel <= 1e-5
