@@ -7,7 +7,11 @@
 // Here all samples of a stage live in GPU memory and advance together: one
 // launch per time step covers every sample that has not reached its own
 // horizon.  Samples are sorted by step count (longest first), so the active
-// samples of step k are a prefix and retired samples cost nothing.
+// samples of step k are a prefix and retired samples cost nothing.  Fields
+// are stored by that sorted position: position p's pool is blocks
+// p*nblocks .. (p+1)*nblocks-1 of one phi buffer per step parity and of one
+// face-coefficient buffer, so one tensor map per parity covers the halos of
+// every sample (the pipelined step, gbfk_step_tma.cu).
 #include "gbfk.h"
 #include "gbfk_exact.cuh"
 #include "gbfk_kernels.cuh"
@@ -38,7 +42,10 @@ struct gbfk_batch {
     int log2_bpd = -1;
     int *d_nbr = nullptr;
     double *d_ih2 = nullptr;
-    // per anatomy
+    // per anatomy (consecutive pools of pw_all, pg_all, meta_all, btype_all)
+    void *pw_all = nullptr, *pg_all = nullptr;
+    unsigned short *meta_all = nullptr;
+    unsigned char *btype_all = nullptr;
     std::vector<void *> pw, pg;
     std::vector<unsigned short *> meta;
     std::vector<unsigned char *> btype;
@@ -46,12 +53,24 @@ struct gbfk_batch {
     // per sample (in the caller's order)
     int nsamples = 0;
     std::vector<gbfk_sample> params;
-    std::vector<void *> phi0, phi1, H;
-    std::vector<int> order;  // position -> caller's sample index (longest horizon first)
+    // per position (sorted by horizon, longest first)
+    void *phi_all[2] = {nullptr, nullptr};
+    void *H_all = nullptr;
+    std::vector<int> order;  // position -> caller's sample index
+    std::vector<int> pos;    // caller's sample index -> position
     void *d_views = nullptr;
-    unsigned *d_nan = nullptr;
-    double *d_scratch_h = nullptr;  // unused placeholder for alignment of future scratch
-    int chosen_spc = 0;
+    unsigned *d_nan = nullptr;   // per position
+    unsigned *d_err = nullptr;   // the pipelined step's error word
+    // pipelined step: work lists, per-position parameters, tensor maps
+    int *d_lists = nullptr;      // lists, list_off, hpref, epref, anatomy (one allocation)
+    size_t lists_cap = 0;
+    BatchLists bl{};
+    void *d_rho = nullptr;
+    double *d_dt = nullptr;
+    double ih2 = 0;
+    CUtensorMap maps[2][3];
+    bool maps_ready = false;
+    int chosen_spc = 0;          // block kernel: samples per CTA; -1: the pipelined kernel
     int64_t launches = 0;
     std::string err;
 };
@@ -113,51 +132,139 @@ __global__ void ic_kernel(int n, int bpd, const Real *__restrict__ pw, const Rea
     }
 }
 
+// Work lists of the pipelined step: per anatomy in use, its heavy blocks
+// (block * 4 + type, mixed first) and empty blocks from the block types the
+// face kernel wrote; per position its anatomy and the prefix sums of the
+// list lengths.  Call after the face kernels of batch_prepare.
+int batch_lists(gbfk_batch *b)
+{
+    const int nb = b->nblocks, na = b->max_anatomies, ns = b->nsamples;
+    std::vector<int> used(na, 0);
+    for (int k = 0; k < ns; k++) used[b->params[b->order[k]].anatomy] = 1;
+    std::vector<int> lists, off(2 * na, 0), nh(na, 0), ne(na, 0);
+    std::vector<unsigned char> bt(nb);
+    for (int a = 0; a < na; a++) {
+        if (!used[a]) continue;
+        BK(cudaMemcpyAsync(bt.data(), b->btype[a], nb, cudaMemcpyDeviceToHost, b->stream));
+        BK(cudaStreamSynchronize(b->stream));
+        off[2 * a] = (int)lists.size();
+        for (int q = 0; q < nb; q++)
+            if (bt[q] == kBlockMixed) lists.push_back(q * 4 + kBlockMixed);
+        for (int q = 0; q < nb; q++)
+            if (bt[q] == kBlockTissue) lists.push_back(q * 4 + kBlockTissue);
+        nh[a] = (int)lists.size() - off[2 * a];
+        off[2 * a + 1] = (int)lists.size();
+        for (int q = 0; q < nb; q++)
+            if (bt[q] == kBlockEmpty) lists.push_back(q);
+        ne[a] = (int)lists.size() - off[2 * a + 1];
+        if (nh[a] + ne[a] != nb) return bfail(b, GBFK_E_CUDA, "batch: unknown block type");
+    }
+    std::vector<int> hpref(ns + 1, 0), epref(ns + 1, 0), anat(ns);
+    for (int k = 0; k < ns; k++) {
+        anat[k] = b->params[b->order[k]].anatomy;
+        hpref[k + 1] = hpref[k] + nh[anat[k]];
+        epref[k + 1] = epref[k] + ne[anat[k]];
+    }
+    // one allocation: lists | list_off | hpref | epref | anatomy
+    const size_t need = lists.size() + off.size() + 2 * (size_t)(ns + 1) + ns;
+    if (b->lists_cap < need) {
+        if (b->d_lists) cudaFree(b->d_lists);
+        b->d_lists = nullptr;
+        b->lists_cap = 0;
+        BK(cudaMalloc(&b->d_lists, need * sizeof(int)));
+        b->lists_cap = need;
+    }
+    std::vector<int> all;
+    all.reserve(need);
+    all.insert(all.end(), lists.begin(), lists.end());
+    all.insert(all.end(), off.begin(), off.end());
+    all.insert(all.end(), hpref.begin(), hpref.end());
+    all.insert(all.end(), epref.begin(), epref.end());
+    all.insert(all.end(), anat.begin(), anat.end());
+    BK(cudaMemcpyAsync(b->d_lists, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    BK(cudaStreamSynchronize(b->stream));
+    int *d = b->d_lists;
+    b->bl.lists = d;
+    b->bl.list_off = d + lists.size();
+    b->bl.hpref = b->bl.list_off + off.size();
+    b->bl.epref = b->bl.hpref + ns + 1;
+    b->bl.anatomy = b->bl.epref + ns + 1;
+    return GBFK_OK;
+}
+
+template <typename Real>
+Real *pos_field(gbfk_batch *b, void *base, int p, int per_block)
+{
+    return (Real *)base + (int64_t)p * b->nblocks * per_block;
+}
+
 template <typename Real>
 int batch_prepare(gbfk_batch *b)
 {
-    // face coefficients and meta words of every sample's (anatomy, Dw, Dg)
-    for (int s = 0; s < b->nsamples; s++) {
-        const gbfk_sample &p = b->params[s];
-        PoolView<Real> v = batch_pool<Real>(b);
-        v.pw = (const Real *)b->pw[p.anatomy];
-        v.pg = (const Real *)b->pg[p.anatomy];
-        v.btype = b->btype[p.anatomy];
-        BK(launch_faces<Real>(v, (Real)p.Dw, (Real)p.Dg, (Real *)b->H[s], b->meta[p.anatomy], b->btype[p.anatomy],
-                              b->stream));
-        int64_t nb = ((int64_t)b->nblocks * kBS3 + 255) / 256;
-        if (nb > 148 * 32) nb = 148 * 32;
-        ic_kernel<Real><<<(int)nb, 256, 0, b->stream>>>(b->n, b->bpd, v.pw, v.pg, p.x0[0], p.x0[1], p.x0[2],
-                                                         p.sigma, (Real *)b->phi0[s]);
-        BK(cudaGetLastError());
-        b->launches += 2;
-    }
-    // views sorted by horizon
+    // positions: sorted by horizon, longest first
     b->order.resize(b->nsamples);
     std::iota(b->order.begin(), b->order.end(), 0);
     std::stable_sort(b->order.begin(), b->order.end(),
                      [&](int i, int j) { return b->params[i].nsteps > b->params[j].nsteps; });
-    std::vector<SampleView<Real>> views(b->nsamples);
+    b->pos.assign(b->nsamples, 0);
+    for (int k = 0; k < b->nsamples; k++) b->pos[b->order[k]] = k;
+    // face coefficients and meta words of every sample's (anatomy, Dw, Dg);
+    // initial conditions in the parity-0 buffer
     for (int k = 0; k < b->nsamples; k++) {
-        const int s = b->order[k];
-        const gbfk_sample &p = b->params[s];
+        const gbfk_sample &p = b->params[b->order[k]];
+        PoolView<Real> v = batch_pool<Real>(b);
+        v.pw = (const Real *)b->pw[p.anatomy];
+        v.pg = (const Real *)b->pg[p.anatomy];
+        v.btype = b->btype[p.anatomy];
+        BK(launch_faces<Real>(v, (Real)p.Dw, (Real)p.Dg, pos_field<Real>(b, b->H_all, k, kFacesPerBlock),
+                              b->meta[p.anatomy], b->btype[p.anatomy], b->stream));
+        int64_t nb = ((int64_t)b->nblocks * kBS3 + 255) / 256;
+        if (nb > 148 * 32) nb = 148 * 32;
+        ic_kernel<Real><<<(int)nb, 256, 0, b->stream>>>(b->n, b->bpd, v.pw, v.pg, p.x0[0], p.x0[1], p.x0[2],
+                                                         p.sigma, pos_field<Real>(b, b->phi_all[0], k, kBS3));
+        BK(cudaGetLastError());
+        b->launches += 2;
+    }
+    std::vector<SampleView<Real>> views(b->nsamples);
+    std::vector<Real> rho(b->nsamples);
+    std::vector<double> dt(b->nsamples);
+    for (int k = 0; k < b->nsamples; k++) {
+        const gbfk_sample &p = b->params[b->order[k]];
         SampleView<Real> &sv = views[k];
         sv.pw = (const Real *)b->pw[p.anatomy];
         sv.pg = (const Real *)b->pg[p.anatomy];
         sv.btype = b->btype[p.anatomy];
         sv.meta = b->meta[p.anatomy];
-        sv.H = (const Real *)b->H[s];
-        sv.phi0 = (Real *)b->phi0[s];
-        sv.phi1 = (Real *)b->phi1[s];
+        sv.H = pos_field<Real>(b, b->H_all, k, kFacesPerBlock);
+        sv.phi0 = pos_field<Real>(b, b->phi_all[0], k, kBS3);
+        sv.phi1 = pos_field<Real>(b, b->phi_all[1], k, kBS3);
         sv.rho = (Real)p.rho;
         sv.dt = p.dt;
         sv.nsteps = p.nsteps;
+        rho[k] = (Real)p.rho;
+        dt[k] = p.dt;
     }
     BK(cudaMemcpyAsync(b->d_views, views.data(), views.size() * sizeof(SampleView<Real>), cudaMemcpyHostToDevice,
                        b->stream));
+    BK(cudaMemcpyAsync(b->d_rho, rho.data(), rho.size() * sizeof(Real), cudaMemcpyHostToDevice, b->stream));
+    BK(cudaMemcpyAsync(b->d_dt, dt.data(), dt.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream));
     BK(cudaMemsetAsync(b->d_nan, 0, b->max_samples * sizeof(unsigned), b->stream));
+    BK(cudaMemsetAsync(b->d_err, 0, sizeof(unsigned), b->stream));
     BK(cudaStreamSynchronize(b->stream));
-    return GBFK_OK;
+    return b->log2_bpd >= 0 ? batch_lists(b) : GBFK_OK;
+}
+
+// One step of the batch with the chosen kernel: the pipelined step
+// (spc == -1) or the per-block kernel with spc samples per CTA.
+template <typename Real>
+cudaError_t batch_step(gbfk_batch *b, const BatchView<Real> &bv, int nactive, int step, int spc)
+{
+    if (spc > 0) return launch_rd_batch_step<Real>(bv, nactive, step, spc, b->stream);
+    const int par = step & 1;
+    return launch_rd_batch_step_tma<Real>(
+        b->bl, nactive, nactive * b->nblocks, b->log2_bpd, b->nblocks, (const Real *)b->phi_all[par],
+        (Real *)b->phi_all[par ^ 1], (const Real *)b->H_all, (const Real *)b->pw_all, (const Real *)b->pg_all,
+        b->meta_all, (const Real *)b->d_rho, b->d_dt, b->ih2, step > 0, b->d_nan, b->d_err, b->maps[par], b->stream);
 }
 
 template <typename Real>
@@ -165,6 +272,13 @@ int batch_run(gbfk_batch *b, int spc)
 {
     int rc = batch_prepare<Real>(b);
     if (rc) return rc;
+    if (spc == -1 && b->log2_bpd < 0)
+        return bfail(b, GBFK_E_STATE, "batch_run: the pipelined step needs a power-of-two block count per direction");
+    if (b->log2_bpd >= 0 && !b->maps_ready) {
+        for (int q = 0; q < 2; q++)
+            BK(make_pool_tensor_maps(b->phi_all[q], b->max_samples * b->nblocks, (int)sizeof(Real), b->maps[q]));
+        b->maps_ready = true;
+    }
     BatchView<Real> bv;
     bv.pool = batch_pool<Real>(b);
     bv.samples = (const SampleView<Real> *)b->d_views;
@@ -180,20 +294,25 @@ int batch_run(gbfk_batch *b, int spc)
         return nactive;
     };
     int step = 0;
-    // autotuner: samples per CTA in {1, 2, 4}, timed on real steps (the
-    // results do not depend on the choice), 3 steps each after 1 warm-up
+    // autotuner: the pipelined step (power-of-two grids) and the per-block
+    // kernel with 1, 2 or 4 samples per CTA, each timed on 3 real steps
+    // after 1 warm-up (every choice gives the same bits), the fastest kept
     if (spc == 0) {
-        const int cands[3] = {1, 2, 4};
+        std::vector<int> cands;
+        if (b->log2_bpd >= 0) cands.push_back(-1);
+        cands.push_back(1);
+        cands.push_back(2);
+        cands.push_back(4);
         float best = 1e30f;
-        int best_spc = 1;
+        int best_spc = cands[0];
         cudaEvent_t e0, e1;
         BK(cudaEventCreate(&e0));
         BK(cudaEventCreate(&e1));
-        for (int ci = 0; ci < 3 && step + 4 <= maxsteps; ci++) {
-            BK(launch_rd_batch_step<Real>(bv, active_at(step), step, cands[ci], b->stream));
+        for (size_t ci = 0; ci < cands.size() && step + 4 <= maxsteps; ci++) {
+            BK(batch_step<Real>(b, bv, active_at(step), step, cands[ci]));
             step++;
             BK(cudaEventRecord(e0, b->stream));
-            for (int r = 0; r < 3; r++, step++) BK(launch_rd_batch_step<Real>(bv, active_at(step), step, cands[ci], b->stream));
+            for (int r = 0; r < 3; r++, step++) BK(batch_step<Real>(b, bv, active_at(step), step, cands[ci]));
             BK(cudaEventRecord(e1, b->stream));
             BK(cudaEventSynchronize(e1));
             float ms = 0;
@@ -210,10 +329,13 @@ int batch_run(gbfk_batch *b, int spc)
     }
     b->chosen_spc = spc;
     for (; step < maxsteps; step++) {
-        BK(launch_rd_batch_step<Real>(bv, active_at(step), step, spc, b->stream));
+        BK(batch_step<Real>(b, bv, active_at(step), step, spc));
         b->launches++;
     }
     BK(cudaStreamSynchronize(b->stream));
+    unsigned err = 0;
+    BK(cudaMemcpy(&err, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (err) return bfail(b, GBFK_E_CUDA, "batch_run: a wait of the pipelined step timed out (1 s)");
     std::vector<unsigned> flags(b->nsamples);
     BK(cudaMemcpy(flags.data(), b->d_nan, b->nsamples * sizeof(unsigned), cudaMemcpyDeviceToHost));
     for (int k = 0; k < b->nsamples; k++)
@@ -270,39 +392,40 @@ int gbfk_batch_create(const gbfk_config *cfg, int bpd, int max_samples, int max_
                 q[4] = id(bx, by, bz - 1); q[5] = id(bx, by, bz + 1);
             }
     const double h = b->precision == GBFK_F64 ? 1.0 / (8.0 * bpd) : (double)(float)(1.0 / (8.0 * bpd));
-    std::vector<double> ih2(nb, 1. / (h * h));
+    b->ih2 = 1. / (h * h);
+    std::vector<double> ih2(nb, b->ih2);
     const size_t field = (size_t)nb * kBS3 * b->rsize;
     if (cudaMalloc(&b->d_nbr, nbr.size() * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_ih2, nb * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&b->d_views, (size_t)max_samples * sizeof(SampleView<double>)) != cudaSuccess ||
-        cudaMalloc(&b->d_nan, (size_t)max_samples * sizeof(unsigned)) != cudaSuccess) {
+        cudaMalloc(&b->d_nan, (size_t)max_samples * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&b->d_err, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&b->d_rho, (size_t)max_samples * b->rsize) != cudaSuccess ||
+        cudaMalloc((void **)&b->d_dt, (size_t)max_samples * sizeof(double)) != cudaSuccess) {
         cudaGetLastError();
         return bail(GBFK_E_OOM);
     }
     cudaMemcpy(b->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(b->d_ih2, ih2.data(), nb * sizeof(double), cudaMemcpyHostToDevice);
+    const size_t na = (size_t)max_anatomies, ns = (size_t)max_samples;
+    if (cudaMalloc(&b->pw_all, na * field) != cudaSuccess || cudaMalloc(&b->pg_all, na * field) != cudaSuccess ||
+        cudaMalloc(&b->meta_all, na * nb * kBS3 * sizeof(unsigned short)) != cudaSuccess ||
+        cudaMalloc(&b->btype_all, na * nb) != cudaSuccess || cudaMalloc(&b->phi_all[0], ns * field) != cudaSuccess ||
+        cudaMalloc(&b->phi_all[1], ns * field) != cudaSuccess ||
+        cudaMalloc(&b->H_all, ns * nb * kFacesPerBlock * b->rsize) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(GBFK_E_OOM);
+    }
     b->pw.assign(max_anatomies, nullptr);
     b->pg.assign(max_anatomies, nullptr);
     b->meta.assign(max_anatomies, nullptr);
     b->btype.assign(max_anatomies, nullptr);
     b->anatomy_set.assign(max_anatomies, false);
     for (int a = 0; a < max_anatomies; a++) {
-        if (cudaMalloc(&b->pw[a], field) != cudaSuccess || cudaMalloc(&b->pg[a], field) != cudaSuccess ||
-            cudaMalloc(&b->meta[a], (size_t)nb * kBS3 * sizeof(unsigned short)) != cudaSuccess ||
-            cudaMalloc(&b->btype[a], (size_t)nb) != cudaSuccess) {
-            cudaGetLastError();
-            return bail(GBFK_E_OOM);
-        }
-    }
-    b->phi0.assign(max_samples, nullptr);
-    b->phi1.assign(max_samples, nullptr);
-    b->H.assign(max_samples, nullptr);
-    for (int s = 0; s < max_samples; s++) {
-        if (cudaMalloc(&b->phi0[s], field) != cudaSuccess || cudaMalloc(&b->phi1[s], field) != cudaSuccess ||
-            cudaMalloc(&b->H[s], (size_t)nb * kFacesPerBlock * b->rsize) != cudaSuccess) {
-            cudaGetLastError();
-            return bail(GBFK_E_OOM);
-        }
+        b->pw[a] = (char *)b->pw_all + a * field;
+        b->pg[a] = (char *)b->pg_all + a * field;
+        b->meta[a] = b->meta_all + (size_t)a * nb * kBS3;
+        b->btype[a] = b->btype_all + (size_t)a * nb;
     }
     *out = b;
     return GBFK_OK;
@@ -313,14 +436,9 @@ int gbfk_batch_destroy(gbfk_batch *b)
     if (!b) return GBFK_OK;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
-    for (auto *v : {&b->pw, &b->pg, &b->phi0, &b->phi1, &b->H})
-        for (void *p : *v)
-            if (p) cudaFree(p);
-    for (auto p : b->meta)
-        if (p) cudaFree(p);
-    for (auto p : b->btype)
-        if (p) cudaFree(p);
-    void *ptrs[] = {b->d_nbr, b->d_ih2, b->d_views, b->d_nan};
+    void *ptrs[] = {b->d_nbr,       b->d_ih2,    b->d_views, b->d_nan,      b->d_err,     b->d_rho, b->d_dt,
+                    b->d_lists,     b->pw_all,   b->pg_all,  b->meta_all,   b->btype_all, b->phi_all[0],
+                    b->phi_all[1],  b->H_all};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -380,8 +498,9 @@ int gbfk_batch_set_samples(gbfk_batch *b, int nsamples, const gbfk_sample *sampl
 int gbfk_batch_run(gbfk_batch *b, int samples_per_cta)
 {
     if (!b) return GBFK_E_INVALID;
-    if (samples_per_cta != 0 && samples_per_cta != 1 && samples_per_cta != 2 && samples_per_cta != 4)
-        return bfail(b, GBFK_E_INVALID, "samples_per_cta must be 0 (autotune), 1, 2 or 4");
+    if (samples_per_cta != -1 && samples_per_cta != 0 && samples_per_cta != 1 && samples_per_cta != 2 &&
+        samples_per_cta != 4)
+        return bfail(b, GBFK_E_INVALID, "samples_per_cta must be 0 (autotune), -1 (pipelined), 1, 2 or 4");
     BK(cudaSetDevice(b->device));
     return b->precision == GBFK_F64 ? batch_run<double>(b, samples_per_cta) : batch_run<float>(b, samples_per_cta);
 }
@@ -396,7 +515,9 @@ int gbfk_batch_download(gbfk_batch *b, int sample, void *dense_out)
     const size_t bytes = (size_t)b->n * b->n * b->n * b->rsize;
     void *stage = nullptr;
     BK(cudaMalloc(&stage, bytes));
-    const void *src = (b->params[sample].nsteps & 1) ? b->phi1[sample] : b->phi0[sample];
+    if (b->pos.size() != (size_t)b->nsamples) return bfail(b, GBFK_E_STATE, "download: the batch has not run");
+    const size_t field = (size_t)b->nblocks * kBS3 * b->rsize;
+    const void *src = (const char *)b->phi_all[b->params[sample].nsteps & 1] + (size_t)b->pos[sample] * field;
     cudaError_t e = b->precision == GBFK_F64
                         ? launch_dense_scatter<double>((const double *)src, (double *)stage, b->n, false, b->stream)
                         : launch_dense_scatter<float>((const float *)src, (float *)stage, b->n, false, b->stream);

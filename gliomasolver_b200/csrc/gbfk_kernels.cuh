@@ -106,6 +106,27 @@ cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const BlockLists &lists,
                                const CUtensorMap *maps, cudaStream_t s);
 cudaError_t make_pool_tensor_maps(void *base, int nslots, int real_bytes, CUtensorMap maps[3]);
 
+// The same for a step of a TMCMC batch: every active sample (positions
+// 0 .. nactive-1) of one uniform 2^log2_bpd grid.  Per-position fields are
+// consecutive pools of nblocks blocks (phi_in/phi_out, H); per-anatomy ones
+// too (pw, pg, meta).  bl: per-anatomy heavy/empty block lists and the
+// prefix sums of their lengths over the positions; total_items = blocks of
+// all active samples; rho, dt, nan_flags per position; maps: the face-box
+// tensor maps of the phi_in buffer (all positions).
+struct BatchLists {
+    const int *lists;     // per anatomy: heavy entries (block * 4 + type), then empty entries (block)
+    const int *list_off;  // [2a]: offset of anatomy a's heavy entries, [2a + 1]: of its empty entries
+    const int *hpref;     // [positions + 1]: heavy blocks of positions before p
+    const int *epref;     // [positions + 1]: empty blocks of positions before p
+    const int *anatomy;   // [positions]
+};
+template <typename Real>
+cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int total_items, int log2_bpd,
+                                     int nblocks, const Real *phi_in, Real *phi_out, const Real *H, const Real *pw,
+                                     const Real *pg, const unsigned short *meta, const Real *rho, const double *dt,
+                                     double ih2, bool clamped, unsigned *nan_flags, unsigned *err_flag,
+                                     const CUtensorMap *maps, cudaStream_t s);
+
 template <typename Real>
 cudaError_t launch_fill_ghosts(const int *rows, int64_t nrows, const int64_t *row_ptr, const int *src,
                                const Real *w, const Real *field, Real *ghosts, cudaStream_t s);

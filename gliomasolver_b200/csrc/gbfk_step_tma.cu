@@ -1,32 +1,37 @@
 // The fused RD step as a persistent, TMA-fed pipeline, for uniform periodic
-// power-of-two grids whose blocks sit in pool slots 0..n-1 (the resident
-// solve: gbfk_set_uniform).  Results are bit-identical to rd_step_kernel
-// (gbfk_kernels.cu), which stays the step of every other topology.
+// power-of-two grids whose blocks sit in consecutive pool slots: one solve
+// (gbfk_set_uniform; gbfk_rd_step) or every active sample of a TMCMC batch
+// (gbfk_batch_run).  Results are bit-identical to rd_step_kernel and
+// rd_batch_step_kernel (gbfk_kernels.cu), which step every other topology.
 //
-// Work lists.  The host sorts the blocks into a heavy list (mixed, then
-// tissue blocks: everything that needs halos and face coefficients) and an
-// empty list (every cell and face-halo cell kEmpty: only the clamp of the
-// update applies).  CTA c of G (all resident) takes entries c, c + G, ... of
-// each list, so every CTA gets the same number of blocks of each kind, and
-// runs its heavy and empty blocks merged evenly in time (item order by
-// (2j + 1) / n of each list), so that the compute of heavy blocks overlaps
-// the streaming of empty ones.
+// Work items.  An item is one block of one sample.  Heavy items (mixed and
+// tissue blocks: they need halos and face coefficients) and empty items
+// (every cell and face-halo cell kEmpty: only the clamp of the update
+// applies) are numbered globally by a work source (PoolSource: the host's
+// block lists of one solve; BatchSource: per-anatomy block lists
+// concatenated over the active samples).  CTA c of G (all resident) takes
+// global items c, c + G, ... of each kind, so every CTA gets the same number
+// of items of each kind, and runs its heavy and empty items merged evenly in
+// time (order by (2j + 1) / n within each kind), so that the compute of
+// heavy blocks overlaps the streaming of empty ones.
 //
-// Two rings of shared memory.  A heavy block lands in a heavy slot: its phi
+// Two rings of shared memory.  A heavy item lands in a heavy slot: its phi
 // (cp.async.bulk), its six face halos as tensor boxes of the neighbouring
-// blocks (cp.async.bulk.tensor.4d on the pool viewed as [slot][z][y][x]; x
-// faces as 4-wide boxes so that the inner extent is 16 bytes, y and z faces
-// as a row set / a plane), its 1728 face coefficients and, for mixed blocks,
-// its meta words.  An empty block's phi (2 KB in FP32) lands in an empty
-// slot.  Warp kWarps is the producer: its lane 0 issues every item in the
-// merged order, each into its ring's next slot once that slot is released,
-// completing on the slot's `full` mbarrier.
+// blocks (cp.async.bulk.tensor.4d on the pool viewed as [slot][z][y][x],
+// slot = sample * blocks + block; x faces as 4-wide boxes so that the inner
+// extent is 16 bytes, y and z faces as a row set / a plane), its 1728 face
+// coefficients and, for mixed blocks, its meta words.  An empty item's phi
+// (2 KB in FP32) lands in an empty slot.  Warp kWarps is the producer: its
+// 32 lanes decode the next 32 items of each kind in parallel, and lane 0
+// issues every item in the merged order into its ring's next slot once that
+// slot is released, with a (sample, block) header, completing on the slot's
+// `full` mbarrier.
 //
-// Consumers.  All kWarps consumer warps compute a heavy block: consumer
+// Consumers.  All kWarps consumer warps compute a heavy item: consumer
 // thread t owns the column x = t % 8, y = (t / 8) % 8 and kCells consecutive
 // z from (t / 64) * kCells (a warp reads 32 consecutive cells of a z plane --
 // no bank conflicts -- and stores 32 consecutive cells); the slot is free
-// when all of them have released it.  Empty block j is computed by warp
+// when all of them have released it.  Empty item j is computed by warp
 // j % kWarps alone, in 16-byte vectors, and lives in empty slot
 // j % kEmptySlots; kEmptySlots is a multiple of kWarps, so each empty slot
 // serves one warp, which observes every phase of it in order (parity waits
@@ -133,16 +138,21 @@ struct alignas(128) HeavySlot {
 };
 static_assert(sizeof(HeavySlot<float>) % 128 == 0 && sizeof(HeavySlot<double>) % 128 == 0, "slot alignment");
 
-constexpr int kMaxItems = 1024;  // heavy + empty blocks of one CTA (staged in shared memory)
+// What the producer tells the consumers about the item in a slot: its
+// sample position, block * 4 + block type, and the sample's dt and rho.
+struct alignas(16) SlotHdr {
+    double dt, rho;
+    int p, e;
+};
 
-// dynamic shared memory: heavy ring, empty ring, barriers, the CTA's items
+// dynamic shared memory: heavy ring, empty ring, barriers, slot headers
 template <typename Real, int kHeavySlots, int kEmptySlots>
 struct SmemLayout {
     static constexpr size_t heavy = 0;
     static constexpr size_t empty = heavy + (size_t)kHeavySlots * sizeof(HeavySlot<Real>);
     static constexpr size_t bars = empty + (size_t)kEmptySlots * kBS3 * sizeof(Real);
-    static constexpr size_t items = bars + (8 * (size_t)(2 * kHeavySlots + 2 * kEmptySlots) + 127) / 128 * 128;
-    static constexpr size_t bytes = items + kMaxItems * sizeof(int);
+    static constexpr size_t hdr = bars + (8 * (size_t)(2 * kHeavySlots + 2 * kEmptySlots) + 127) / 128 * 128;
+    static constexpr size_t bytes = hdr + sizeof(SlotHdr) * (size_t)(kHeavySlots + kEmptySlots);
 };
 
 // Merged item order of a CTA: true when item (jh, je) is the heavy one.
@@ -150,7 +160,7 @@ __device__ __forceinline__ bool heavy_next(int jh, int je, int nh, int ne)
 {
     if (jh >= nh) return false;
     if (je >= ne) return true;
-    return (2 * jh + 1) * ne <= (2 * je + 1) * nh;
+    return (int64_t)(2 * jh + 1) * ne <= (int64_t)(2 * je + 1) * nh;
 }
 
 // same-level periodic neighbour of block blk across face f on a 2^L grid
@@ -163,23 +173,6 @@ __device__ __forceinline__ int nb_of(int blk, int L, int f)
     else if (d == 1) by = (by + s) & m;
     else bz = (bz + s) & m;
     return bx | (by << L) | (bz << (2 * L));
-}
-
-// p_w, p_g of lab cell (x, y, z) of block blk: the interior or one face halo
-template <typename Real>
-__device__ __forceinline__ void pwpg_at(const PoolView<Real> &v, int blk, int x, int y, int z, Real &pw, Real &pg)
-{
-    const int L = v.log2_bpd;
-    int b = blk;
-    if (x < 0) { b = nb_of(blk, L, 0); x += 8; }
-    else if (x > 7) { b = nb_of(blk, L, 1); x -= 8; }
-    else if (y < 0) { b = nb_of(blk, L, 2); y += 8; }
-    else if (y > 7) { b = nb_of(blk, L, 3); y -= 8; }
-    else if (z < 0) { b = nb_of(blk, L, 4); z += 8; }
-    else if (z > 7) { b = nb_of(blk, L, 5); z -= 8; }
-    const int64_t g = (int64_t)b * kBS3 + x + kBS * (y + kBS * z);
-    pw = v.pw[g];
-    pg = v.pg[g];
 }
 
 // N consecutive Real from shared / to global memory in one 16- or 8-byte access
@@ -216,14 +209,127 @@ __device__ __forceinline__ void vec_stg(Real *dst, const Real (&d)[N])
     }
 }
 
+// The fields of one sample that the rare slow paths read from global
+// memory: its anatomy (p_w, p_g), its phi and face coefficients.
+template <typename Real>
+struct ItemCtx {
+    const Real *pw, *pg, *phi_in, *H;  // pool order, block 0 of the sample
+    int L;                             // log2 of the blocks per direction
+};
+
+// p_w, p_g of lab cell (x, y, z) of block blk: the interior or one face halo
+template <typename Real>
+__device__ __forceinline__ void pwpg_at(const ItemCtx<Real> &v, int blk, int x, int y, int z, Real &pw, Real &pg)
+{
+    const int L = v.L;
+    int b = blk;
+    if (x < 0) { b = nb_of(blk, L, 0); x += 8; }
+    else if (x > 7) { b = nb_of(blk, L, 1); x -= 8; }
+    else if (y < 0) { b = nb_of(blk, L, 2); y += 8; }
+    else if (y > 7) { b = nb_of(blk, L, 3); y -= 8; }
+    else if (z < 0) { b = nb_of(blk, L, 4); z += 8; }
+    else if (z > 7) { b = nb_of(blk, L, 5); z -= 8; }
+    const int64_t g = (int64_t)b * kBS3 + x + kBS * (y + kBS * z);
+    pw = v.pw[g];
+    pg = v.pg[g];
+}
+
+// Work source of one solve: the host-built block lists (heavy entries
+// block * 4 + type, mixed blocks first; empty entries block).
+template <typename Real>
+struct PoolSource {
+    const int *heavy, *empty;
+    int nh, ne;
+    const Real *phi_in;
+    Real *phi_out;
+    const Real *H, *pw, *pg;
+    const unsigned short *meta;
+    Real rho;
+    double dt;
+    int L, nblocks;
+    unsigned *nan_flag;
+
+    __device__ int total_heavy() const { return nh; }
+    __device__ int total_empty() const { return ne; }
+    __device__ void heavy_item(int g, int &p, int &e) const { p = 0; e = heavy[g]; }
+    __device__ void empty_item(int g, int &p, int &e) const { p = 0; e = empty[g] * 4; }
+    __device__ void params(int, double &r, double &d) const { r = (double)rho; d = dt; }
+    __device__ const unsigned short *meta_of(int) const { return meta; }
+    __device__ const Real *H_of(int) const { return H; }
+    __device__ int64_t slot0(int) const { return 0; }
+    __device__ ItemCtx<Real> ctx(int) const { return ItemCtx<Real>{pw, pg, phi_in, H, L}; }
+    __device__ Real rho_of(int) const { return rho; }
+    __device__ double dt_of(int) const { return dt; }
+    __device__ unsigned *nan_of(int) const { return nan_flag; }
+};
+
+// Work source of a TMCMC batch step: the active samples (positions
+// 0 .. nactive-1, longest horizon first) with their per-anatomy block lists;
+// hpref / epref are prefix sums of the heavy / empty block counts over the
+// positions.  Sample p's pool starts at block p * nblocks of the phi buffers
+// and of the face coefficients.
+template <typename Real>
+struct BatchSource {
+    const int *lists;       // per anatomy a: heavy entries at list_off[2a], empty entries at list_off[2a + 1]
+    const int *list_off;
+    const int *hpref, *epref;
+    const int *anatomy;     // per position
+    int nactive;
+    const Real *phi_in;
+    Real *phi_out;
+    const Real *H;          // all positions
+    const Real *pw, *pg;    // all anatomies
+    const unsigned short *meta;
+    const Real *rho;        // per position
+    const double *dt;       // per position
+    int L, nblocks;
+    unsigned *nan_flags;    // per position
+
+    __device__ int total_heavy() const { return hpref[nactive]; }
+    __device__ int total_empty() const { return epref[nactive]; }
+    // position p with pref[p] <= g < pref[p + 1]
+    __device__ static int position(const int *pref, int n, int g)
+    {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pref[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        return lo;
+    }
+    __device__ void heavy_item(int g, int &p, int &e) const
+    {
+        p = position(hpref, nactive, g);
+        e = lists[list_off[2 * anatomy[p]] + (g - hpref[p])];
+    }
+    __device__ void empty_item(int g, int &p, int &e) const
+    {
+        p = position(epref, nactive, g);
+        e = lists[list_off[2 * anatomy[p] + 1] + (g - epref[p])] * 4;
+    }
+    __device__ void params(int p, double &r, double &d) const { r = (double)rho[p]; d = dt[p]; }
+    __device__ const unsigned short *meta_of(int p) const { return meta + (int64_t)anatomy[p] * nblocks * kBS3; }
+    __device__ const Real *H_of(int p) const { return H + (int64_t)p * nblocks * kFacesPerBlock; }
+    __device__ int64_t slot0(int p) const { return (int64_t)p * nblocks; }
+    __device__ ItemCtx<Real> ctx(int p) const
+    {
+        const int64_t a = (int64_t)anatomy[p] * nblocks * kBS3;
+        return ItemCtx<Real>{pw + a, pg + a, phi_in + (int64_t)p * nblocks * kBS3, H_of(p), L};
+    }
+    __device__ Real rho_of(int p) const { return rho[p]; }
+    __device__ double dt_of(int p) const { return dt[p]; }
+    __device__ unsigned *nan_of(int p) const { return nan_flags + p; }
+};
+
 // The no-flux tests of a cell's six neighbours (x-, x+, y-, y+, z-, z+):
 // low[k] = chf of neighbour k < 0.1, from its class bits in the meta word
 // (kMixed) or, in a tissue block, knowing that every neighbour is kTissue.
 // A kTissue neighbour with phi >= 0 has chf >= 0.1; so has one whose phi is
 // NaN (the comparison is false), so with kClamped (phi_in holds the output
 // of a step: +0 <= phi <= 1 or NaN) its test needs no evaluation.
-template <typename Real, bool kMixed, bool kClamped>
-__device__ __forceinline__ void neighbour_low(const PoolView<Real> &v, int blk, int x, int y, int z, unsigned mw,
+template <typename Real, bool kMixed, bool kClamped, typename Source>
+__device__ __forceinline__ void neighbour_low(const Source &src, int sp, int blk, int x, int y, int z, unsigned mw,
                                               const Real (&phn)[6], bool (&low)[6])
 {
     const Real eps = (Real)0.1;
@@ -242,7 +348,7 @@ __device__ __forceinline__ void neighbour_low(const PoolView<Real> &v, int blk, 
             const int ny = y + (kk == 2 ? -1 : kk == 3 ? 1 : 0);
             const int nz = z + (kk == 4 ? -1 : kk == 5 ? 1 : 0);
             Real pw, pg;
-            pwpg_at(v, blk, nx, ny, nz, pw, pg);
+            pwpg_at(src.ctx(sp), blk, nx, ny, nz, pw, pg);
             low[kk] = domain_chf(phn[kk], pw, pg) < eps;
         }
     }
@@ -251,9 +357,10 @@ __device__ __forceinline__ void neighbour_low(const PoolView<Real> &v, int blk, 
 // The cells of one thread in a tissue (kMixed = false) or mixed block: its
 // column (x, y) at z = z0 .. z0 + kCells - 1, everything from the stage.
 // With kClamped a kTissue cell is inside the domain without a test (phi >= 0;
-// a NaN phi yields NaN either way).
-template <typename Real, int kCells, bool kMixed, bool kClamped>
-__device__ __forceinline__ void column_cells(const PoolView<Real> &v, const HeavySlot<Real> &S, int blk, int x,
+// a NaN phi yields NaN either way).  sp: the item's sample position, whose
+// fields the rare slow paths read from global memory.
+template <typename Real, int kCells, bool kMixed, bool kClamped, typename Source>
+__device__ __forceinline__ void column_cells(const Source &src, int sp, const HeavySlot<Real> &S, int blk, int x,
                                              int y, int z0, int c0, Real rho, double ih2, double dt, int dt_finite,
                                              Real (&out)[kCells])
 {
@@ -275,7 +382,7 @@ __device__ __forceinline__ void column_cells(const PoolView<Real> &v, const Heav
         else if (cls == kEmpty) dom = phi > (Real)0;
         else {
             Real pw, pg;
-            pwpg_at(v, blk, x, y, z, pw, pg);
+            pwpg_at(src.ctx(sp), blk, x, y, z, pw, pg);
             dom = in_domain(pw, pg, phi);
         }
         if (!dom) {
@@ -298,7 +405,7 @@ __device__ __forceinline__ void column_cells(const PoolView<Real> &v, const Heav
 #pragma unroll
             for (int kk = 0; kk < 6; kk++) low[kk] = false;
         } else {
-            neighbour_low<Real, kMixed, kClamped>(v, blk, x, y, z, mw[i], phn, low);
+            neighbour_low<Real, kMixed, kClamped>(src, sp, blk, x, y, z, mw[i], phn, low);
         }
         const Real dphidt = cell_rhs_flags<Real>(S.H[rx], S.H[rx + 1], S.H[ry], S.H[ry + 8], S.H[rz], S.H[rz + 64],
                                                  low, phn, phi, rho, ih2);
@@ -309,11 +416,12 @@ __device__ __forceinline__ void column_cells(const PoolView<Real> &v, const Heav
 // A cell of an empty block (every cell and face-halo cell kEmpty) with
 // phi > 0: inside the domain, neighbours and coefficients from global memory.
 template <typename Real>
-__device__ __noinline__ Real empty_cell(const PoolView<Real> &v, int blk, int c, Real phi, const Real *H,
-                                        const Real *phi_in, Real rho, double ih2, double dt, int dt_finite)
+__device__ __noinline__ Real empty_cell(const ItemCtx<Real> v, int blk, int c, Real phi, Real rho, double ih2,
+                                        double dt, int dt_finite)
 {
+    const Real *phi_in = v.phi_in, *H = v.H;
     if (!(phi > (Real)0)) return dt_finite ? clamp01(phi) : cell_update(phi, (Real)0., dt);
-    const int L = v.log2_bpd;
+    const int L = v.L;
     const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
     const Real *b0 = phi_in + (int64_t)blk * kBS3;
     Real phn[6];
@@ -342,12 +450,20 @@ __device__ __forceinline__ unsigned bits_or(double a)
     return (unsigned)b | (unsigned)(b >> 32);
 }
 
-template <typename Real, int kWarps, int kHeavySlots, int kEmptySlots, bool kClamped>
-__global__ void __launch_bounds__((kWarps + 1) * 32)
-rd_step_tma_kernel(PoolView<Real> v, BlockLists lists, const Real *__restrict__ H,
-                   const unsigned short *__restrict__ meta, double ih2, const Real *__restrict__ phi_in,
-                   Real *__restrict__ phi_out, Real rho, double dt, int dt_finite, unsigned *nan_flag,
-                   unsigned *err_flag, const __grid_constant__ CUtensorMap map_x,
+// resident CTAs per SM the register allocation targets: what the shared
+// memory of the default shapes allows (FP32 4, FP64 3)
+#ifndef GBFK_TMA_MIN_BLOCKS_F32
+#define GBFK_TMA_MIN_BLOCKS_F32 4
+#endif
+#ifndef GBFK_TMA_MIN_BLOCKS_F64
+#define GBFK_TMA_MIN_BLOCKS_F64 3
+#endif
+
+template <typename Real, int kWarps, int kHeavySlots, int kEmptySlots, bool kClamped, typename Source>
+__global__ void __launch_bounds__((kWarps + 1) * 32, kWarps == 8 ? (sizeof(Real) == 4 ? GBFK_TMA_MIN_BLOCKS_F32
+                                                                                       : GBFK_TMA_MIN_BLOCKS_F64)
+                                                                  : 1)
+rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __grid_constant__ CUtensorMap map_x,
                    const __grid_constant__ CUtensorMap map_y, const __grid_constant__ CUtensorMap map_z)
 {
     using Lay = SmemLayout<Real, kHeavySlots, kEmptySlots>;
@@ -364,18 +480,14 @@ rd_step_tma_kernel(PoolView<Real> v, BlockLists lists, const Real *__restrict__ 
     uint64_t *hfree = hfull + kHeavySlots;
     uint64_t *efull = hfree + kHeavySlots;
     uint64_t *efree = efull + kEmptySlots;
-    int *items = reinterpret_cast<int *>(smem + Lay::items);
+    SlotHdr *hhdr = reinterpret_cast<SlotHdr *>(smem + Lay::hdr);
+    SlotHdr *ehdr = hhdr + kHeavySlots;
     const int t = threadIdx.x;
     const int c = blockIdx.x, G = gridDim.x;
-    const int nh = lists.n_heavy > c ? (lists.n_heavy - 1 - c) / G + 1 : 0;
-    const int ne = lists.n_empty > c ? (lists.n_empty - 1 - c) / G + 1 : 0;
+    const int NH = src.total_heavy(), NE = src.total_empty();
+    const int nh = NH > c ? (NH - 1 - c) / G + 1 : 0;
+    const int ne = NE > c ? (NE - 1 - c) / G + 1 : 0;
     if (nh + ne == 0) return;  // uniform across the CTA
-    if (nh + ne > kMaxItems) {  // the launcher keeps nh + ne in range
-        if (t == 0) atomicOr(err_flag, 2u);
-        return;
-    }
-    for (int i = t; i < nh; i += blockDim.x) items[i] = lists.heavy[c + i * G];
-    for (int i = t; i < ne; i += blockDim.x) items[nh + i] = lists.empty[c + i * G];
     if (t == 0) {
         for (int i = 0; i < kHeavySlots; i++) {
             mbar_init(&hfull[i], 1);
@@ -389,64 +501,114 @@ rd_step_tma_kernel(PoolView<Real> v, BlockLists lists, const Real *__restrict__ 
     }
     __syncthreads();  // the only CTA-wide barrier
 
-    const int L = v.log2_bpd;
+    const int L = src.L;
+    const int lane = t & 31;
     if (t >= kThreads) {
-        // producer warp
-        if (t != kThreads) return;
-        int jh = 0, je = 0;  // heavy / empty items put in flight
+        // producer warp: the lanes decode 32 items of each kind at a time,
+        // lane 0 issues them
+        int jh = 0, je = 0, hbase = 0, ebase = 0;
+        int hp = 0, he = 0, ep = 0, ee = 0;
+        double hrho = 0, hdt = 0, erho = 0, edt = 0;
+        if (lane < nh) {
+            src.heavy_item(c + lane * G, hp, he);
+            src.params(hp, hrho, hdt);
+        }
+        if (lane < ne) {
+            src.empty_item(c + lane * G, ep, ee);
+            src.params(ep, erho, edt);
+        }
         bool ok = true;
-        while (ok && (jh < nh || je < ne)) {
+        while (jh < nh || je < ne) {
             if (heavy_next(jh, je, nh, ne)) {
+                if (jh == hbase + 32) {
+                    hbase = jh;
+                    if (jh + lane < nh) {
+                        src.heavy_item(c + (jh + lane) * G, hp, he);
+                        src.params(hp, hrho, hdt);
+                    }
+                }
+                const int p = __shfl_sync(0xffffffffu, hp, jh - hbase);
+                const int e = __shfl_sync(0xffffffffu, he, jh - hbase);
+                const double irho = __shfl_sync(0xffffffffu, hrho, jh - hbase);
+                const double idt = __shfl_sync(0xffffffffu, hdt, jh - hbase);
                 const int s = jh % kHeavySlots;
-                if (jh >= kHeavySlots && !mbar_wait(&hfree[s], ((jh / kHeavySlots) - 1) & 1)) {
+                bool w = true;
+                if (lane == 0 && jh >= kHeavySlots) w = mbar_wait(&hfree[s], ((jh / kHeavySlots) - 1) & 1);
+                if (!__shfl_sync(0xffffffffu, w, 0)) {
                     ok = false;
                     break;
                 }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                const int it = items[jh];
-                const int blk = it >> 2, bt = it & 3;
-                HeavySlot<Real> &S = heavy[s];
-                uint64_t *bar = &hfull[s];
-                uint32_t bytes = (kBS3 + 2 * 256 + 4 * 64 + kFacesPerBlock) * sizeof(Real);
-                if (bt == kBlockMixed) bytes += kBS3 * sizeof(unsigned short);
-                mbar_arrive_expect_tx(bar, bytes);
-                bulk_g2s(S.in, phi_in + (int64_t)blk * kBS3, kBS3 * sizeof(Real), bar);
-                box_g2s(S.xm, &map_x, 4, 0, 0, nb_of(blk, L, 0), bar);
-                box_g2s(S.xp, &map_x, 0, 0, 0, nb_of(blk, L, 1), bar);
-                box_g2s(S.ym, &map_y, 0, 7, 0, nb_of(blk, L, 2), bar);
-                box_g2s(S.yp, &map_y, 0, 0, 0, nb_of(blk, L, 3), bar);
-                box_g2s(S.zm, &map_z, 0, 0, 7, nb_of(blk, L, 4), bar);
-                box_g2s(S.zp, &map_z, 0, 0, 0, nb_of(blk, L, 5), bar);
-                bulk_g2s(S.H, H + (int64_t)blk * kFacesPerBlock, kFacesPerBlock * sizeof(Real), bar);
-                if (bt == kBlockMixed)
-                    bulk_g2s(S.meta, meta + (int64_t)blk * kBS3, kBS3 * sizeof(unsigned short), bar);
+                if (lane == 0) {
+                    const int blk = e >> 2, bt = e & 3;
+                    const int64_t s0 = src.slot0(p);
+                    hhdr[s].dt = idt;
+                    hhdr[s].rho = irho;
+                    hhdr[s].p = p;
+                    hhdr[s].e = e;
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    HeavySlot<Real> &S = heavy[s];
+                    uint64_t *bar = &hfull[s];
+                    uint32_t bytes = (kBS3 + 2 * 256 + 4 * 64 + kFacesPerBlock) * sizeof(Real);
+                    if (bt == kBlockMixed) bytes += kBS3 * sizeof(unsigned short);
+                    mbar_arrive_expect_tx(bar, bytes);
+                    bulk_g2s(S.in, src.phi_in + (s0 + blk) * kBS3, kBS3 * sizeof(Real), bar);
+                    box_g2s(S.xm, &map_x, 4, 0, 0, (int)(s0 + nb_of(blk, L, 0)), bar);
+                    box_g2s(S.xp, &map_x, 0, 0, 0, (int)(s0 + nb_of(blk, L, 1)), bar);
+                    box_g2s(S.ym, &map_y, 0, 7, 0, (int)(s0 + nb_of(blk, L, 2)), bar);
+                    box_g2s(S.yp, &map_y, 0, 0, 0, (int)(s0 + nb_of(blk, L, 3)), bar);
+                    box_g2s(S.zm, &map_z, 0, 0, 7, (int)(s0 + nb_of(blk, L, 4)), bar);
+                    box_g2s(S.zp, &map_z, 0, 0, 0, (int)(s0 + nb_of(blk, L, 5)), bar);
+                    bulk_g2s(S.H, src.H_of(p) + (int64_t)blk * kFacesPerBlock, kFacesPerBlock * sizeof(Real), bar);
+                    if (bt == kBlockMixed)
+                        bulk_g2s(S.meta, src.meta_of(p) + (int64_t)blk * kBS3, kBS3 * sizeof(unsigned short), bar);
+                }
                 jh++;
             } else {
+                if (je == ebase + 32) {
+                    ebase = je;
+                    if (je + lane < ne) {
+                        src.empty_item(c + (je + lane) * G, ep, ee);
+                        src.params(ep, erho, edt);
+                    }
+                }
+                const int p = __shfl_sync(0xffffffffu, ep, je - ebase);
+                const int e = __shfl_sync(0xffffffffu, ee, je - ebase);
+                const double irho = __shfl_sync(0xffffffffu, erho, je - ebase);
+                const double idt = __shfl_sync(0xffffffffu, edt, je - ebase);
                 const int s = je % kEmptySlots;
-                if (je >= kEmptySlots && !mbar_wait(&efree[s], ((je / kEmptySlots) - 1) & 1)) {
+                bool w = true;
+                if (lane == 0 && je >= kEmptySlots) w = mbar_wait(&efree[s], ((je / kEmptySlots) - 1) & 1);
+                if (!__shfl_sync(0xffffffffu, w, 0)) {
                     ok = false;
                     break;
                 }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                const int blk = items[nh + je];
-                mbar_arrive_expect_tx(&efull[s], kBS3 * sizeof(Real));
-                bulk_g2s(empties + s * kBS3, phi_in + (int64_t)blk * kBS3, kBS3 * sizeof(Real), &efull[s]);
+                if (lane == 0) {
+                    ehdr[s].dt = idt;
+                    ehdr[s].rho = irho;
+                    ehdr[s].p = p;
+                    ehdr[s].e = e;
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    mbar_arrive_expect_tx(&efull[s], kBS3 * sizeof(Real));
+                    bulk_g2s(empties + s * kBS3, src.phi_in + (src.slot0(p) + (e >> 2)) * kBS3, kBS3 * sizeof(Real),
+                             &efull[s]);
+                }
                 je++;
             }
         }
-        if (!ok) atomicOr(err_flag, 1u);
-        // the CTA's shared memory must outlive every copy in flight (bounded)
-        for (int j = jh - kHeavySlots > 0 ? jh - kHeavySlots : 0; j < jh; j++)
-            mbar_wait(&hfull[j % kHeavySlots], (j / kHeavySlots) & 1);
-        for (int j = je - kEmptySlots > 0 ? je - kEmptySlots : 0; j < je; j++)
-            mbar_wait(&efull[j % kEmptySlots], (j / kEmptySlots) & 1);
+        if (lane == 0) {
+            if (!ok) atomicOr(err_flag, 1u);
+            // the CTA's shared memory must outlive every copy in flight (bounded)
+            for (int j = jh - kHeavySlots > 0 ? jh - kHeavySlots : 0; j < jh; j++)
+                mbar_wait(&hfull[j % kHeavySlots], (j / kHeavySlots) & 1);
+            for (int j = je - kEmptySlots > 0 ? je - kEmptySlots : 0; j < je; j++)
+                mbar_wait(&efull[j % kEmptySlots], (j / kEmptySlots) & 1);
+        }
         return;
     }
 
-    const int warp = t >> 5, lane = t & 31;
+    const int warp = t >> 5;
     const int x = t & 7, y = (t >> 3) & 7, z0 = (t >> 6) * kCells;
     const int c0 = x + kBS * (y + kBS * z0);
-    bool bad = false;
     int jh = 0, je = warp;  // next heavy item; next empty item of this warp (j % kWarps == warp)
     while (jh < nh || je < ne) {
         if (heavy_next(jh, je, nh, ne)) {
@@ -455,24 +617,27 @@ rd_step_tma_kernel(PoolView<Real> v, BlockLists lists, const Real *__restrict__ 
                 if (lane == 0) atomicOr(err_flag, 1u);
                 break;
             }
-            const int it = items[jh];
-            const int blk = it >> 2;
+            const SlotHdr hd = hhdr[s];
+            const int p = hd.p, blk = hd.e >> 2;
+            const Real rho = (Real)hd.rho;
             Real out[kCells];
-            if ((it & 3) == kBlockTissue)
-                column_cells<Real, kCells, false, kClamped>(v, heavy[s], blk, x, y, z0, c0, rho, ih2, dt, dt_finite,
-                                                            out);
+            if ((hd.e & 3) == kBlockTissue)
+                column_cells<Real, kCells, false, kClamped>(src, p, heavy[s], blk, x, y, z0, c0, rho, ih2, hd.dt,
+                                                            isfinite(hd.dt), out);
             else
-                column_cells<Real, kCells, true, kClamped>(v, heavy[s], blk, x, y, z0, c0, rho, ih2, dt, dt_finite,
-                                                           out);
+                column_cells<Real, kCells, true, kClamped>(src, p, heavy[s], blk, x, y, z0, c0, rho, ih2, hd.dt,
+                                                           isfinite(hd.dt), out);
             // every shared read of this warp is done: release the slot
             __syncwarp();
             if (lane == 0) mbar_arrive(&hfree[s], 1);
-            Real *ob = phi_out + (int64_t)blk * kBS3;
+            Real *ob = src.phi_out + (src.slot0(p) + blk) * kBS3;
+            bool bad = false;
 #pragma unroll
             for (int i = 0; i < kCells; i++) {
                 bad |= (out[i] != out[i]);
                 ob[c0 + 64 * i] = out[i];
             }
+            if (bad) atomicOr(src.nan_of(p), 1u);
             jh++;
             continue;
         }
@@ -484,57 +649,62 @@ rd_step_tma_kernel(PoolView<Real> v, BlockLists lists, const Real *__restrict__ 
             break;
         }
         const Real *in = empties + s * kBS3;
-        const int blk = items[nh + j];
-        Real *ob = phi_out + (int64_t)blk * kBS3;
-        Real p[kOwnVecs][kVec];
+        const SlotHdr hd = ehdr[s];
+        const int p = hd.p, blk = hd.e >> 2;
+        Real *ob = src.phi_out + (src.slot0(p) + blk) * kBS3;
+        Real pv[kOwnVecs][kVec];
         unsigned bits = 0;
 #pragma unroll
         for (int q = 0; q < kOwnVecs; q++) {
-            vec_lds<Real, kVec>(in + (q * 32 + lane) * kVec, p[q]);
+            vec_lds<Real, kVec>(in + (q * 32 + lane) * kVec, pv[q]);
 #pragma unroll
-            for (int i = 0; i < kVec; i++) bits |= bits_or(p[q][i]);
+            for (int i = 0; i < kVec; i++) bits |= bits_or(pv[q][i]);
         }
         if (bits == 0) {
             // every cell +0.0: outside the domain, and the clamp leaves +0.0
             __syncwarp();
             if (lane == 0) mbar_arrive(&efree[s], 1);
 #pragma unroll
-            for (int q = 0; q < kOwnVecs; q++) vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, p[q]);
+            for (int q = 0; q < kOwnVecs; q++) vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, pv[q]);
             continue;
         }
-        bool any = false;
+        const double dt = hd.dt;
+        const int dt_finite = isfinite(dt);
+        bool any = false, bad = false;
 #pragma unroll
         for (int q = 0; q < kOwnVecs; q++)
 #pragma unroll
-            for (int i = 0; i < kVec; i++) any |= p[q][i] > (Real)0;  // the domain test of a kEmpty cell
+            for (int i = 0; i < kVec; i++) any |= pv[q][i] > (Real)0;  // the domain test of a kEmpty cell
         if (any) {
             // tumour outside the anatomy: an empty block's slot holds no halo
             // or coefficients, read them from global memory (rare)
+            const ItemCtx<Real> cx = src.ctx(p);
+            const Real rho = (Real)hd.rho;
 #pragma unroll 1
             for (int q = 0; q < kOwnVecs * kVec; q++) {
                 const int cc = ((q / kVec) * 32 + lane) * kVec + q % kVec;
-                const Real o = empty_cell(v, blk, cc, in[cc], H, phi_in, rho, ih2, dt, dt_finite);
+                const Real o = empty_cell(cx, blk, cc, in[cc], rho, ih2, dt, dt_finite);
                 bad |= (o != o);
                 ob[cc] = o;
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&efree[s], 1);
-            continue;
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&efree[s], 1);
+        } else {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&efree[s], 1);
 #pragma unroll
-        for (int q = 0; q < kOwnVecs; q++) {
-            Real o[kVec];
+            for (int q = 0; q < kOwnVecs; q++) {
+                Real o[kVec];
 #pragma unroll
-            for (int i = 0; i < kVec; i++) {
-                o[i] = dt_finite ? clamp01(p[q][i]) : cell_update(p[q][i], (Real)0., dt);
-                bad |= (o[i] != o[i]);
+                for (int i = 0; i < kVec; i++) {
+                    o[i] = dt_finite ? clamp01(pv[q][i]) : cell_update(pv[q][i], (Real)0., dt);
+                    bad |= (o[i] != o[i]);
+                }
+                vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, o);
             }
-            vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, o);
         }
+        if (bad) atomicOr(src.nan_of(p), 1u);
     }
-    if (bad) atomicOr(nan_flag, 1u);
 }
 
 typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -562,15 +732,17 @@ struct Shape {
     static constexpr int kThreads = (kWarps + 1) * 32;
     static constexpr size_t kSmem = SmemLayout<Real, kHeavySlots, kEmptySlots>::bytes;
 
-    // resident CTAs on this part, taken once per process
+    // resident CTAs on this part for the kernels of one work source, taken
+    // once per process
+    template <typename Source>
     static cudaError_t grid(int &g)
     {
         static int cached = 0;
         static std::mutex mu;
         std::lock_guard<std::mutex> lk(mu);
         if (!cached) {
-            auto k = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false>;
-            auto kc = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true>;
+            auto k = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false, Source>;
+            auto kc = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true, Source>;
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
             if (e != cudaSuccess) return e;
             e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
@@ -586,22 +758,17 @@ struct Shape {
         return cudaSuccess;
     }
 
-    static cudaError_t launch(const PoolView<Real> &v, const BlockLists &lists, const Real *H,
-                              const unsigned short *meta, double ih2, const Real *phi_in, bool clamped,
-                              Real *phi_out, Real rho, double dt, unsigned *nan_flag, unsigned *err_flag,
+    template <typename Source>
+    static cudaError_t launch(const Source &src, int items, double ih2, bool clamped, unsigned *err_flag,
                               const CUtensorMap *maps, cudaStream_t s)
     {
         int g = 0;
-        cudaError_t e = grid(g);
+        cudaError_t e = grid<Source>(g);
         if (e != cudaSuccess) return e;
-        const int n = lists.n_heavy + lists.n_empty;
-        const int nctas = n < g ? n : g;
-        if ((lists.n_heavy + nctas - 1) / nctas + (lists.n_empty + nctas - 1) / nctas > kMaxItems)
-            return cudaErrorInvalidValue;
-        auto k = clamped ? rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true>
-                         : rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false>;
-        k<<<nctas, kThreads, kSmem, s>>>(v, lists, H, meta, ih2, phi_in, phi_out, rho, dt, isfinite(dt) ? 1 : 0,
-                                         nan_flag, err_flag, maps[0], maps[1], maps[2]);
+        const int nctas = items < g ? items : g;
+        auto k = clamped ? rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true, Source>
+                         : rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false, Source>;
+        k<<<nctas, kThreads, kSmem, s>>>(src, ih2, err_flag, maps[0], maps[1], maps[2]);
         return cudaGetLastError();
     }
 };
@@ -628,7 +795,6 @@ int tma_shape_code()
     X(8, 2, 16)            \
     X(8, 1, 8)             \
     X(4, 2, 8)             \
-    X(4, 3, 8)             \
     X(16, 2, 16)
 
 template <typename Real, typename F>
@@ -669,16 +835,12 @@ cudaError_t make_pool_tensor_maps(void *base, int nslots, int real_bytes, CUtens
     return cudaSuccess;
 }
 
-// Whether the pipelined step applies to a view: uniform periodic 2^L grid,
-// identity slots, and at most kMaxItems blocks per CTA whatever the split
-// into heavy and empty blocks.
+// Whether the pipelined step applies to a view: a uniform periodic 2^L grid
+// in slots 0..n-1.
 template <typename Real>
 bool tma_step_eligible(const PoolView<Real> &v)
 {
-    if (v.log2_bpd < 0 || !v.identity_slots || v.nblocks <= 0) return false;
-    int g = 0;
-    if (with_shape<Real>([&](auto sh) { return decltype(sh)::grid(g); }) != cudaSuccess) return false;
-    return (int64_t)v.nblocks <= (int64_t)g * (kMaxItems - 2);
+    return v.log2_bpd >= 0 && v.identity_slots && v.nblocks > 0;
 }
 
 template <typename Real>
@@ -689,9 +851,56 @@ cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const BlockLists &lists,
 {
     if (lists.n_heavy + lists.n_empty <= 0) return cudaSuccess;
     if (!tma_step_eligible(v) || lists.n_heavy + lists.n_empty != v.nblocks) return cudaErrorInvalidValue;
+    PoolSource<Real> src;
+    src.heavy = lists.heavy;
+    src.empty = lists.empty;
+    src.nh = lists.n_heavy;
+    src.ne = lists.n_empty;
+    src.phi_in = phi_in;
+    src.phi_out = phi_out;
+    src.H = H;
+    src.pw = v.pw;
+    src.pg = v.pg;
+    src.meta = meta;
+    src.rho = rho;
+    src.dt = dt;
+    src.L = v.log2_bpd;
+    src.nblocks = v.nblocks;
+    src.nan_flag = nan_flag;
     return with_shape<Real>([&](auto sh) {
-        return decltype(sh)::launch(v, lists, H, meta, ih2, phi_in, clamped, phi_out, rho, dt, nan_flag, err_flag,
-                                    maps, s);
+        return decltype(sh)::template launch<PoolSource<Real>>(src, v.nblocks, ih2, clamped, err_flag, maps, s);
+    });
+}
+
+template <typename Real>
+cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int total_items, int log2_bpd,
+                                     int nblocks, const Real *phi_in, Real *phi_out, const Real *H, const Real *pw,
+                                     const Real *pg, const unsigned short *meta, const Real *rho, const double *dt,
+                                     double ih2, bool clamped, unsigned *nan_flags, unsigned *err_flag,
+                                     const CUtensorMap *maps, cudaStream_t s)
+{
+    if (nactive <= 0 || total_items <= 0) return cudaSuccess;
+    if (log2_bpd < 0) return cudaErrorInvalidValue;
+    BatchSource<Real> src;
+    src.lists = bl.lists;
+    src.list_off = bl.list_off;
+    src.hpref = bl.hpref;
+    src.epref = bl.epref;
+    src.anatomy = bl.anatomy;
+    src.nactive = nactive;
+    src.phi_in = phi_in;
+    src.phi_out = phi_out;
+    src.H = H;
+    src.pw = pw;
+    src.pg = pg;
+    src.meta = meta;
+    src.rho = rho;
+    src.dt = dt;
+    src.L = log2_bpd;
+    src.nblocks = nblocks;
+    src.nan_flags = nan_flags;
+    return with_shape<Real>([&](auto sh) {
+        return decltype(sh)::template launch<BatchSource<Real>>(src, total_items, ih2, clamped, err_flag, maps, s);
     });
 }
 
@@ -704,5 +913,14 @@ template cudaError_t launch_rd_step_tma<double>(const PoolView<double> &, const 
                                                 const unsigned short *, double, const double *, bool, double *,
                                                 double, double, unsigned *, unsigned *, const CUtensorMap *,
                                                 cudaStream_t);
+template cudaError_t launch_rd_batch_step_tma<float>(const BatchLists &, int, int, int, int, const float *, float *,
+                                                     const float *, const float *, const float *,
+                                                     const unsigned short *, const float *, const double *, double,
+                                                     bool, unsigned *, unsigned *, const CUtensorMap *, cudaStream_t);
+template cudaError_t launch_rd_batch_step_tma<double>(const BatchLists &, int, int, int, int, const double *,
+                                                      double *, const double *, const double *, const double *,
+                                                      const unsigned short *, const double *, const double *, double,
+                                                      bool, unsigned *, unsigned *, const CUtensorMap *,
+                                                      cudaStream_t);
 
 }  // namespace gbfk

@@ -120,6 +120,8 @@ class Batch:
         self._check(self.lib.gbfk_batch_set_samples(self.b, len(samples), samples))
 
     def run(self, samples_per_cta: int = 0):
+        """Run every sample to its horizon: samples_per_cta -1 = the
+        pipelined step, 1/2/4 = the per-block kernel, 0 = autotune."""
         self._check(self.lib.gbfk_batch_run(self.b, int(samples_per_cta)))
 
     def download(self, sample: int) -> np.ndarray:

@@ -196,11 +196,14 @@ int64_t gbfk_batch_launch_count(const gbfk_batch *b);
 int gbfk_batch_set_anatomy(gbfk_batch *b, int anatomy, const void *pw_dense, const void *pg_dense);
 int gbfk_batch_set_samples(gbfk_batch *b, int nsamples, const gbfk_sample *samples);
 /* Build every sample's initial condition and face coefficients, then run all
- * samples to their horizons.  samples_per_cta: 1, 2 or 4 samples per CTA, or
- * 0 to let the autotuner time the three on the first steps and keep the
- * fastest (the results do not depend on it).  GBFK_E_NAN if a sample became NaN. */
+ * samples to their horizons.  samples_per_cta: -1 for the persistent
+ * pipelined step over all active samples (a power-of-two bpd only), 1, 2 or
+ * 4 for the one-CTA-per-block kernel with that many samples per CTA, or 0 to
+ * let the autotuner time the candidates on the first steps and keep the
+ * fastest (the results do not depend on it).  GBFK_E_NAN if a sample became
+ * NaN; GBFK_E_STATE for -1 on a grid it does not apply to. */
 int gbfk_batch_run(gbfk_batch *b, int samples_per_cta);
-/* The samples-per-CTA the last run used. */
+/* The samples_per_cta choice the last run used (-1: the pipelined step). */
 int gbfk_batch_samples_per_cta(const gbfk_batch *b);
 /* phi of one sample after the run, dense n^3 Real. */
 int gbfk_batch_download(gbfk_batch *b, int sample, void *dense_out);

@@ -1,6 +1,8 @@
 """Batched TMCMC-stage forward solves: every sample of a batch must equal the
 same sample solved alone (gbfk_rd_step on a BlockPool) bit for bit, whatever
-the samples-per-CTA choice, with uneven horizons and several anatomies."""
+the kernel choice (the pipelined step over all active samples, or the
+per-block kernel with 1, 2 or 4 samples per CTA), with uneven horizons and
+several anatomies."""
 import numpy as np
 import pytest
 
@@ -51,12 +53,12 @@ def test_batch_equals_sequential_solves(gbfk_lib, prec):
         b.run(1)
         c0 = [b.download(i) for i in range(10)]
         results = {}
-        for spc in (1, 2, 4, 0):
+        for spc in (1, 2, 4, -1, 0):
             b.set_samples(samples)
             b.run(spc)
             results[spc] = [b.download(i) for i in range(10)]
             if spc == 0:
-                assert b.samples_per_cta in (1, 2, 4)
+                assert b.samples_per_cta in (-1, 1, 2, 4)
 
     for i in range(10):
         pw, pg = anat[which[i]]
