@@ -138,6 +138,10 @@ struct alignas(128) HeavySlot {
 };
 static_assert(sizeof(HeavySlot<float>) % 128 == 0 && sizeof(HeavySlot<double>) % 128 == 0, "slot alignment");
 
+// Items of one CTA that a one-pool launch stages in shared memory (a batch
+// decodes its items 32 at a time instead).
+constexpr int kMaxItems = 1024;
+
 // What the producer tells the consumers about the item in a slot: its
 // sample position, block * 4 + block type, and the sample's dt and rho.
 struct alignas(16) SlotHdr {
@@ -152,7 +156,8 @@ struct SmemLayout {
     static constexpr size_t empty = heavy + (size_t)kHeavySlots * sizeof(HeavySlot<Real>);
     static constexpr size_t bars = empty + (size_t)kEmptySlots * kBS3 * sizeof(Real);
     static constexpr size_t hdr = bars + (8 * (size_t)(2 * kHeavySlots + 2 * kEmptySlots) + 127) / 128 * 128;
-    static constexpr size_t bytes = hdr + sizeof(SlotHdr) * (size_t)(kHeavySlots + kEmptySlots);
+    static constexpr size_t items = hdr + sizeof(SlotHdr) * (size_t)(kHeavySlots + kEmptySlots);
+    static constexpr size_t bytes = items + kMaxItems * sizeof(int);
 };
 
 // Merged item order of a CTA: true when item (jh, je) is the heavy one.
@@ -238,6 +243,7 @@ __device__ __forceinline__ void pwpg_at(const ItemCtx<Real> &v, int blk, int x, 
 // block * 4 + type, mixed blocks first; empty entries block).
 template <typename Real>
 struct PoolSource {
+    static constexpr bool kSamples = false;  // one sample: rho and dt are constants
     const int *heavy, *empty;
     int nh, ne;
     const Real *phi_in;
@@ -270,6 +276,7 @@ struct PoolSource {
 // and of the face coefficients.
 template <typename Real>
 struct BatchSource {
+    static constexpr bool kSamples = true;
     const int *lists;       // per anatomy a: heavy entries at list_off[2a], empty entries at list_off[2a + 1]
     const int *list_off;
     const int *hpref, *epref;
@@ -488,6 +495,19 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
     const int nh = NH > c ? (NH - 1 - c) / G + 1 : 0;
     const int ne = NE > c ? (NE - 1 - c) / G + 1 : 0;
     if (nh + ne == 0) return;  // uniform across the CTA
+    // one pool: the CTA's items staged in shared memory, issued by lane 0
+    // alone; a batch: decoded 32 at a time by the producer warp
+    constexpr bool kStaged = !Source::kSamples;
+    int *items = reinterpret_cast<int *>(smem + Lay::items);
+    if (kStaged) {
+        if (nh + ne > kMaxItems) {  // the launcher keeps nh + ne in range
+            if (t == 0) atomicOr(err_flag, 2u);
+            return;
+        }
+        int unused;
+        for (int i = t; i < nh; i += blockDim.x) src.heavy_item(c + i * G, unused, items[i]);
+        for (int i = t; i < ne; i += blockDim.x) src.empty_item(c + i * G, unused, items[nh + i]);
+    }
     if (t == 0) {
         for (int i = 0; i < kHeavySlots; i++) {
             mbar_init(&hfull[i], 1);
@@ -504,95 +524,123 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
     const int L = src.L;
     const int lane = t & 31;
     if (t >= kThreads) {
-        // producer warp: the lanes decode 32 items of each kind at a time,
-        // lane 0 issues them
-        int jh = 0, je = 0, hbase = 0, ebase = 0;
-        int hp = 0, he = 0, ep = 0, ee = 0;
-        double hrho = 0, hdt = 0, erho = 0, edt = 0;
-        if (lane < nh) {
-            src.heavy_item(c + lane * G, hp, he);
-            src.params(hp, hrho, hdt);
-        }
-        if (lane < ne) {
-            src.empty_item(c + lane * G, ep, ee);
-            src.params(ep, erho, edt);
-        }
+        // producer warp; lane 0 puts an item in flight in slot s
+        auto issue_heavy = [&](int s, int p, int e, double irho, double idt) {
+            const int blk = e >> 2, bt = e & 3;
+            const int64_t s0 = src.slot0(p);
+            if (Source::kSamples) {
+                hhdr[s].dt = idt;
+                hhdr[s].rho = irho;
+                hhdr[s].p = p;
+            }
+            hhdr[s].e = e;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            HeavySlot<Real> &S = heavy[s];
+            uint64_t *bar = &hfull[s];
+            uint32_t bytes = (kBS3 + 2 * 256 + 4 * 64 + kFacesPerBlock) * sizeof(Real);
+            if (bt == kBlockMixed) bytes += kBS3 * sizeof(unsigned short);
+            mbar_arrive_expect_tx(bar, bytes);
+            bulk_g2s(S.in, src.phi_in + (s0 + blk) * kBS3, kBS3 * sizeof(Real), bar);
+            box_g2s(S.xm, &map_x, 4, 0, 0, (int)(s0 + nb_of(blk, L, 0)), bar);
+            box_g2s(S.xp, &map_x, 0, 0, 0, (int)(s0 + nb_of(blk, L, 1)), bar);
+            box_g2s(S.ym, &map_y, 0, 7, 0, (int)(s0 + nb_of(blk, L, 2)), bar);
+            box_g2s(S.yp, &map_y, 0, 0, 0, (int)(s0 + nb_of(blk, L, 3)), bar);
+            box_g2s(S.zm, &map_z, 0, 0, 7, (int)(s0 + nb_of(blk, L, 4)), bar);
+            box_g2s(S.zp, &map_z, 0, 0, 0, (int)(s0 + nb_of(blk, L, 5)), bar);
+            bulk_g2s(S.H, src.H_of(p) + (int64_t)blk * kFacesPerBlock, kFacesPerBlock * sizeof(Real), bar);
+            if (bt == kBlockMixed)
+                bulk_g2s(S.meta, src.meta_of(p) + (int64_t)blk * kBS3, kBS3 * sizeof(unsigned short), bar);
+        };
+        auto issue_empty = [&](int s, int p, int e, double irho, double idt) {
+            if (Source::kSamples) {
+                ehdr[s].dt = idt;
+                ehdr[s].rho = irho;
+                ehdr[s].p = p;
+            }
+            ehdr[s].e = e;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive_expect_tx(&efull[s], kBS3 * sizeof(Real));
+            bulk_g2s(empties + s * kBS3, src.phi_in + (src.slot0(p) + (e >> 2)) * kBS3, kBS3 * sizeof(Real),
+                     &efull[s]);
+        };
+        int jh = 0, je = 0;
         bool ok = true;
-        while (jh < nh || je < ne) {
-            if (heavy_next(jh, je, nh, ne)) {
-                if (jh == hbase + 32) {
-                    hbase = jh;
-                    if (jh + lane < nh) {
-                        src.heavy_item(c + (jh + lane) * G, hp, he);
-                        src.params(hp, hrho, hdt);
+        if (kStaged) {
+            if (lane != 0) return;
+            while (jh < nh || je < ne) {
+                if (heavy_next(jh, je, nh, ne)) {
+                    const int s = jh % kHeavySlots;
+                    if (jh >= kHeavySlots && !mbar_wait(&hfree[s], ((jh / kHeavySlots) - 1) & 1)) {
+                        ok = false;
+                        break;
                     }
-                }
-                const int p = __shfl_sync(0xffffffffu, hp, jh - hbase);
-                const int e = __shfl_sync(0xffffffffu, he, jh - hbase);
-                const double irho = __shfl_sync(0xffffffffu, hrho, jh - hbase);
-                const double idt = __shfl_sync(0xffffffffu, hdt, jh - hbase);
-                const int s = jh % kHeavySlots;
-                bool w = true;
-                if (lane == 0 && jh >= kHeavySlots) w = mbar_wait(&hfree[s], ((jh / kHeavySlots) - 1) & 1);
-                if (!__shfl_sync(0xffffffffu, w, 0)) {
-                    ok = false;
-                    break;
-                }
-                if (lane == 0) {
-                    const int blk = e >> 2, bt = e & 3;
-                    const int64_t s0 = src.slot0(p);
-                    hhdr[s].dt = idt;
-                    hhdr[s].rho = irho;
-                    hhdr[s].p = p;
-                    hhdr[s].e = e;
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    HeavySlot<Real> &S = heavy[s];
-                    uint64_t *bar = &hfull[s];
-                    uint32_t bytes = (kBS3 + 2 * 256 + 4 * 64 + kFacesPerBlock) * sizeof(Real);
-                    if (bt == kBlockMixed) bytes += kBS3 * sizeof(unsigned short);
-                    mbar_arrive_expect_tx(bar, bytes);
-                    bulk_g2s(S.in, src.phi_in + (s0 + blk) * kBS3, kBS3 * sizeof(Real), bar);
-                    box_g2s(S.xm, &map_x, 4, 0, 0, (int)(s0 + nb_of(blk, L, 0)), bar);
-                    box_g2s(S.xp, &map_x, 0, 0, 0, (int)(s0 + nb_of(blk, L, 1)), bar);
-                    box_g2s(S.ym, &map_y, 0, 7, 0, (int)(s0 + nb_of(blk, L, 2)), bar);
-                    box_g2s(S.yp, &map_y, 0, 0, 0, (int)(s0 + nb_of(blk, L, 3)), bar);
-                    box_g2s(S.zm, &map_z, 0, 0, 7, (int)(s0 + nb_of(blk, L, 4)), bar);
-                    box_g2s(S.zp, &map_z, 0, 0, 0, (int)(s0 + nb_of(blk, L, 5)), bar);
-                    bulk_g2s(S.H, src.H_of(p) + (int64_t)blk * kFacesPerBlock, kFacesPerBlock * sizeof(Real), bar);
-                    if (bt == kBlockMixed)
-                        bulk_g2s(S.meta, src.meta_of(p) + (int64_t)blk * kBS3, kBS3 * sizeof(unsigned short), bar);
-                }
-                jh++;
-            } else {
-                if (je == ebase + 32) {
-                    ebase = je;
-                    if (je + lane < ne) {
-                        src.empty_item(c + (je + lane) * G, ep, ee);
-                        src.params(ep, erho, edt);
+                    issue_heavy(s, 0, items[jh], 0., 0.);
+                    jh++;
+                } else {
+                    const int s = je % kEmptySlots;
+                    if (je >= kEmptySlots && !mbar_wait(&efree[s], ((je / kEmptySlots) - 1) & 1)) {
+                        ok = false;
+                        break;
                     }
+                    issue_empty(s, 0, items[nh + je], 0., 0.);
+                    je++;
                 }
-                const int p = __shfl_sync(0xffffffffu, ep, je - ebase);
-                const int e = __shfl_sync(0xffffffffu, ee, je - ebase);
-                const double irho = __shfl_sync(0xffffffffu, erho, je - ebase);
-                const double idt = __shfl_sync(0xffffffffu, edt, je - ebase);
-                const int s = je % kEmptySlots;
-                bool w = true;
-                if (lane == 0 && je >= kEmptySlots) w = mbar_wait(&efree[s], ((je / kEmptySlots) - 1) & 1);
-                if (!__shfl_sync(0xffffffffu, w, 0)) {
-                    ok = false;
-                    break;
+            }
+        } else {
+            // the lanes decode 32 items of each kind at a time, lane 0 issues them
+            int hbase = 0, ebase = 0;
+            int hp = 0, he = 0, ep = 0, ee = 0;
+            double hrho = 0, hdt = 0, erho = 0, edt = 0;
+            if (lane < nh) {
+                src.heavy_item(c + lane * G, hp, he);
+                src.params(hp, hrho, hdt);
+            }
+            if (lane < ne) {
+                src.empty_item(c + lane * G, ep, ee);
+                src.params(ep, erho, edt);
+            }
+            while (jh < nh || je < ne) {
+                if (heavy_next(jh, je, nh, ne)) {
+                    if (jh == hbase + 32) {
+                        hbase = jh;
+                        if (jh + lane < nh) {
+                            src.heavy_item(c + (jh + lane) * G, hp, he);
+                            src.params(hp, hrho, hdt);
+                        }
+                    }
+                    const int k = jh - hbase;
+                    const int e = __shfl_sync(0xffffffffu, he, k), p = __shfl_sync(0xffffffffu, hp, k);
+                    const double irho = __shfl_sync(0xffffffffu, hrho, k), idt = __shfl_sync(0xffffffffu, hdt, k);
+                    const int s = jh % kHeavySlots;
+                    bool w = true;
+                    if (lane == 0 && jh >= kHeavySlots) w = mbar_wait(&hfree[s], ((jh / kHeavySlots) - 1) & 1);
+                    if (!__shfl_sync(0xffffffffu, w, 0)) {
+                        ok = false;
+                        break;
+                    }
+                    if (lane == 0) issue_heavy(s, p, e, irho, idt);
+                    jh++;
+                } else {
+                    if (je == ebase + 32) {
+                        ebase = je;
+                        if (je + lane < ne) {
+                            src.empty_item(c + (je + lane) * G, ep, ee);
+                            src.params(ep, erho, edt);
+                        }
+                    }
+                    const int k = je - ebase;
+                    const int e = __shfl_sync(0xffffffffu, ee, k), p = __shfl_sync(0xffffffffu, ep, k);
+                    const double irho = __shfl_sync(0xffffffffu, erho, k), idt = __shfl_sync(0xffffffffu, edt, k);
+                    const int s = je % kEmptySlots;
+                    bool w = true;
+                    if (lane == 0 && je >= kEmptySlots) w = mbar_wait(&efree[s], ((je / kEmptySlots) - 1) & 1);
+                    if (!__shfl_sync(0xffffffffu, w, 0)) {
+                        ok = false;
+                        break;
+                    }
+                    if (lane == 0) issue_empty(s, p, e, irho, idt);
+                    je++;
                 }
-                if (lane == 0) {
-                    ehdr[s].dt = idt;
-                    ehdr[s].rho = irho;
-                    ehdr[s].p = p;
-                    ehdr[s].e = e;
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    mbar_arrive_expect_tx(&efull[s], kBS3 * sizeof(Real));
-                    bulk_g2s(empties + s * kBS3, src.phi_in + (src.slot0(p) + (e >> 2)) * kBS3, kBS3 * sizeof(Real),
-                             &efull[s]);
-                }
-                je++;
             }
         }
         if (lane == 0) {
@@ -617,16 +665,25 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
                 if (lane == 0) atomicOr(err_flag, 1u);
                 break;
             }
-            const SlotHdr hd = hhdr[s];
-            const int p = hd.p, blk = hd.e >> 2;
-            const Real rho = (Real)hd.rho;
+            const int e = hhdr[s].e, blk = e >> 2;
+            int p = 0;
+            double dt;
+            Real rho;
+            if (Source::kSamples) {
+                p = hhdr[s].p;
+                dt = hhdr[s].dt;
+                rho = (Real)hhdr[s].rho;
+            } else {
+                dt = src.dt_of(0);
+                rho = src.rho_of(0);
+            }
             Real out[kCells];
-            if ((hd.e & 3) == kBlockTissue)
-                column_cells<Real, kCells, false, kClamped>(src, p, heavy[s], blk, x, y, z0, c0, rho, ih2, hd.dt,
-                                                            isfinite(hd.dt), out);
+            if ((e & 3) == kBlockTissue)
+                column_cells<Real, kCells, false, kClamped>(src, p, heavy[s], blk, x, y, z0, c0, rho, ih2, dt,
+                                                            isfinite(dt), out);
             else
-                column_cells<Real, kCells, true, kClamped>(src, p, heavy[s], blk, x, y, z0, c0, rho, ih2, hd.dt,
-                                                           isfinite(hd.dt), out);
+                column_cells<Real, kCells, true, kClamped>(src, p, heavy[s], blk, x, y, z0, c0, rho, ih2, dt,
+                                                           isfinite(dt), out);
             // every shared read of this warp is done: release the slot
             __syncwarp();
             if (lane == 0) mbar_arrive(&hfree[s], 1);
@@ -649,8 +706,8 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
             break;
         }
         const Real *in = empties + s * kBS3;
-        const SlotHdr hd = ehdr[s];
-        const int p = hd.p, blk = hd.e >> 2;
+        const int blk = ehdr[s].e >> 2;
+        const int p = Source::kSamples ? ehdr[s].p : 0;
         Real *ob = src.phi_out + (src.slot0(p) + blk) * kBS3;
         Real pv[kOwnVecs][kVec];
         unsigned bits = 0;
@@ -668,7 +725,7 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
             for (int q = 0; q < kOwnVecs; q++) vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, pv[q]);
             continue;
         }
-        const double dt = hd.dt;
+        const double dt = Source::kSamples ? ehdr[s].dt : src.dt_of(0);
         const int dt_finite = isfinite(dt);
         bool any = false, bad = false;
 #pragma unroll
@@ -679,7 +736,7 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
             // tumour outside the anatomy: an empty block's slot holds no halo
             // or coefficients, read them from global memory (rare)
             const ItemCtx<Real> cx = src.ctx(p);
-            const Real rho = (Real)hd.rho;
+            const Real rho = Source::kSamples ? (Real)ehdr[s].rho : src.rho_of(0);
 #pragma unroll 1
             for (int q = 0; q < kOwnVecs * kVec; q++) {
                 const int cc = ((q / kVec) * 32 + lane) * kVec + q % kVec;
@@ -836,11 +893,15 @@ cudaError_t make_pool_tensor_maps(void *base, int nslots, int real_bytes, CUtens
 }
 
 // Whether the pipelined step applies to a view: a uniform periodic 2^L grid
-// in slots 0..n-1.
+// in slots 0..n-1 whose items fit each CTA's staging buffer.
 template <typename Real>
 bool tma_step_eligible(const PoolView<Real> &v)
 {
-    return v.log2_bpd >= 0 && v.identity_slots && v.nblocks > 0;
+    if (v.log2_bpd < 0 || !v.identity_slots || v.nblocks <= 0) return false;
+    int g = 0;
+    if (with_shape<Real>([&](auto sh) { return decltype(sh)::template grid<PoolSource<Real>>(g); }) != cudaSuccess)
+        return false;
+    return (int64_t)v.nblocks <= (int64_t)g * (kMaxItems - 2);
 }
 
 template <typename Real>
