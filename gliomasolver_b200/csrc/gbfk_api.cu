@@ -1072,12 +1072,41 @@ struct Adjoint {
     double dt, Dw;
     int64_t fsteps = 0, asteps = 0;
     cudaError_t err = cudaSuccess;
+    // forward steps on the pipelined kernel: its work lists, 1/(h*h) of the
+    // uniform grid, and the face-box tensor maps of every buffer a step reads
+    bool pipelined = false;
+    BlockLists lists{};
+    double ih2 = 0;
+    const Real *X0 = nullptr;  // the initial condition: the only step input not written by a step
+    struct Maps {
+        const void *buf;
+        CUtensorMap m[3];
+    };
+    std::vector<Maps> maps;
+
+    cudaError_t add_maps(const void *buf)
+    {
+        maps.emplace_back();
+        maps.back().buf = buf;
+        return make_pool_tensor_maps(const_cast<void *>(buf), ctx->max_blocks, (int)sizeof(Real), maps.back().m);
+    }
+    const CUtensorMap *maps_of(const void *buf) const
+    {
+        for (const Maps &m : maps)
+            if (m.buf == buf) return m.m;
+        return nullptr;
+    }
 
     void step(const Real *in, Real *out)
     {
         if (err != cudaSuccess) return;
-        err = launch_rd_step<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, in, out, nullptr, rho, dt,
-                                   ctx->d_nan, ctx->stream);
+        const CUtensorMap *m = pipelined ? maps_of(in) : nullptr;
+        if (m)
+            err = launch_rd_step_tma<Real>(v, lists, (const Real *)ctx->d_H, ctx->d_meta, ih2, in, in != X0, out, rho,
+                                           dt, ctx->d_nan, ctx->d_nan + 1, m, ctx->stream);
+        else
+            err = launch_rd_step<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, in, out, nullptr, rho, dt,
+                                       ctx->d_nan, ctx->stream);
         fsteps++;
         ctx->launches++;
     }
@@ -1185,6 +1214,24 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
         return fail(ctx, GBFK_E_OOM, "forward_adjoint: %s", cudaGetErrorString(e));
     }
     e = cudaMemsetAsync(A.grad_acc, 0, (size_t)nb * kGradSlots * sizeof(double), ctx->stream);
+    // forward steps on the pipelined kernel where it applies (bit-identical)
+    A.X0 = X0;
+    if (e == cudaSuccess && tma_step_eligible<Real>(A.v) && ctx->step_pref != GBFK_STEP_BLOCK) {
+        rc = build_step_lists(ctx);
+        if (rc) {
+            cleanup();
+            return rc;
+        }
+        A.lists = {ctx->d_lists, ctx->n_heavy, ctx->d_lists + ctx->n_heavy, ctx->n_empty};
+        const double h = sizeof(Real) == 8 ? ctx->h_h[0] : (double)(float)ctx->h_h[0];
+        A.ih2 = 1. / (h * h);
+        const Real *inputs[] = {X0, A.T0, A.T1};
+        for (const Real *b : inputs)
+            if (e == cudaSuccess) e = A.add_maps(b);
+        for (Real *b : A.slots)
+            if (e == cudaSuccess) e = A.add_maps(b);
+        A.pipelined = e == cudaSuccess;
+    }
     // initial condition
     if (e == cudaSuccess) {
         if (p->sigma > 0) {
