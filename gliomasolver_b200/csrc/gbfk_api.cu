@@ -1203,7 +1203,7 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
                      (void **)&A.MU};
     for (void **b : bufs)
         if (e == cudaSuccess) e = alloc(A.fbytes, b);
-    if (e == cudaSuccess) e = alloc((size_t)nb * kBS3, (void **)&A.FL);
+    if (e == cudaSuccess) e = alloc((size_t)nb * kBS3 + nb, (void **)&A.FL);  // per-cell flags + per-block tail
     if (e == cudaSuccess) e = alloc((size_t)nb * kGradSlots * sizeof(double), (void **)&A.grad_acc);
     if (e == cudaSuccess) e = alloc((size_t)xparts * 6 * sizeof(double), (void **)&xpart);
     A.slots.assign(p->nsnapshots, nullptr);

@@ -498,7 +498,11 @@ cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigne
 // dL/dDw += sum_i mu_i dt dom_i (diffusive part of r_i) / Dw (the face
 // coefficients are homogeneous of degree 1 in (Dw, Dg = 0.1 Dw)).
 // adj_mu recomputes the forward step of its block exactly like step_block and
-// records per cell: bit 0 = dom, bit 1+k = coefficient k doubled.
+// records per cell: bit 0 = dom, bit 1+k = coefficient k doubled; and per
+// block whether any of its cells is inside the domain.  A block with no such
+// cell has mu = lambda' [0 < phi <= 1], no gradient terms and, unless a face
+// neighbour has a domain cell, lambda = mu: both kernels take that short
+// path without the halo, the coefficients or the reductions.
 
 __device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
 {
@@ -512,8 +516,8 @@ template <typename Real>
 __global__ void __launch_bounds__(128)
 adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
               const double *__restrict__ ih2blk, const Real *__restrict__ phi, const Real *__restrict__ lam_next,
-              Real *__restrict__ mu, unsigned char *__restrict__ flags, Real rho, double dt, double inv_Dw,
-              double *__restrict__ grad_acc)
+              Real *__restrict__ mu, unsigned char *__restrict__ flags, unsigned char *__restrict__ blk_dom,
+              Real rho, double dt, double inv_Dw, double *__restrict__ grad_acc)
 {
     __shared__ __align__(16) Real ph[kStepLab];
     __shared__ double red[4][128];
@@ -524,6 +528,43 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
     const int l0 = lab_p(x4, y, z);
     Vec4<Real> p;
     p.load(phi + base + c0);
+    const unsigned char bt = v.btype[blk];
+    unsigned mw[4];
+    if (bt == kBlockMixed) {
+        for (int i = 0; i < 4; i++) mw[i] = meta[base + c0 + i];
+    } else {
+        const unsigned m = bt == kBlockEmpty ? kMetaAllEmpty : kMetaAllTissue;
+        mw[0] = mw[1] = mw[2] = mw[3] = m;
+    }
+    bool doms[4], any = false;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const Real ph0 = p.v[i];
+        const unsigned cls = mw[i] & 3u;
+        if (cls == kTissue && ph0 >= (Real)0) doms[i] = true;
+        else if (cls == kEmpty) doms[i] = ph0 > (Real)0;
+        else {
+            Real pw, pg;
+            lab_pwpg(v, blk, base, x4 + i, y, z, pw, pg);
+            doms[i] = in_domain(pw, pg, ph0);
+        }
+        any |= doms[i];
+    }
+    if (!__syncthreads_or(any)) {
+        // no cell inside the domain: dphidt = 0, pre = phi, no gradient terms
+        Vec4<Real> lam, out;
+        lam.load(lam_next + base + c0);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const Real pre = to_real<Real>(__dadd_rn((double)p.v[i], __dmul_rn(dt, 0.)));
+            out.v[i] = (pre > (Real)0 && pre <= (Real)1) ? lam.v[i] : (Real)0;
+        }
+        out.store(mu + base + c0);
+        *reinterpret_cast<uchar4 *>(flags + base + c0) = make_uchar4(0, 0, 0, 0);
+        if (t == 0) blk_dom[blk] = 0;
+        return;
+    }
+    if (t == 0) blk_dom[blk] = 1;
     p.store(ph + l0);
 #pragma unroll
     for (int i = 0; i < 3; i++) {
@@ -533,14 +574,6 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
         face_cell(f, pc, lx, ly, lz, sc);
         const int nb = face_neighbour(v, blk, f);
         ph[lab_p(lx, ly, lz)] = phi[(int64_t)nb * kBS3 + sc];
-    }
-    const unsigned char bt = v.btype[blk];
-    unsigned mw[4];
-    if (bt == kBlockMixed) {
-        for (int i = 0; i < 4; i++) mw[i] = meta[base + c0 + i];
-    } else {
-        const unsigned m = bt == kBlockEmpty ? kMetaAllEmpty : kMetaAllTissue;
-        mw[0] = mw[1] = mw[2] = mw[3] = m;
     }
     __syncthreads();
     const Real *Hb = H + (int64_t)blk * kFacesPerBlock;
@@ -555,15 +588,7 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
     for (int i = 0; i < 4; i++) {
         const int x = x4 + i;
         const Real ph0 = p.v[i];
-        const unsigned cls = mw[i] & 3u;
-        bool dom;
-        if (cls == kTissue && ph0 >= (Real)0) dom = true;
-        else if (cls == kEmpty) dom = ph0 > (Real)0;
-        else {
-            Real pw, pg;
-            lab_pwpg(v, blk, base, x, y, z, pw, pg);
-            dom = in_domain(pw, pg, ph0);
-        }
+        const bool dom = doms[i];
         unsigned char f = dom ? 1 : 0;
         Real dphidt = (Real)0.;
         double flux_diff = 0;
@@ -644,7 +669,7 @@ template <typename Real>
 __global__ void __launch_bounds__(128)
 adj_lambda_kernel(PoolView<Real> v, const Real *__restrict__ H, const double *__restrict__ ih2blk,
                   const Real *__restrict__ phi, const Real *__restrict__ mu, const unsigned char *__restrict__ flags,
-                  Real *__restrict__ lam, Real rho, double dt)
+                  const unsigned char *__restrict__ blk_dom, Real *__restrict__ lam, Real rho, double dt)
 {
     __shared__ __align__(16) Real smu[kStepLab];
     __shared__ unsigned char sfl[kStepLab];
@@ -655,6 +680,13 @@ adj_lambda_kernel(PoolView<Real> v, const Real *__restrict__ H, const double *__
     const int l0 = lab_p(x4, y, z);
     Vec4<Real> m;
     m.load(mu + base + c0);
+    // threads 0..5: the face neighbours, thread 6: the block itself
+    const int d = t < 7 ? blk_dom[t == 6 ? blk : face_neighbour(v, blk, t)] : 0;
+    if (!__syncthreads_or(d)) {
+        // no domain cell in the block or its face neighbours: lambda = mu
+        m.store(lam + base + c0);
+        return;
+    }
     m.store(smu + l0);
     const uchar4 f4 = *reinterpret_cast<const uchar4 *>(flags + base + c0);
     sfl[l0] = f4.x; sfl[l0 + 1] = f4.y; sfl[l0 + 2] = f4.z; sfl[l0 + 3] = f4.w;
@@ -710,8 +742,10 @@ cudaError_t launch_adjoint_step(const PoolView<Real> &v, const Real *H, const un
                                 double Dw, double *grad_acc, cudaStream_t s)
 {
     if (v.nblocks <= 0) return cudaSuccess;
-    adj_mu_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, meta, ih2, phi, lam, mu, flags, rho, dt, 1. / Dw, grad_acc);
-    adj_lambda_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, ih2, phi, mu, flags, lam, rho, dt);
+    unsigned char *blk_dom = flags + (int64_t)v.nblocks * kBS3;  // the flag buffer's per-block tail
+    adj_mu_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, meta, ih2, phi, lam, mu, flags, blk_dom, rho, dt, 1. / Dw,
+                                                   grad_acc);
+    adj_lambda_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, ih2, phi, mu, flags, blk_dom, lam, rho, dt);
     return cudaGetLastError();
 }
 

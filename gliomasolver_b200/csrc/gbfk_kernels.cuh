@@ -159,7 +159,9 @@ cudaError_t launch_likelihood(const double *model, int n, const unsigned char *t
 
 // Discrete adjoint (uniform grids): one adjoint step through the step that
 // maps phi (input state) to the next state; lam holds dL/dphi' on entry and
-// dL/dphi on exit; grad_acc: nblocks * 4 doubles (rho sum/comp, Dw sum/comp).
+// dL/dphi on exit; flags: nblocks * 512 + nblocks bytes of scratch (per-cell
+// switches, then per-block domain flags); grad_acc: nblocks * 4 doubles (rho
+// sum/comp, Dw sum/comp).
 template <typename Real>
 cudaError_t launch_adjoint_step(const PoolView<Real> &v, const Real *H, const unsigned short *meta, const double *ih2,
                                 const Real *phi, Real *lam, Real *mu, unsigned char *flags, Real rho, double dt,
