@@ -242,8 +242,8 @@ int check_stage_timeout(gbfk_ctx *ctx)
     CK(cudaStreamSynchronize(ctx->stream));
     if (flag) {
         CK(cudaMemsetAsync(ctx->d_nan + 1, 0, sizeof(unsigned), ctx->stream));
-        return fail(ctx, GBFK_E_CUDA, (flag & 1u) ? "rd_step: a wait of the pipelined step timed out (1 s)"
-                                                  : "rd_step: a CTA's work list of the pipelined step overflowed");
+        if (flag & 1u) return fail(ctx, GBFK_E_TIMEOUT, "rd_step: a wait of the pipelined step timed out (1 s)");
+        return fail(ctx, GBFK_E_CUDA, "rd_step: a CTA's work list of the pipelined step overflowed");
     }
     return GBFK_OK;
 }

@@ -335,7 +335,7 @@ int batch_run(gbfk_batch *b, int spc)
     BK(cudaStreamSynchronize(b->stream));
     unsigned err = 0;
     BK(cudaMemcpy(&err, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    if (err) return bfail(b, GBFK_E_CUDA, "batch_run: a wait of the pipelined step timed out (1 s)");
+    if (err) return bfail(b, GBFK_E_TIMEOUT, "batch_run: a wait of the pipelined step timed out (1 s)");
     std::vector<unsigned> flags(b->nsamples);
     BK(cudaMemcpy(flags.data(), b->d_nan, b->nsamples * sizeof(unsigned), cudaMemcpyDeviceToHost));
     for (int k = 0; k < b->nsamples; k++)

@@ -144,7 +144,7 @@ int gbfk_rd_step(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
  * gbfk_step_kernel reports the kernel of the last gbfk_rd_step (0 before
  * any).  A pipeline stage whose copies never complete ends its wait after
  * about a second; gbfk_rd_step with check_nan, or gbfk_sync, then returns
- * GBFK_E_CUDA. */
+ * GBFK_E_TIMEOUT. */
 #define GBFK_STEP_AUTO 0
 #define GBFK_STEP_BLOCK 1
 #define GBFK_STEP_PIPELINED 2
