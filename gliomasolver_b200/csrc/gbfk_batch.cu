@@ -71,6 +71,16 @@ struct gbfk_batch {
     CUtensorMap maps[2][3];
     bool maps_ready = false;
     int chosen_spc = 0;          // block kernel: samples per CTA; -1: the pipelined kernel
+    bool ran = false;            // the samples hold their final states
+    // observations of the likelihood step (n^3 grid) and its scratch
+    unsigned char *d_t1c = nullptr, *d_flair = nullptr;
+    double *d_pet = nullptr;
+    int *d_roi = nullptr;
+    int nroi = 0;
+    bool have_obs = false;
+    double *d_model = nullptr;   // one sample's dump grid
+    double *d_partial = nullptr; // likelihood partial sums
+    double *d_lik = nullptr;     // 4 per sample
     int64_t launches = 0;
     std::string err;
 };
@@ -95,6 +105,21 @@ int bfail(gbfk_batch *b, int code, const char *fmt, ...)
             return bfail(b, e_ == cudaErrorMemoryAllocation ? GBFK_E_OOM : GBFK_E_CUDA, "%s: %s (%s:%d)", \
                          #call, cudaGetErrorString(e_), __FILE__, __LINE__);                              \
     } while (0)
+
+// One sample's phi (block-pool order of a uniform bpd^3 grid) as doubles on
+// the n^3 grid, x fastest: the dump of a uniform grid at its own resolution
+// (each cell written once, Glioma_ReactionDiffusion.cpp:208-262).
+template <typename Real>
+__global__ void pool_to_dense_kernel(const Real *__restrict__ pool, int n, double *__restrict__ out)
+{
+    const int64_t N = (int64_t)n * n * n;
+    const int bpd = n / kBS;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < N; g += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(g % n), y = (int)((g / n) % n), z = (int)(g / ((int64_t)n * n));
+        const int64_t slot = (x >> 3) + (int64_t)bpd * ((y >> 3) + (int64_t)bpd * (z >> 3));
+        out[g] = (double)pool[slot * kBS3 + (x & 7) + kBS * ((y & 7) + kBS * (z & 7))];
+    }
+}
 
 template <typename Real>
 PoolView<Real> batch_pool(gbfk_batch *b)
@@ -328,6 +353,7 @@ int batch_run(gbfk_batch *b, int spc)
         spc = best_spc;
     }
     b->chosen_spc = spc;
+    b->ran = false;
     for (; step < maxsteps; step++) {
         BK(batch_step<Real>(b, bv, active_at(step), step, spc));
         b->launches++;
@@ -340,6 +366,39 @@ int batch_run(gbfk_batch *b, int spc)
     BK(cudaMemcpy(flags.data(), b->d_nan, b->nsamples * sizeof(unsigned), cudaMemcpyDeviceToHost));
     for (int k = 0; k < b->nsamples; k++)
         if (flags[k]) return bfail(b, GBFK_E_NAN, "sample %d became NaN", b->order[k]);
+    b->ran = true;
+    return GBFK_OK;
+}
+
+template <typename Real>
+int batch_likelihood(gbfk_batch *b, const gbfk_likelihood_params *p, double *out)
+{
+    const int n = b->n, nparts = 148 * 4;
+    const size_t N = (size_t)n * n * n;
+    if (!b->d_model) BK(cudaMalloc(&b->d_model, N * sizeof(double)));
+    if (!b->d_partial) BK(cudaMalloc(&b->d_partial, (size_t)nparts * 7 * sizeof(double)));
+    if (!b->d_lik) BK(cudaMalloc(&b->d_lik, (size_t)b->max_samples * 4 * sizeof(double)));
+    LikelihoodParams lp;
+    lp.pet_sigma2 = p->pet_sigma2;
+    lp.pet_scale = p->pet_scale;
+    lp.t1_uc = p->t1_uc;
+    lp.t2_uc = p->t2_uc;
+    lp.slope = p->slope;
+    lp.step_pet = p->step_pet;
+    lp.step_mri = p->step_mri;
+    const size_t field = (size_t)b->nblocks * kBS3;
+    int64_t grid = (N + 255) / 256;
+    if (grid > 148 * 32) grid = 148 * 32;
+    for (int s = 0; s < b->nsamples; s++) {
+        const Real *final = (const Real *)b->phi_all[b->params[s].nsteps & 1] + (size_t)b->pos[s] * field;
+        pool_to_dense_kernel<Real><<<(int)grid, 256, 0, b->stream>>>(final, n, b->d_model);
+        BK(cudaGetLastError());
+        BK(launch_likelihood(b->d_model, n, b->d_t1c, b->d_flair, b->d_pet, b->nroi ? b->d_roi : nullptr, b->nroi,
+                             lp, b->d_partial, nparts, b->d_lik + 4 * (size_t)s, b->stream));
+        b->launches += 3;
+    }
+    BK(cudaMemcpyAsync(out, b->d_lik, (size_t)b->nsamples * 4 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    BK(cudaStreamSynchronize(b->stream));
     return GBFK_OK;
 }
 
@@ -438,7 +497,8 @@ int gbfk_batch_destroy(gbfk_batch *b)
     if (b->stream) cudaStreamSynchronize(b->stream);
     void *ptrs[] = {b->d_nbr,       b->d_ih2,    b->d_views, b->d_nan,      b->d_err,     b->d_rho, b->d_dt,
                     b->d_lists,     b->pw_all,   b->pg_all,  b->meta_all,   b->btype_all, b->phi_all[0],
-                    b->phi_all[1],  b->H_all};
+                    b->phi_all[1],  b->H_all,    b->d_t1c,   b->d_flair,    b->d_pet,     b->d_roi, b->d_model,
+                    b->d_partial,   b->d_lik};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -492,6 +552,7 @@ int gbfk_batch_set_samples(gbfk_batch *b, int nsamples, const gbfk_sample *sampl
     }
     b->nsamples = nsamples;
     b->params.assign(samples, samples + nsamples);
+    b->ran = false;
     return GBFK_OK;
 }
 
@@ -527,6 +588,59 @@ int gbfk_batch_download(gbfk_batch *b, int sample, void *dense_out)
     BK(e);
     b->launches++;
     return GBFK_OK;
+}
+
+int gbfk_batch_set_observations(gbfk_batch *b, const double *t1c, const double *flair, const double *pet,
+                                const int *roi, int nroi)
+{
+    if (!b) return GBFK_E_INVALID;
+    if (!t1c || !flair || nroi < 0 || (nroi > 0 && !roi))
+        return bfail(b, GBFK_E_INVALID, "batch_set_observations: bad arguments");
+    BK(cudaSetDevice(b->device));
+    BK(cudaStreamSynchronize(b->stream));
+    const int n = b->n;
+    const size_t N = (size_t)n * n * n;
+    for (int i = 0; i < 3 * nroi; i++)
+        if (roi[i] < 0 || roi[i] >= n) return bfail(b, GBFK_E_INVALID, "batch_set_observations: ROI point out of the grid");
+    void *old[] = {b->d_t1c, b->d_flair, b->d_pet, b->d_roi};
+    for (void *q : old)
+        if (q) cudaFree(q);
+    b->d_t1c = b->d_flair = nullptr;
+    b->d_pet = nullptr;
+    b->d_roi = nullptr;
+    b->have_obs = false;
+    std::vector<unsigned char> a(N), c(N);
+    for (size_t i = 0; i < N; i++) {
+        a[i] = t1c[i] == 1 ? 1 : 0;  // HGG_Likelihood.cpp:141-148: a voxel counts where the mask equals 1
+        c[i] = flair[i] == 1 ? 1 : 0;
+    }
+    BK(cudaMalloc(&b->d_t1c, N));
+    BK(cudaMalloc(&b->d_flair, N));
+    BK(cudaMemcpy(b->d_t1c, a.data(), N, cudaMemcpyHostToDevice));
+    BK(cudaMemcpy(b->d_flair, c.data(), N, cudaMemcpyHostToDevice));
+    if (pet) {
+        BK(cudaMalloc(&b->d_pet, N * sizeof(double)));
+        BK(cudaMemcpy(b->d_pet, pet, N * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (roi && nroi > 0) {
+        BK(cudaMalloc(&b->d_roi, (size_t)nroi * 3 * sizeof(int)));
+        BK(cudaMemcpy(b->d_roi, roi, (size_t)nroi * 3 * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    b->nroi = roi ? nroi : 0;
+    b->have_obs = true;
+    return GBFK_OK;
+}
+
+int gbfk_batch_log_likelihood(gbfk_batch *b, const gbfk_likelihood_params *p, double *out)
+{
+    if (!b) return GBFK_E_INVALID;
+    if (!p || !out) return bfail(b, GBFK_E_INVALID, "batch_log_likelihood: null argument");
+    if (!b->have_obs) return bfail(b, GBFK_E_STATE, "batch_log_likelihood: no observations");
+    if (!b->ran) return bfail(b, GBFK_E_STATE, "batch_log_likelihood: the batch has not run");
+    if (p->step_pet <= 0 || p->step_mri <= 0 || !(p->slope != 0))
+        return bfail(b, GBFK_E_INVALID, "batch_log_likelihood: bad parameters");
+    BK(cudaSetDevice(b->device));
+    return b->precision == GBFK_F64 ? batch_likelihood<double>(b, p, out) : batch_likelihood<float>(b, p, out);
 }
 
 }  // extern "C"

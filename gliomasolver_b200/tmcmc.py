@@ -124,6 +124,28 @@ class Batch:
         pipelined step, 1/2/4 = the per-block kernel, 0 = autotune."""
         self._check(self.lib.gbfk_batch_run(self.b, int(samples_per_cta)))
 
+    def set_observations(self, t1c, flair, pet=None, roi=None):
+        """Observations of the likelihood step on the batch's n^3 grid (as
+        BlockPool.set_observations), shared by every sample."""
+        t1 = np.ascontiguousarray(t1c, dtype=np.float64)
+        fl = np.ascontiguousarray(flair, dtype=np.float64)
+        pe = None if pet is None else np.ascontiguousarray(pet, dtype=np.float64)
+        ro = None if roi is None else np.ascontiguousarray(roi, dtype=np.int32).reshape(-1, 3)
+        self._keep_obs = (t1, fl, pe, ro)
+        ptr = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        self._check(self.lib.gbfk_batch_set_observations(self.b, ptr(t1), ptr(fl), ptr(pe), ptr(ro),
+                                                         0 if ro is None else ro.shape[0]))
+
+    def log_likelihood(self, pet_sigma2=0.000361, pet_scale=0.85, t1_uc=0.7, t2_uc=0.25, slope=2.0, step_pet=1,
+                       step_mri=1) -> np.ndarray:
+        """[L_PET, L_T1c, L_FLAIR, sum] of every sample after run(), shape
+        (samples, 4), in the order of set_samples (HGG_Likelihood::run)."""
+        p = _lib.LikelihoodParams(pet_sigma2, pet_scale, t1_uc, t2_uc, slope, step_pet, step_mri)
+        n = len(self._samples) if self._samples is not None else 0
+        out = np.empty((n, 4), dtype=np.float64)
+        self._check(self.lib.gbfk_batch_log_likelihood(self.b, ctypes.byref(p), out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
     def download(self, sample: int) -> np.ndarray:
         out = np.empty((self.n, self.n, self.n), dtype=self.dtype)
         self._check(self.lib.gbfk_batch_download(self.b, int(sample), out.ctypes.data_as(ctypes.c_void_p)))

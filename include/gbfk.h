@@ -231,6 +231,17 @@ int gbfk_uq_dump(gbfk_ctx *ctx, int n, double *host_out);
  * out[1] = T1c, out[2] = FLAIR, out[3] = their sum (the reference writes
  * -out[3] to Likelihood.txt).  Sums are FP64 with compensation. */
 int gbfk_log_likelihood(gbfk_ctx *ctx, const gbfk_likelihood_params *params, double out[4]);
+/* The likelihood step of every sample after the run, on the device: in the
+ * reference each TMCMC sample dumps its state to a file
+ * (Glioma_ReactionDiffusion.cpp:208-262) and a separate likelihood process
+ * reads it (HGG_Likelihood::run, HGG_Likelihood.cpp:176-192).  Observations
+ * as for gbfk_set_observations, on the batch's n^3 grid, shared by all
+ * samples; gbfk_batch_log_likelihood writes out[4 * s .. 4 * s + 3] =
+ * PET, T1c, FLAIR and their sum for sample s (the caller's order).  The
+ * grid is uniform, so the dump is the samples' own cells. */
+int gbfk_batch_set_observations(gbfk_batch *b, const double *t1c, const double *flair, const double *pet,
+                                const int *roi, int nroi);
+int gbfk_batch_log_likelihood(gbfk_batch *b, const gbfk_likelihood_params *params, double *out);
 
 /* --- discrete adjoint ------------------------------------------------- */
 /* No counterpart in the reference (which samples with TMCMC and never

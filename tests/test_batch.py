@@ -73,3 +73,48 @@ def test_batch_equals_sequential_solves(gbfk_lib, prec):
         assert c0[i].max() > 0.5
         for spc, res in results.items():
             assert np.array_equal(res[i], want), (i, spc)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_batch_likelihood_equals_per_sample_likelihood(gbfk_lib, prec):
+    """The likelihood step run on the device after a batch equals, for every
+    sample, the dump + likelihood of the same sample solved alone (same
+    observations: T1c / FLAIR masks, PET signal, ROI subset)."""
+    from gliomasolver_b200 import BlockPool
+    from gliomasolver_b200.tmcmc import Batch
+
+    R = np.float64 if prec == "f64" else np.float32
+    bpd, n = 4, 32
+    pw, pg, _ = make_anatomy(n, 2)
+    pw, pg = pw.astype(R), pg.astype(R)
+    stage = sample_stage(6, pw, seed=4, tend_range=(5.0, 30.0))
+    samples, scheds = to_gbfk_samples(stage, bpd, prec)
+    rng = np.random.default_rng(9)
+    t1 = (rng.random((n, n, n)) < 0.05).astype(float)
+    fl = np.maximum(t1, (rng.random((n, n, n)) < 0.1)).astype(float)
+    pet = rng.random((n, n, n)) * 0.3
+    roi = rng.integers(0, n, (200, 3))
+    kw = dict(step_pet=2, step_mri=1)
+    with Batch(bpd, 6, prec) as b:
+        b.set_anatomy(0, pw, pg)
+        zero, _ = to_gbfk_samples(stage, bpd, prec)
+        for r in zero:
+            r.nsteps = 0
+        b.set_samples(zero)
+        b.run(1)
+        c0 = [b.download(i) for i in range(6)]
+        b.set_samples(samples)
+        b.run(0)
+        b.set_observations(t1, fl, pet, roi)
+        got = b.log_likelihood(**kw)
+    with BlockPool(bpd ** 3, prec) as pool:
+        pool.set_uniform(bpd)
+        pool.upload_dense("p_w", pw)
+        pool.upload_dense("p_g", pg)
+        pool.set_observations(t1, fl, pet, roi)
+        for i, s in enumerate(scheds):
+            pool.upload_dense("phi", c0[i])
+            pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, s.nsteps)
+            assert np.array_equal(got[i], pool.log_likelihood(**kw)), i
+    assert np.all(np.isfinite(got)) and len({tuple(r) for r in got}) == 6
