@@ -23,6 +23,7 @@ STATUS = {
     6: "GBFK_E_STATE",
     7: "GBFK_E_TOO_LARGE",
 }
+STATUS_CODES = {v: k for k, v in STATUS.items()}
 GBFK_F64, GBFK_F32 = 0, 1
 GBFK_PHI, GBFK_PW, GBFK_PG = 0, 1, 2
 # step kernels (gbfk_set_step_kernel)
@@ -169,7 +170,7 @@ def load(path: Path | str | None = None):
         "gbfk_batch_samples_per_cta": (I, [P]),
         "gbfk_batch_download": (I, [P, I, P]),
         "gbfk_batch_set_observations": (I, [P, P, P, P, P, I]),
-        "gbfk_batch_log_likelihood": (I, [P, ctypes.POINTER(LikelihoodParams), P]),
+        "gbfk_batch_log_likelihood": (I, [P, ctypes.POINTER(LikelihoodParams), I, P]),
         "gbfk_forward_adjoint": (I, [P, ctypes.POINTER(AdjointParams), ctypes.POINTER(AdjointResult), P]),
     }
     for name, (res, args) in sig.items():

@@ -362,34 +362,35 @@ int batch_run(gbfk_batch *b, int spc)
     unsigned err = 0;
     BK(cudaMemcpy(&err, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (err) return bfail(b, GBFK_E_TIMEOUT, "batch_run: a wait of the pipelined step timed out (1 s)");
+    b->ran = true;  // final states, NaN ones included
     std::vector<unsigned> flags(b->nsamples);
     BK(cudaMemcpy(flags.data(), b->d_nan, b->nsamples * sizeof(unsigned), cudaMemcpyDeviceToHost));
     for (int k = 0; k < b->nsamples; k++)
         if (flags[k]) return bfail(b, GBFK_E_NAN, "sample %d became NaN", b->order[k]);
-    b->ran = true;
     return GBFK_OK;
 }
 
 template <typename Real>
-int batch_likelihood(gbfk_batch *b, const gbfk_likelihood_params *p, double *out)
+int batch_likelihood(gbfk_batch *b, const gbfk_likelihood_params *params, int per_sample, double *out)
 {
     const int n = b->n, nparts = 148 * 4;
     const size_t N = (size_t)n * n * n;
     if (!b->d_model) BK(cudaMalloc(&b->d_model, N * sizeof(double)));
     if (!b->d_partial) BK(cudaMalloc(&b->d_partial, (size_t)nparts * 7 * sizeof(double)));
     if (!b->d_lik) BK(cudaMalloc(&b->d_lik, (size_t)b->max_samples * 4 * sizeof(double)));
-    LikelihoodParams lp;
-    lp.pet_sigma2 = p->pet_sigma2;
-    lp.pet_scale = p->pet_scale;
-    lp.t1_uc = p->t1_uc;
-    lp.t2_uc = p->t2_uc;
-    lp.slope = p->slope;
-    lp.step_pet = p->step_pet;
-    lp.step_mri = p->step_mri;
     const size_t field = (size_t)b->nblocks * kBS3;
     int64_t grid = (N + 255) / 256;
     if (grid > 148 * 32) grid = 148 * 32;
     for (int s = 0; s < b->nsamples; s++) {
+        const gbfk_likelihood_params *p = params + (per_sample ? s : 0);
+        LikelihoodParams lp;
+        lp.pet_sigma2 = p->pet_sigma2;
+        lp.pet_scale = p->pet_scale;
+        lp.t1_uc = p->t1_uc;
+        lp.t2_uc = p->t2_uc;
+        lp.slope = p->slope;
+        lp.step_pet = p->step_pet;
+        lp.step_mri = p->step_mri;
         const Real *final = (const Real *)b->phi_all[b->params[s].nsteps & 1] + (size_t)b->pos[s] * field;
         pool_to_dense_kernel<Real><<<(int)grid, 256, 0, b->stream>>>(final, n, b->d_model);
         BK(cudaGetLastError());
@@ -631,16 +632,20 @@ int gbfk_batch_set_observations(gbfk_batch *b, const double *t1c, const double *
     return GBFK_OK;
 }
 
-int gbfk_batch_log_likelihood(gbfk_batch *b, const gbfk_likelihood_params *p, double *out)
+int gbfk_batch_log_likelihood(gbfk_batch *b, const gbfk_likelihood_params *params, int per_sample, double *out)
 {
     if (!b) return GBFK_E_INVALID;
-    if (!p || !out) return bfail(b, GBFK_E_INVALID, "batch_log_likelihood: null argument");
+    if (!params || !out) return bfail(b, GBFK_E_INVALID, "batch_log_likelihood: null argument");
     if (!b->have_obs) return bfail(b, GBFK_E_STATE, "batch_log_likelihood: no observations");
     if (!b->ran) return bfail(b, GBFK_E_STATE, "batch_log_likelihood: the batch has not run");
-    if (p->step_pet <= 0 || p->step_mri <= 0 || !(p->slope != 0))
-        return bfail(b, GBFK_E_INVALID, "batch_log_likelihood: bad parameters");
+    for (int s = 0; s < (per_sample ? b->nsamples : 1); s++) {
+        const gbfk_likelihood_params *p = params + s;
+        if (p->step_pet <= 0 || p->step_mri <= 0 || !(p->slope != 0))
+            return bfail(b, GBFK_E_INVALID, "batch_log_likelihood: bad parameters (set %d)", s);
+    }
     BK(cudaSetDevice(b->device));
-    return b->precision == GBFK_F64 ? batch_likelihood<double>(b, p, out) : batch_likelihood<float>(b, p, out);
+    return b->precision == GBFK_F64 ? batch_likelihood<double>(b, params, per_sample, out)
+                                    : batch_likelihood<float>(b, params, per_sample, out);
 }
 
 }  // extern "C"

@@ -139,14 +139,219 @@ class Batch:
     def log_likelihood(self, pet_sigma2=0.000361, pet_scale=0.85, t1_uc=0.7, t2_uc=0.25, slope=2.0, step_pet=1,
                        step_mri=1) -> np.ndarray:
         """[L_PET, L_T1c, L_FLAIR, sum] of every sample after run(), shape
-        (samples, 4), in the order of set_samples (HGG_Likelihood::run)."""
-        p = _lib.LikelihoodParams(pet_sigma2, pet_scale, t1_uc, t2_uc, slope, step_pet, step_mri)
+        (samples, 4), in the order of set_samples (HGG_Likelihood::run).
+        pet_sigma2 .. slope may be scalars or one value per sample."""
         n = len(self._samples) if self._samples is not None else 0
+        cols = [np.broadcast_to(np.asarray(v, dtype=np.float64), (n,)) for v in
+                (pet_sigma2, pet_scale, t1_uc, t2_uc, slope)]
+        per_sample = any(np.ndim(v) > 0 for v in (pet_sigma2, pet_scale, t1_uc, t2_uc, slope))
+        m = n if per_sample else 1
+        ps = (_lib.LikelihoodParams * max(m, 1))()
+        for i in range(m):
+            ps[i] = _lib.LikelihoodParams(*(float(c[i]) for c in cols), int(step_pet), int(step_mri))
         out = np.empty((n, 4), dtype=np.float64)
-        self._check(self.lib.gbfk_batch_log_likelihood(self.b, ctypes.byref(p), out.ctypes.data_as(ctypes.c_void_p)))
+        self._check(self.lib.gbfk_batch_log_likelihood(self.b, ps, int(per_sample), out.ctypes.data_as(ctypes.c_void_p)))
         return out
 
     def download(self, sample: int) -> np.ndarray:
         out = np.empty((self.n, self.n, self.n), dtype=self.dtype)
         self._check(self.lib.gbfk_batch_download(self.b, int(sample), out.ctypes.data_as(ctypes.c_void_p)))
         return out
+
+
+# ---------------------------------------------------------------------------
+# In-process TMCMC (transitional Markov chain Monte Carlo).
+#
+# The reference's engine (tools/pi4u_lite/Inference/engine_tmcmc.c with
+# tmcmc_stats.c) tempers the likelihood, L^p_j with p_0 = 0 .. 1, stage by
+# stage.  Per stage: the next exponent makes the coefficient of variation of
+# the plausibility weights L^(p_{j+1} - p_j) equal TolCOV
+# (calculate_statistics, tmcmc_stats.c:545-620); the stage's log-evidence
+# factor is log(sum w) + max - log n (:641-652); PopSize leaders are drawn
+# multinomially by weight; the proposal covariance is bbeta times the
+# weighted sample covariance (:700-757, compute_candidate engine_tmcmc.c:
+# 661-681, redrawn until inside the bounds); chains longer than
+# MaxChainLength are split (prepare_newgen :880-900); each chain step is a
+# Metropolis decision at p_{j+1} with a uniform prior (chaintask :683-738).
+# Here every chain's step k of a stage is evaluated in one call of the
+# log-likelihood over all proposals (one batched launch for the glioma model)
+# instead of one solver process per sample.
+
+@dataclass
+class TMCMCOptions:
+    pop_size: int = 512
+    max_stages: int = 100
+    tol_cov: float = 1.0          # TolCOV
+    bbeta: float = 0.2            # proposal covariance scale
+    min_chain: int = 0            # MinChainLength
+    max_chain: int = 1            # MaxChainLength
+    seed: int = 280675
+    penalty: float = -1.0e12      # log-likelihood of a failed / NaN evaluation (fitfun_glioma.c:203-217)
+
+
+@dataclass
+class TMCMCResult:
+    theta: np.ndarray             # final population (pop_size, d)
+    loglik: np.ndarray            # its log-likelihoods
+    p: list                       # tempering exponents p_0 = 0 .. p_last
+    log_evidence: float
+    acceptance: list              # per stage: accepted proposals / proposals
+    evaluations: int
+
+
+def _cov_of_weights(F, dp):
+    w = np.exp((F - F.max()) * dp)
+    q = w / w.sum()
+    return q.std(ddof=1) / q.mean()
+
+
+def next_exponent(F, p, tol_cov):
+    """p_{j+1} in (p, 1] with COV(L^(p_{j+1} - p)) = tol_cov (bisection on
+    the increasing COV), or 1 when even p_{j+1} = 1 stays below it."""
+    if _cov_of_weights(F, 1.0 - p) <= tol_cov:
+        return 1.0
+    lo, hi = p, 1.0
+    for _ in range(100):
+        mid = 0.5 * (lo + hi)
+        if _cov_of_weights(F, mid - p) > tol_cov:
+            hi = mid
+        else:
+            lo = mid
+    return max(lo, p + 1e-12)
+
+
+def _posdef(S):
+    """The symmetric part of S with its eigenvalues raised to a small
+    positive floor (the reference forces positive definiteness,
+    posdef.c)."""
+    S = 0.5 * (S + S.T)
+    w, V = np.linalg.eigh(S)
+    floor = max(w.max(), 1e-300) * 1e-12
+    return (V * np.maximum(w, floor)) @ V.T
+
+
+def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions()):
+    """Sample the posterior of a uniform prior on the box [lower, upper]
+    times exp(loglik).  ``loglik(theta)`` takes an (n, d) array and returns n
+    log-likelihoods (NaN/inf count as ``opts.penalty``)."""
+    rng = np.random.default_rng(opts.seed)
+    lower = np.asarray(lower, dtype=np.float64)
+    upper = np.asarray(upper, dtype=np.float64)
+    d = lower.size
+    nevals = 0
+
+    def evaluate(th):
+        nonlocal nevals
+        nevals += len(th)
+        F = np.asarray(loglik(th), dtype=np.float64)
+        return np.where(np.isfinite(F), F, opts.penalty)
+
+    theta = lower + (upper - lower) * rng.random((opts.pop_size, d))
+    F = evaluate(theta)
+    p = [0.0]
+    log_ev = 0.0
+    acc = []
+    for _ in range(opts.max_stages):
+        pj = p[-1]
+        pn = next_exponent(F, pj, opts.tol_cov)
+        flcp = F * (pn - pj)
+        w = np.exp(flcp - flcp.max())
+        log_ev += np.log(w.sum()) + flcp.max() - np.log(len(F))
+        q = w / w.sum()
+        sel = rng.multinomial(opts.pop_size, q)
+        mean = q @ theta
+        dev = theta - mean
+        cov = _posdef(opts.bbeta * (dev.T * q) @ dev)
+        # leaders with chain lengths (split at max_chain, raised to min_chain)
+        chains = []
+        for i in np.flatnonzero(sel):
+            k = int(sel[i])
+            while opts.max_chain > 0 and k > opts.max_chain:
+                chains.append([i, opts.max_chain])
+                k -= opts.max_chain
+            chains.append([i, max(k, opts.min_chain)])
+        lead = np.array([theta[i] for i, _ in chains])
+        flead = np.array([F[i] for i, _ in chains])
+        steps = np.array([k for _, k in chains])
+        chol = np.linalg.cholesky(cov)
+        new_theta, new_F = [], []
+        naccept = nprop = 0
+        for s in range(int(steps.max()) if len(steps) else 0):
+            act = np.flatnonzero(steps > s)
+            cand = np.empty((len(act), d))
+            for j, c in enumerate(act):
+                for _try in range(10000):
+                    x = lead[c] + chol @ rng.standard_normal(d)
+                    if np.all(x >= lower) and np.all(x <= upper):
+                        break
+                else:
+                    x = np.clip(x, lower, upper)
+                cand[j] = x
+            fc = evaluate(cand)
+            u = rng.random(len(act))
+            ok = u < np.exp(np.minimum(0.0, (fc - flead[act]) * pn))
+            naccept += int(ok.sum())
+            nprop += len(act)
+            lead[act[ok]] = cand[ok]
+            flead[act[ok]] = fc[ok]
+            new_theta.append(lead[act].copy())
+            new_F.append(flead[act].copy())
+        theta = np.concatenate(new_theta) if new_theta else theta
+        F = np.concatenate(new_F) if new_F else F
+        p.append(pn)
+        acc.append(naccept / max(nprop, 1))
+        if pn >= 1.0:
+            break
+    return TMCMCResult(theta, F, p, float(log_ev), acc, nevals)
+
+
+class GliomaModel:
+    """The likelihood of the reference's glioma calibration
+    (fitfun_glioma.c:128-151) evaluated for a whole population at once:
+    theta = log of (Dw [cm^2/day], rho [1/day], c = Tend^2 rho, x0, y0, z0,
+    PET sigma, PET scale, T1c threshold, FLAIR threshold, sigmoid slope)
+    rows; every row's forward solve runs in one batch and its likelihood on
+    the device after it."""
+
+    def __init__(self, p_w, p_g, t1c, flair, pet=None, roi=None, L_cm=25.6, precision="f32", max_samples=4096,
+                 device=0, stream=None, step_pet=1, step_mri=1):
+        n = p_w.shape[0]
+        if n % 8:
+            raise ValueError("the grid must be 8 * blocks per direction")
+        self.bpd = n // 8
+        self.n = n
+        self.L_cm = L_cm
+        self.precision = precision
+        self.steps = (step_pet, step_mri)
+        self.batch = Batch(self.bpd, max_samples, precision, device=device, stream=stream)
+        R = np.float64 if precision == "f64" else np.float32
+        self.batch.set_anatomy(0, p_w.astype(R), p_g.astype(R))
+        self.batch.set_observations(t1c, flair, pet, roi)
+        self.max_samples = max_samples
+
+    def parameters(self, theta):
+        v = np.exp(np.asarray(theta, dtype=np.float64))
+        Dw, rho = v[:, 0], v[:, 1]
+        tend = np.sqrt(v[:, 2] / rho)
+        return Dw, rho, tend, v[:, 3:6], v[:, 6] ** 2, v[:, 7], v[:, 8], v[:, 9], v[:, 10]
+
+    def __call__(self, theta):
+        Dw, rho, tend, x0, pet_s2, pet_scale, t1uc, t2uc, slope = self.parameters(theta)
+        out = np.empty(len(Dw))
+        for a in range(0, len(Dw), self.max_samples):
+            sl = slice(a, min(a + self.max_samples, len(Dw)))
+            stage = [StageSample(float(Dw[i]), float(rho[i]), float(tend[i]), tuple(x0[i])) for i in
+                     range(sl.start, sl.stop)]
+            samples, _ = to_gbfk_samples(stage, self.bpd, self.precision, self.L_cm)
+            self.batch.set_samples(samples)
+            try:
+                self.batch.run(0)
+            except GbfkError as e:
+                if e.code != _lib.STATUS_CODES["GBFK_E_NAN"]:
+                    raise
+            lik = self.batch.log_likelihood(pet_s2[sl], pet_scale[sl], t1uc[sl], t2uc[sl], slope[sl], *self.steps)
+            out[sl] = lik[:, 3]
+        return out
+
+    def close(self):
+        self.batch.close()

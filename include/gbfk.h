@@ -237,11 +237,14 @@ int gbfk_log_likelihood(gbfk_ctx *ctx, const gbfk_likelihood_params *params, dou
  * reads it (HGG_Likelihood::run, HGG_Likelihood.cpp:176-192).  Observations
  * as for gbfk_set_observations, on the batch's n^3 grid, shared by all
  * samples; gbfk_batch_log_likelihood writes out[4 * s .. 4 * s + 3] =
- * PET, T1c, FLAIR and their sum for sample s (the caller's order).  The
- * grid is uniform, so the dump is the samples' own cells. */
+ * PET, T1c, FLAIR and their sum for sample s (the caller's order), with
+ * params[0] for every sample or, if per_sample, params[s] (a TMCMC sample
+ * carries its own PET and threshold parameters, fitfun_glioma.c:128-151).
+ * The grid is uniform, so the dump is the samples' own cells.  After a run
+ * that reported GBFK_E_NAN the values of the NaN samples are NaN. */
 int gbfk_batch_set_observations(gbfk_batch *b, const double *t1c, const double *flair, const double *pet,
                                 const int *roi, int nroi);
-int gbfk_batch_log_likelihood(gbfk_batch *b, const gbfk_likelihood_params *params, double *out);
+int gbfk_batch_log_likelihood(gbfk_batch *b, const gbfk_likelihood_params *params, int per_sample, double *out);
 
 /* --- discrete adjoint ------------------------------------------------- */
 /* No counterpart in the reference (which samples with TMCMC and never
