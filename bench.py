@@ -315,6 +315,79 @@ def adjoint_sample(stream, local, bpd=16, nsnap=64):
     }
 
 
+def adjoint_batch(stream, local, nsamples=16, bpd=32, nsnap=64, seed=5):
+    """Config 5: forward + discrete adjoint for 16 samples at 256^3, FP32 state,
+    each sample with its own seeded anatomy (brain scale U[0.8, 1.2]) and
+    parameters sampled as in config 3 (Dw log-U[0.02,0.3], rho
+    log-U[0.002,0.2], T U[30,300] d, x0 in white matter).  Observations: the
+    sample's own forward run thresholded at 0.7 / 0.25 with 2% label noise;
+    gradients at Dw * 1.1, rho * 0.9.  The samples run one after the other
+    (one gbfk_forward_adjoint call each; 64 checkpoint buffers of 67 MB).
+    Sample 0 is repeated in FP64 for the FP32-vs-FP64 gradient error."""
+    import torch
+
+    from gliomasolver_b200 import BlockPool
+    from gliomasolver_b200.anatomy import make_anatomy, tumor_ic
+    from gliomasolver_b200.tmcmc import sample_stage
+
+    n = 8 * bpd
+    rng = np.random.default_rng(seed)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    t_total, steps_total, recs = 0.0, 0, []
+    peak, _ = measured_peak()
+
+    def one(prec, p_w, p_g, st, masks=None):
+        R = np.float32 if prec == "f32" else np.float64
+        s = make_schedule(st.Dw_cm2_day, st.rho_day, st.tend_day, L_CM, bpd, prec)
+        with BlockPool(bpd ** 3, prec, device=local, stream=stream.cuda_stream) as pool:
+            pool.set_uniform(bpd)
+            pool.upload_dense("p_w", p_w.astype(R))
+            pool.upload_dense("p_g", p_g.astype(R))
+            if masks is None:
+                pool.upload_dense("phi", tumor_ic(n, st.x0, p_w, p_g).astype(R))
+                pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, s.nsteps)
+                u = pool.download_dense("phi").astype(np.float64)
+                masks = [(u > 0.7).astype(float), (u > 0.25).astype(float)]
+                for m in masks:
+                    flip = rng.random(m.shape) < 0.02
+                    m[flip] = 1 - m[flip]
+            pool.set_observations(*masks)
+            Dw = float(R(R(st.Dw_cm2_day * 1.1) / R(L_CM * L_CM)))
+            Dg = float(R(0.1 * Dw))
+            torch.cuda.synchronize()
+            e0, e1 = ev(), ev()
+            e0.record(stream)
+            res = pool.forward_adjoint(Dw, Dg, st.rho_day * 0.9, s.dt, s.nsteps, x0=st.x0, sigma=2.0 / n,
+                                       nsnapshots=nsnap)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return res, e0.elapsed_time(e1) / 1e3, s.nsteps, masks
+
+    first = None
+    for i in range(nsamples):
+        p_w, p_g, _ = make_anatomy(n, seed + 100 + i, scale=float(rng.uniform(0.8, 1.2)))
+        st = sample_stage(1, p_w, seed=seed + 200 + i)[0]
+        res, t, k, masks = one("f32", p_w, p_g, st)
+        t_total += t
+        steps_total += k
+        recs.append({"steps": k, "seconds": t, "loss": res["loss"], "dDw": res["dDw"], "drho": res["drho"]})
+        if first is None:
+            first = (p_w, p_g, st, res, masks)
+    p_w, p_g, st, r32, masks = first
+    r64 = one("f64", p_w, p_g, st, masks)[0]
+    rel = {k: abs(r32[k] - r64[k]) / max(abs(r64[k]), 1e-300) for k in ("loss", "dDw", "drho")}
+    alg = 9 * 4 * (n ** 3) * steps_total  # (4 forward + 5 adjoint) words per cell and step, FP32
+    return {
+        "workload": f"{nsamples} samples, forward + discrete adjoint at {n}^3, FP32 state, own anatomy each "
+                    f"(scale U[0.8,1.2]), config-3 parameter sampling, {nsnap} checkpoint buffers, one sample per call",
+        "samples": nsamples, "steps_total": steps_total, "seconds": t_total,
+        "gradient_samples_per_s": nsamples / t_total,
+        "roofline": {"achieved": alg / t_total / 1e9, "peak": peak, "unit": "GB/s", "frac": alg / t_total / 1e9 / peak,
+                     "algorithmic_bytes": "9 words (forward 4 + adjoint 5) x cells x steps; recomputation not counted"},
+        "fp32_vs_fp64_rel": rel, "per_sample": recs,
+    }
+
+
 def gpu_arm(args):
     import torch
     import torch.distributed as dist
@@ -420,9 +493,12 @@ def gpu_arm(args):
 
     batch = None
     adj = None
+    adj5 = None
     if not args.no_batch:
         batch = batched_stage(args, stream, local)
         adj = adjoint_sample(stream, local)
+    if args.adjoint_batch:
+        adj5 = adjoint_batch(stream, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -438,7 +514,7 @@ def gpu_arm(args):
             "vs_baseline": None, "dtype": prec, "data": "synthetic", "config": workload_config(n, prec),
             "parallelism": "replicas" if world > 1 else "single",
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-            "batched_stage": batch, "forward_adjoint": adj,
+            "batched_stage": batch, "forward_adjoint": adj, "forward_adjoint_16x256": adj5,
         }
         print(json.dumps(line), flush=True)
     pool.close()
@@ -458,6 +534,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched TMCMC-stage measurement")
+    ap.add_argument("--adjoint-batch", action="store_true",
+                    help="also run config 5 (16 gradient samples at 256^3, a few minutes)")
     ap.add_argument("--step-kernel", default="auto", choices=["auto", "block", "pipelined"],
                     help="step kernel of the resident solve (auto: pipelined on uniform power-of-two grids)")
     args = ap.parse_args()
