@@ -520,7 +520,7 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
               Real rho, double dt, double inv_Dw, double *__restrict__ grad_acc)
 {
     __shared__ __align__(16) Real ph[kStepLab];
-    __shared__ double red[4][128];
+    __shared__ double red[4][4];
     const int blk = blockIdx.x, t = threadIdx.x;
     const int64_t base = slot_of(v, blk) * kBS3;
     const int x4 = (t & 1) * 4, y = (t >> 1) & 7, z = t >> 4;
@@ -584,7 +584,7 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
     lam.load(lam_next + base + c0);
     Vec4<Real> out;
     unsigned char fl[4];
-#pragma unroll 1
+#pragma unroll
     for (int i = 0; i < 4; i++) {
         const int x = x4 + i;
         const Real ph0 = p.v[i];
@@ -596,6 +596,7 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
             const int l = l0 + i;
             Real phn[6] = {ph[l - 1], ph[l + 1], ph[l - kPitch], ph[l + kPitch], ph[l - kPlane], ph[l + kPlane]};
             bool low[6];
+#pragma unroll
             for (int k = 0; k < 6; k++) {
                 bool slow;
                 if ((mw[i] >> (2 + k)) & 1u) {
@@ -617,12 +618,14 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
             const int rx = (z * 8 + y) * 9 + x, ry = 576 + (z * 9 + y) * 8 + x, rz = 1152 + (z * 8 + y) * 8 + x;
             Real df[6] = {Hb[rx], Hb[rx + 1], Hb[ry], Hb[ry + 8], Hb[rz], Hb[rz + 64]};
             // _applyNoFluxBC: neighbour k below 0.1 doubles the opposite coefficient k^1
+#pragma unroll
             for (int k = 0; k < 6; k++)
                 if (low[k]) {
                     df[k ^ 1] = rmul(df[k ^ 1], (Real)2.0);
                     f |= (unsigned char)(1u << (1 + (k ^ 1)));
                 }
             Real sin_ = rmul(df[0], phn[0]);
+#pragma unroll
             for (int k = 1; k < 6; k++) sin_ = radd(sin_, rmul(df[k], phn[k]));
             const double fluxIn = __dmul_rn(ih2, (double)sin_);
             const Real sdf = radd(radd(radd(radd(radd(df[0], df[1]), df[2]), df[3]), df[4]), df[5]);
@@ -643,20 +646,32 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
     }
     out.store(mu + base + c0);
     *reinterpret_cast<uchar4 *>(flags + base + c0) = make_uchar4(fl[0], fl[1], fl[2], fl[3]);
-    // CTA partials, accumulated into this CTA's own slot (deterministic: one
-    // writer per slot and launches are ordered on the stream)
-    red[0][t] = grho; red[1][t] = grho_c; red[2][t] = gdw; red[3][t] = gdw_c;
-    __syncthreads();
-    for (int w = 64; w > 0; w >>= 1) {
-        if (t < w) {
-            neumaier_add(red[0][t], red[1][t], red[0][t + w]);
-            neumaier_add(red[0][t], red[1][t], red[1][t + w]);
-            neumaier_add(red[2][t], red[3][t], red[2][t + w]);
-            neumaier_add(red[2][t], red[3][t], red[3][t + w]);
-        }
-        __syncthreads();
+    // CTA partials (warp shuffles, then the 4 warps in order), accumulated
+    // into this CTA's own slot (deterministic: one writer per slot and
+    // launches are ordered on the stream)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double a0 = __shfl_down_sync(0xffffffffu, grho, off), a1 = __shfl_down_sync(0xffffffffu, grho_c, off);
+        const double b0 = __shfl_down_sync(0xffffffffu, gdw, off), b1 = __shfl_down_sync(0xffffffffu, gdw_c, off);
+        neumaier_add(grho, grho_c, a0);
+        neumaier_add(grho, grho_c, a1);
+        neumaier_add(gdw, gdw_c, b0);
+        neumaier_add(gdw, gdw_c, b1);
     }
+    if ((t & 31) == 0) {
+        red[0][t >> 5] = grho;
+        red[1][t >> 5] = grho_c;
+        red[2][t >> 5] = gdw;
+        red[3][t >> 5] = gdw_c;
+    }
+    __syncthreads();
     if (t == 0) {
+        for (int w = 1; w < 4; w++) {
+            neumaier_add(red[0][0], red[1][0], red[0][w]);
+            neumaier_add(red[0][0], red[1][0], red[1][w]);
+            neumaier_add(red[2][0], red[3][0], red[2][w]);
+            neumaier_add(red[2][0], red[3][0], red[3][w]);
+        }
         double *acc = grad_acc + (int64_t)blk * kGradSlots;
         neumaier_add(acc[0], acc[1], red[0][0]);
         neumaier_add(acc[0], acc[1], red[1][0]);
@@ -707,7 +722,7 @@ adj_lambda_kernel(PoolView<Real> v, const Real *__restrict__ H, const double *__
     const Real *Hb = H + (int64_t)blk * kFacesPerBlock;
     const double ih2 = ih2blk[blk];
     Vec4<Real> out;
-#pragma unroll 1
+#pragma unroll
     for (int i = 0; i < 4; i++) {
         const int x = x4 + i;
         const int l = l0 + i;
@@ -720,10 +735,12 @@ adj_lambda_kernel(PoolView<Real> v, const Real *__restrict__ H, const double *__
         double acc = 0;
         if (fj & 1u) {
             double sdf = 0;
+#pragma unroll
             for (int k = 0; k < 6; k++) sdf += ((fj >> (1 + k)) & 1u) ? 2. * hf[k] : hf[k];
             const double ph0 = (double)p.v[i];
             acc += muj * (-ih2 * sdf + (double)rho * (1. - 2. * ph0));
         }
+#pragma unroll
         for (int k = 0; k < 6; k++) {
             const unsigned fi = sfl[ln[k]];
             if (!(fi & 1u)) continue;
