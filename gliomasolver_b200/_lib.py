@@ -22,6 +22,7 @@ STATUS = {
     5: "GBFK_E_TIMEOUT",
     6: "GBFK_E_STATE",
     7: "GBFK_E_TOO_LARGE",
+    8: "GBFK_E_IO",
 }
 STATUS_CODES = {v: k for k, v in STATUS.items()}
 GBFK_F64, GBFK_F32 = 0, 1
@@ -42,6 +43,7 @@ EXPORTS = (
     "gbfk_batch_set_anatomy", "gbfk_batch_set_samples", "gbfk_batch_run", "gbfk_batch_samples_per_cta",
     "gbfk_batch_download", "gbfk_batch_set_observations", "gbfk_batch_log_likelihood",
     "gbfk_forward_adjoint",
+    "gbfk_host_last_error", "gbfk_matrix_info", "gbfk_matrix_read", "gbfk_matrix_write", "gbfk_map_anatomy",
 )
 
 
@@ -172,6 +174,12 @@ def load(path: Path | str | None = None):
         "gbfk_batch_set_observations": (I, [P, P, P, P, P, I]),
         "gbfk_batch_log_likelihood": (I, [P, ctypes.POINTER(LikelihoodParams), I, P]),
         "gbfk_forward_adjoint": (I, [P, ctypes.POINTER(AdjointParams), ctypes.POINTER(AdjointResult), P]),
+        "gbfk_host_last_error": (ctypes.c_char_p, []),
+        "gbfk_matrix_info": (I, [ctypes.c_char_p, ctypes.POINTER(I), ctypes.POINTER(I * 3), ctypes.POINTER(I)]),
+        "gbfk_matrix_read": (I, [ctypes.c_char_p, P, I64]),
+        "gbfk_matrix_write": (I, [ctypes.c_char_p, I, ctypes.POINTER(I * 3), I, P]),
+        "gbfk_map_anatomy": (I, [I, I, ctypes.POINTER(I * 3), P, P, P, ctypes.POINTER(D * 3), P, P, P, P, P,
+                                 ctypes.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -11,7 +11,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 SOURCES = ["csrc/gbfk_kernels.cu", "csrc/gbfk_api.cu", "csrc/gbfk_static.cu", "csrc/gbfk_uq.cu", "csrc/gbfk_batch.cu",
-           "csrc/gbfk_step_tma.cu"]
+           "csrc/gbfk_step_tma.cu", "csrc/gbfk_patient.cpp"]
 OUT = HERE / "libgbfk.so"
 
 NVCC_FLAGS = [
@@ -20,7 +20,7 @@ NVCC_FLAGS = [
     "-lineinfo",
     # the RD arithmetic must round exactly like the reference's CPU code
     "-fmad=false",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared",
 ]
 
 

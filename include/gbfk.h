@@ -52,7 +52,8 @@ enum gbfk_status {
     GBFK_E_NAN = 4,     /* a step produced NaN/Inf in phi */
     GBFK_E_TIMEOUT = 5, /* a bounded device wait gave up */
     GBFK_E_STATE = 6,   /* required data (topology, fields) not uploaded */
-    GBFK_E_TOO_LARGE = 7 /* grid larger than gbfk_rd_step_static's fixed scratch */
+    GBFK_E_TOO_LARGE = 7, /* grid larger than gbfk_rd_step_static's fixed scratch */
+    GBFK_E_IO = 8         /* a file could not be opened, read or written, or is malformed */
 };
 
 enum gbfk_precision { GBFK_F64 = 0, GBFK_F32 = 1 };
@@ -274,6 +275,51 @@ typedef struct {
 /* grad_c0_dense: NULL, or n^3 Real (x fastest) receiving d loss / d c0. */
 int gbfk_forward_adjoint(gbfk_ctx *ctx, const gbfk_adjoint_params *params, gbfk_adjoint_result *out,
                          void *grad_c0_dense);
+
+/* --- patient data: Matrix files and the anatomy mapping ---------------- */
+/* Host-only functions (no GPU, no context).  Their failure message is
+ * gbfk_host_last_error(), kept per calling thread. */
+const char *gbfk_host_last_error(void);
+/* The reference's Matrix file (Glioma/Matrix.h:20-34,71-88,141-240 and the
+ * D2D/D3D dump/load at :390-445,609-665; the likelihood program reads the
+ * same layout through its own copy of Matrix.h): int32 1234 (the magic
+ * number; a byte-swapped file fails it), int32 dim (2 or 3), dim int32
+ * sizes (x first), int32 type id (0 double, 1 float, 2 int32), then the
+ * values, x fastest.  gbfk_matrix_info reads the header; sizes[d] = 1 for
+ * d >= dim.  GBFK_E_IO for a missing file, a short read, a wrong magic
+ * number, a dim other than 2 or 3, a negative size or an unknown type id
+ * (the reference prints a message and keeps an unusable matrix). */
+int gbfk_matrix_info(const char *path, int *dim, int sizes[3], int *type_id);
+/* All values converted to double, as MatrixD2D/MatrixD3D<double> load them
+ * (Matrix.h:116-169): capacity must hold sizes[0]*sizes[1]*sizes[2] values. */
+int gbfk_matrix_read(const char *path, double *out, int64_t capacity);
+/* Writes data (sizes[0]*...*sizes[dim-1] doubles, x fastest) with the given
+ * type id (Matrix.h:184-240): float rounds to nearest, int32 truncates
+ * towards zero and rejects values outside int32 (GBFK_E_INVALID). */
+int gbfk_matrix_write(const char *path, int dim, const int *sizes, int type_id, const double *data);
+/* Glioma_ReactionDiffusion::_ic (Glioma/Glioma_ReactionDiffusion.cpp:79-172)
+ * on the uniform bpd^3-block grid the reference constructs before its first
+ * refinement: for each cell at vertex position x (BlockInfo::pos,
+ * MRAG/MRAGcore/MRAGCommon.h:199-205) the anatomy voxel floor(x / (1/M)),
+ * M = max(msize), is mapped when it lies inside the volumes (all fields stay
+ * 0 elsewhere, the Cell defaults of Glioma/Glioma_Types.h:54-77); CSF wins
+ * the majority vote against p_w + p_g (:144-147), p_w and p_g are then
+ * normalised by the remaining tissue (:149-151), and the tumour is the
+ * smoothed ball of radius 0.005 and width 1/64 around tumor_ic (:157-164).
+ *   gm, wm, csf : msize[0] x msize[1] x msize[2] doubles, x fastest (the
+ *                 MatrixD3D files {prefix}GM.dat, WM.dat, CSF.dat);
+ *   tumor_ic    : tumour centre in the unit cube, rounded to Real;
+ *   pw, pg, pcsf, phi : NULL or dense (8*bpd)^3 Real outputs, x fastest;
+ *   tissue      : NULL or dense (8*bpd)^3 Real: p_w + p_g after the vote and
+ *                 before the normalisation (the tumour's tissue test);
+ *   L           : NULL or the characteristic length M * 0.1 (cm) in Real.
+ * Arithmetic follows the reference in its Real (GBFK_F64: double; GBFK_F32:
+ * float, with the mixed float/double expressions of the reference's default
+ * build), so the outputs are bit-identical to the reference's cells.  Runs
+ * on host threads over z-planes. */
+int gbfk_map_anatomy(int precision, int bpd, const int msize[3], const double *gm, const double *wm,
+                     const double *csf, const double tumor_ic[3], void *pw, void *pg, void *pcsf, void *phi,
+                     void *tissue, double *L);
 
 /* --- allocation-free step -------------------------------------------- */
 /* No counterpart in the reference.  One fused RD step (the operator and the

@@ -73,6 +73,8 @@ def _declare(L):
     L.orc_collapse_blocks_f32.argtypes = [P, P]
     L.orc_uq_dump_f64.argtypes = [I, P, P, P, P, I, P]
     L.orc_uq_dump_f32.argtypes = [I, P, P, P, P, I, P]
+    L.orc_map_anatomy_f64.argtypes = [I, I, I, I, P, P, P, P, P, P, P, P, P]
+    L.orc_map_anatomy_f32.argtypes = [I, I, I, I, P, P, P, P, P, P, P, P, P]
     L.orc_log_likelihood.argtypes = [I, P, P, P, P, P, I, D, D, D, D, D, I, I, P]
 
 
@@ -175,6 +177,20 @@ def log_likelihood(model, t1c, flair, pet=None, roi=None, pet_sigma2=0.000361, p
     return np.array([float(out[0]), float(out[1]), float(out[2])])
 
 
+def map_anatomy(gm, wm, csf, bpd, tumor_ic, precision="f64"):
+    """Glioma_ReactionDiffusion::_ic restated (orc_map_anatomy_*): dense
+    (8 bpd)^3 arrays p_w, p_g, p_csf, phi, tissue in the precision's Real."""
+    vols = [np.ascontiguousarray(v, dtype=np.float64) for v in (gm, wm, csf)]
+    sz, sy, sx = vols[0].shape
+    dtype = np.float64 if precision == "f64" else np.float32
+    n = 8 * int(bpd)
+    outs = [np.zeros((n, n, n), dtype=dtype) for _ in range(5)]
+    tic = np.ascontiguousarray(tumor_ic, dtype=np.float64)
+    getattr(lib(), f"orc_map_anatomy_{precision}")(int(bpd), sx, sy, sz, *(_p(v) for v in vols), _p(tic),
+                                                    *(_p(o) for o in outs))
+    return dict(zip(("p_w", "p_g", "p_csf", "phi", "tissue"), outs))
+
+
 # ------------------------------------------------- the reference's own code
 def ref_available(precision: str = "f64") -> bool:
     return (REF_DIR / f"ref_harness_{precision}").exists()
@@ -270,3 +286,26 @@ def ref_likelihood(model, t1c, flair, pet, roi=None, pet_sigma2=0.000361, pet_sc
         r = subprocess.run(args, cwd=td, check=True, capture_output=True, text=True)
         with open(os.path.join(td, "Likelihood.txt")) as f:
             return float(f.read().split()[0]), r.stdout
+
+
+def ref_ic_available(precision: str = "f64") -> bool:
+    return (REF_DIR / f"ic_harness_{precision}").exists()
+
+
+def ref_map_anatomy(prefix, bpd, tumor_ic, precision="f64"):
+    """Run the reference's own Glioma_ReactionDiffusion::_ic on
+    {prefix}GM.dat, WM.dat, CSF.dat (oracle/_ref/ic_harness_*).  Returns a
+    dict with L, p_w, p_g, p_csf, phi (float64 copies of the Real cells) and
+    the seconds _ic took."""
+    n = 8 * int(bpd)
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "ic.bin")
+        r = subprocess.run([str(REF_DIR / f"ic_harness_{precision}"), os.fspath(prefix), str(int(bpd)),
+                            *(_fmt(v) for v in tumor_ic), out], check=True, capture_output=True, text=True)
+        rec = json.loads(r.stdout.strip().splitlines()[-1])
+        raw = np.fromfile(out, dtype=np.float64)
+    n3 = n ** 3
+    res = {"L": float(raw[0]), "seconds": rec["ic_seconds"]}
+    for k, name in enumerate(("p_w", "p_g", "p_csf", "phi")):
+        res[name] = raw[1 + k * n3:1 + (k + 1) * n3].reshape(n, n, n)
+    return res

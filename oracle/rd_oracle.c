@@ -412,3 +412,70 @@ void orc_log_likelihood(int n, const double *model, const double *t1c, const dou
         out[ti] = sum;
     }
 }
+
+/* Glioma_ReactionDiffusion::_ic (Glioma/Glioma_ReactionDiffusion.cpp:79-172),
+ * restated cell by cell in the build's Real.  In the float build the
+ * reference mixes float and double: the voxel index divides a float
+ * position by a double spacing (:125-127), `double tissue = pWM + pGM` adds
+ * in float (:144,149), the normalisation divides in double (:150-151), the
+ * tumour distance is float (:155-157) and the smoothing profile evaluates
+ * (1 - psi) in float and the rest in double (:161-162). */
+#define ORC_MAP_ANATOMY(SUF, Real, SQRT)                                                                        \
+    void orc_map_anatomy_##SUF(int bpd, int sx, int sy, int sz, const double *gm, const double *wm,             \
+                               const double *csf, const double tumor_ic[3], Real *pw, Real *pg, Real *pcsf,     \
+                               Real *phi, Real *tissue_out)                                                     \
+    {                                                                                                          \
+        int level = 0;                                                                                         \
+        while ((1 << level) < bpd) level++;                                                                    \
+        const int n = 8 * bpd;                                                                                 \
+        const Real hcell = (Real)(1.0 / (8 << level)); /* BlockInfo::h = 2^-level / 8 */                       \
+        int smax = sx > sy ? sx : sy;                                                                          \
+        smax = smax > sz ? smax : sz;                                                                          \
+        const double brainHx = 1.0 / ((double)smax); /* :98 */                                                 \
+        const Real tumorRadius = 0.005, smooth_sup = 2., hs = 1. / 128; /* :103-105 */                         \
+        const Real iw = 1. / (smooth_sup * hs);                           /* :106 */                           \
+        const Real ic[3] = {(Real)tumor_ic[0], (Real)tumor_ic[1], (Real)tumor_ic[2]};                          \
+        for (int iz = 0; iz < n; iz++)                                                                         \
+            for (int iy = 0; iy < n; iy++)                                                                     \
+                for (int ix = 0; ix < n; ix++) {                                                               \
+                    const size_t c = ix + (size_t)n * (iy + (size_t)n * iz);                                   \
+                    /* origin = (i / 8) * 8 * hcell, + hcell * (i % 8): exact either way */                    \
+                    Real x[3];                                                                                 \
+                    x[0] = (Real)((ix / 8) * 8) * hcell + hcell * (ix % 8);                                    \
+                    x[1] = (Real)((iy / 8) * 8) * hcell + hcell * (iy % 8);                                    \
+                    x[2] = (Real)((iz / 8) * 8) * hcell + hcell * (iz % 8);                                    \
+                    const int mX = (int)floor(x[0] / brainHx);                                                 \
+                    const int mY = (int)floor(x[1] / brainHx);                                                 \
+                    const int mZ = (int)floor(x[2] / brainHx);                                                 \
+                    Real o_w = 0, o_g = 0, o_c = 0, o_phi = 0, o_t = 0;                                        \
+                    if (mX >= 0 && mX < sx && mY >= 0 && mY < sy && mZ >= 0 && mZ < sz) {                      \
+                        const size_t v = mX + (size_t)sx * (mY + (size_t)sy * mZ);                             \
+                        Real pGM = gm[v], pWM = wm[v], pCSF = csf[v];                                          \
+                        double tissue = pWM + pGM;                                                             \
+                        pCSF = (pCSF > tissue) ? 1. : 0.;                                                      \
+                        pWM = (pCSF > tissue) ? 0. : pWM;                                                      \
+                        pGM = (pCSF > tissue) ? 0. : pGM;                                                      \
+                        tissue = pWM + pGM;                                                                    \
+                        o_w = (tissue > 0.) ? (pWM / tissue) : 0.;                                             \
+                        o_g = (tissue > 0.) ? (pGM / tissue) : 0.;                                             \
+                        o_c = pCSF;                                                                            \
+                        o_t = pGM + pWM;                                                                       \
+                        const Real p[3] = {x[0] - ic[0], x[1] - ic[1], x[2] - ic[2]};                          \
+                        const Real dist = SQRT(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);                       \
+                        const Real psi = (dist - tumorRadius) * iw;                                            \
+                        if ((psi < -1) && (pGM + pWM > 0.001))                                                 \
+                            o_phi = 1.0;                                                                       \
+                        else if (((-1 <= psi) && (psi <= 1)) && (pGM + pWM > 0))                               \
+                            o_phi = 1.0 * 0.5 * (1 - psi - sin(M_PI * psi) / (M_PI));                          \
+                        else                                                                                   \
+                            o_phi = 0.0;                                                                       \
+                    }                                                                                          \
+                    if (pw) pw[c] = o_w;                                                                       \
+                    if (pg) pg[c] = o_g;                                                                       \
+                    if (pcsf) pcsf[c] = o_c;                                                                   \
+                    if (phi) phi[c] = o_phi;                                                                   \
+                    if (tissue_out) tissue_out[c] = o_t;                                                       \
+                }                                                                                              \
+    }
+ORC_MAP_ANATOMY(f64, double, sqrt)
+ORC_MAP_ANATOMY(f32, float, sqrtf)

@@ -116,6 +116,19 @@ void orc_log_likelihood(int n, const double *model, const double *t1c, const dou
                         const int *roi, int nroi, double pet_sigma2, double pet_scale, double t1uc,
                         double t2uc, double slope, int step_pet, int step_mri, long double out[3]);
 
+/* Glioma_ReactionDiffusion::_ic (Glioma/Glioma_ReactionDiffusion.cpp:79-172)
+ * on the uniform grid of bpd blocks per direction (level ceil(log2 bpd),
+ * MRAG/MRAGcore/MRAGridHelpers.h:9-17), n = 8*bpd cells per direction, cell
+ * positions x = i * 2^-level / 8.  gm, wm, csf: sx*sy*sz doubles, x fastest
+ * (MatrixD3D).  Outputs (n^3 Real each, x fastest, any may be NULL): p_w,
+ * p_g, p_csf, phi and the tissue sum p_g + p_w after the vote that the
+ * tumour test uses.  Cells whose voxel lies outside the volumes stay 0. */
+void orc_map_anatomy_f64(int bpd, int sx, int sy, int sz, const double *gm, const double *wm, const double *csf,
+                         const double tumor_ic[3], double *pw, double *pg, double *pcsf, double *phi,
+                         double *tissue);
+void orc_map_anatomy_f32(int bpd, int sx, int sy, int sz, const double *gm, const double *wm, const double *csf,
+                         const double tumor_ic[3], float *pw, float *pg, float *pcsf, float *phi, float *tissue);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,45 @@
+"""A patient case through the device path: Matrix files mapped by
+gbfk_map_anatomy (the reference's _ic), uploaded to a block pool and stepped
+on the GPU with the schedule of the mapped characteristic length; the
+result must equal the oracle's steps on the same cells bit for bit."""
+import numpy as np
+import pytest
+
+from gliomasolver_b200 import BlockPool, patient
+from gliomasolver_b200.schedule import make_schedule
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _volumes(shape, seed):
+    """A smooth brain-like volume: tissue inside an ellipsoid, CSF in a core."""
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(*(np.linspace(-1, 1, s) for s in shape), indexing="ij")
+    r = np.sqrt((x / 0.9) ** 2 + (y / 0.8) ** 2 + (z / 0.85) ** 2)
+    wm = np.clip(1.2 - r, 0, 1) * rng.uniform(0.8, 1.0, shape)
+    gm = np.clip(1.0 - np.abs(r - 0.8) * 3, 0, 1) * rng.uniform(0.8, 1.0, shape)
+    csf = np.where(r < 0.15, 1.0, 0.0) + np.where(r > 1.0, 0.3, 0.0)
+    return gm, wm, csf
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_patient_case_steps_like_the_oracle(gbfk_lib, tmp_path, prec):
+    bpd, tic = 4, (0.3 + 0.004, 0.5 - 0.006, 0.4 + 0.002)
+    for k, v in zip(("GM", "WM", "CSF"), _volumes((36, 44, 40), 1)):
+        patient.write_matrix(tmp_path / f"P_{k}.dat", v, type_id=1)
+    a = patient.load_patient(tmp_path / "P_", bpd, tic, prec)
+    assert np.count_nonzero(a.phi) > 0 and a.L_cm == pytest.approx(4.4)
+    s = make_schedule(0.13, 0.025, 150.0, a.L_cm, bpd, prec)
+    n = 8 * bpd
+    steps = min(int(s.nsteps), 60)
+    with BlockPool(bpd ** 3, prec) as pool:
+        pool.set_uniform(bpd)
+        pool.upload_dense("p_w", a.p_w)
+        pool.upload_dense("p_g", a.p_g)
+        pool.upload_dense("phi", a.phi)
+        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, steps, check_nan=True)
+        out = pool.download_dense("phi")
+    want = O.rd_steps_dense(a.p_w, a.p_g, a.phi, s.Dw, s.Dg, s.rho, s.h, s.dt, steps)
+    assert out.shape == (n, n, n)
+    assert np.array_equal(out, want)
