@@ -93,7 +93,12 @@ class Sample(ctypes.Structure):
         ("anatomy", ctypes.c_int),
         ("x0", ctypes.c_double * 3),
         ("sigma", ctypes.c_double),
+        ("ic", ctypes.c_int),
     ]
+
+
+# initial conditions of a batch sample (enum gbfk_ic)
+IC_KINDS = {"gaussian": 0, "ball": 1}
 
 
 class AdjointParams(ctypes.Structure):

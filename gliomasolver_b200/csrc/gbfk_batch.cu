@@ -14,6 +14,7 @@
 // every sample (the pipelined step, gbfk_step_tma.cu).
 #include "gbfk.h"
 #include "gbfk_exact.cuh"
+#include "gbfk_host.h"
 #include "gbfk_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -81,6 +82,9 @@ struct gbfk_batch {
     double *d_model = nullptr;   // one sample's dump grid
     double *d_partial = nullptr; // likelihood partial sums
     double *d_lik = nullptr;     // 4 per sample
+    // GBFK_IC_BALL samples: band cells (int64 pool index) and their values
+    void *d_ball = nullptr;
+    size_t ball_cap = 0;
     int64_t launches = 0;
     std::string err;
 };
@@ -154,6 +158,18 @@ __global__ void ic_kernel(int n, int bpd, const Real *__restrict__ pw, const Rea
         const double r2 = (x - x0) * (x - x0) + (y - y0) * (y - y0) + (z - z0) * (z - z0);
         const double v = exp(-r2 / (2. * sigma * sigma));
         out[i] = (pw[i] + pg[i] > (Real)0) ? (Real)v : (Real)0;
+    }
+}
+
+// The reference's smoothed-ball tumour of a sample: the band cells computed
+// on the host, scattered into the zeroed state where the cell has tissue.
+template <typename Real>
+__global__ void ball_ic_kernel(int count, const int64_t *__restrict__ cell, const Real *__restrict__ value,
+                               const Real *__restrict__ pw, const Real *__restrict__ pg, Real *__restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const int64_t c = cell[i];
+        out[c] = (pw[c] + pg[c] > (Real)0) ? value[i] : (Real)0;
     }
 }
 
@@ -233,6 +249,45 @@ int batch_prepare(gbfk_batch *b)
                      [&](int i, int j) { return b->params[i].nsteps > b->params[j].nsteps; });
     b->pos.assign(b->nsamples, 0);
     for (int k = 0; k < b->nsamples; k++) b->pos[b->order[k]] = k;
+    // band cells of every GBFK_IC_BALL sample in pool order, one upload
+    std::vector<int64_t> bcell;
+    std::vector<Real> bval;
+    std::vector<size_t> boff(b->nsamples + 1, 0);
+    {
+        std::vector<gbfk_host::BallCell<Real>> cells;
+        const int bpd = b->bpd;
+        for (int k = 0; k < b->nsamples; k++) {
+            const gbfk_sample &p = b->params[b->order[k]];
+            if (p.ic == GBFK_IC_BALL) {
+                if (!gbfk_host::ball_band_cells<Real>(bpd, p.x0, cells))
+                    return bfail(b, GBFK_E_INVALID, "sample %d: a cell in the ball's core", b->order[k]);
+                for (const auto &c : cells) {
+                    const int64_t slot = (c.x >> 3) + (int64_t)bpd * ((c.y >> 3) + (int64_t)bpd * (c.z >> 3));
+                    bcell.push_back(slot * kBS3 + (c.x & 7) + 8 * ((c.y & 7) + 8 * (c.z & 7)));
+                    bval.push_back(c.value);
+                }
+            }
+            boff[k + 1] = bcell.size();
+        }
+    }
+    const size_t nball = bcell.size();
+    const size_t val_off = (nball * sizeof(int64_t) + 255) & ~(size_t)255;
+    if (nball) {
+        const size_t need = val_off + nball * sizeof(Real);
+        if (need > b->ball_cap) {
+            if (b->d_ball) BK(cudaFree(b->d_ball));
+            b->d_ball = nullptr;
+            b->ball_cap = 0;
+            if (cudaMalloc(&b->d_ball, need) != cudaSuccess) {
+                cudaGetLastError();
+                return bfail(b, GBFK_E_OOM, "ball initial conditions: %zu bytes", need);
+            }
+            b->ball_cap = need;
+        }
+        BK(cudaMemcpyAsync(b->d_ball, bcell.data(), nball * sizeof(int64_t), cudaMemcpyHostToDevice, b->stream));
+        BK(cudaMemcpyAsync((char *)b->d_ball + val_off, bval.data(), nball * sizeof(Real), cudaMemcpyHostToDevice,
+                           b->stream));
+    }
     // face coefficients and meta words of every sample's (anatomy, Dw, Dg);
     // initial conditions in the parity-0 buffer
     for (int k = 0; k < b->nsamples; k++) {
@@ -245,10 +300,24 @@ int batch_prepare(gbfk_batch *b)
                               b->meta[p.anatomy], b->btype[p.anatomy], b->stream));
         int64_t nb = ((int64_t)b->nblocks * kBS3 + 255) / 256;
         if (nb > 148 * 32) nb = 148 * 32;
-        ic_kernel<Real><<<(int)nb, 256, 0, b->stream>>>(b->n, b->bpd, v.pw, v.pg, p.x0[0], p.x0[1], p.x0[2],
-                                                         p.sigma, pos_field<Real>(b, b->phi_all[0], k, kBS3));
-        BK(cudaGetLastError());
-        b->launches += 2;
+        Real *phi0 = pos_field<Real>(b, b->phi_all[0], k, kBS3);
+        if (p.ic == GBFK_IC_BALL) {
+            BK(cudaMemsetAsync(phi0, 0, (size_t)b->nblocks * kBS3 * sizeof(Real), b->stream));
+            const int count = (int)(boff[k + 1] - boff[k]);
+            if (count > 0) {
+                ball_ic_kernel<Real><<<(count + 255) / 256, 256, 0, b->stream>>>(
+                    count, (const int64_t *)b->d_ball + boff[k], (const Real *)((char *)b->d_ball + val_off) + boff[k],
+                    v.pw, v.pg, phi0);
+                BK(cudaGetLastError());
+                b->launches++;
+            }
+        } else {
+            ic_kernel<Real><<<(int)nb, 256, 0, b->stream>>>(b->n, b->bpd, v.pw, v.pg, p.x0[0], p.x0[1], p.x0[2],
+                                                             p.sigma, phi0);
+            BK(cudaGetLastError());
+            b->launches++;
+        }
+        b->launches++;
     }
     std::vector<SampleView<Real>> views(b->nsamples);
     std::vector<Real> rho(b->nsamples);
@@ -499,7 +568,7 @@ int gbfk_batch_destroy(gbfk_batch *b)
     void *ptrs[] = {b->d_nbr,       b->d_ih2,    b->d_views, b->d_nan,      b->d_err,     b->d_rho, b->d_dt,
                     b->d_lists,     b->pw_all,   b->pg_all,  b->meta_all,   b->btype_all, b->phi_all[0],
                     b->phi_all[1],  b->H_all,    b->d_t1c,   b->d_flair,    b->d_pet,     b->d_roi, b->d_model,
-                    b->d_partial,   b->d_lik};
+                    b->d_partial,   b->d_lik,    b->d_ball};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -549,7 +618,10 @@ int gbfk_batch_set_samples(gbfk_batch *b, int nsamples, const gbfk_sample *sampl
         const gbfk_sample &p = samples[s];
         if (p.anatomy < 0 || p.anatomy >= b->max_anatomies || !b->anatomy_set[p.anatomy])
             return bfail(b, GBFK_E_STATE, "sample %d: anatomy %d not set", s, p.anatomy);
-        if (p.nsteps < 0 || !(p.sigma > 0)) return bfail(b, GBFK_E_INVALID, "sample %d: bad nsteps or sigma", s);
+        if (p.ic != GBFK_IC_GAUSSIAN && p.ic != GBFK_IC_BALL)
+            return bfail(b, GBFK_E_INVALID, "sample %d: initial condition %d", s, p.ic);
+        if (p.nsteps < 0 || (p.ic == GBFK_IC_GAUSSIAN && !(p.sigma > 0)))
+            return bfail(b, GBFK_E_INVALID, "sample %d: bad nsteps or sigma", s);
     }
     b->nsamples = nsamples;
     b->params.assign(samples, samples + nsamples);

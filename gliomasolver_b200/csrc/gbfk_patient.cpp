@@ -8,6 +8,7 @@
 // float/double mix of the default float build; glibc's sin and the IEEE
 // division and square root give the same bits as the reference's cells.
 #include "gbfk.h"
+#include "gbfk_host.h"
 
 #include <algorithm>
 #include <cerrno>
@@ -101,6 +102,45 @@ struct MapArgs {
     void *pw, *pg, *pcsf, *phi, *tissue;
 };
 
+// The tumour profile of _ic at one cell (:155-164), in Real: 0 = the ball's
+// core (psi < -1), 1 = the smoothing band (-1 <= psi <= 1; *value is the
+// profile there), 2 = outside (also for a NaN psi, as the reference's
+// comparisons then all fail).
+template <class Real>
+inline int ball_zone(const Real x[3], const Real tic[3], Real *value)
+{
+    // :103-106: tumour radius, smoothing support and width (fixed h = 1/128)
+    const Real tumorRadius = (Real)0.005;
+    const Real smooth_sup = (Real)2.;
+    const Real h = (Real)(1. / 128);
+    const Real iw = (Real)(1. / (smooth_sup * h));
+    const Real p[3] = {(Real)(x[0] - tic[0]), (Real)(x[1] - tic[1]), (Real)(x[2] - tic[2])};
+    const Real dist = std::sqrt((Real)((Real)(p[0] * p[0]) + (Real)(p[1] * p[1])) + (Real)(p[2] * p[2]));
+    const Real psi = (Real)((Real)(dist - tumorRadius) * iw);
+    if (psi < (Real)-1) return 0;
+    if ((Real)-1 <= psi && psi <= (Real)1) {
+        *value = (Real)(1.0 * 0.5 * ((double)(Real)((Real)1 - psi) - sin(M_PI * (double)psi) / (M_PI)));
+        return 1;
+    }
+    return 2;
+}
+
+// BlockInfo::pos of grid cell i: origin + h * i, exact multiples of the spacing.
+template <class Real>
+inline Real cell_pos(int i, double spacing)
+{
+    return (Real)(i * spacing);
+}
+
+inline double grid_spacing(int bpd)
+{
+    // MRAG places bpd blocks at level ceil(log2 bpd) (MRAGridHelpers.h:9-17),
+    // block spacing 2^-level (MRAGrid.inl:200-212).
+    int level = 0;
+    while ((1 << level) < bpd) level++;
+    return 1.0 / (double)(8 << level);
+}
+
 // One z-plane range of Glioma_ReactionDiffusion::_ic (:117-167), in Real.
 template <class Real>
 void map_planes(const MapArgs &a, int z0, int z1)
@@ -108,11 +148,6 @@ void map_planes(const MapArgs &a, int z0, int z1)
     const int n = a.ncell;
     // :98-100: voxel spacing w.r.t. the longest dimension
     const double brainH = 1.0 / (double)a.mmax;
-    // :103-106: tumour radius, smoothing support and width (fixed h = 1/128)
-    const Real tumorRadius = (Real)0.005;
-    const Real smooth_sup = (Real)2.;
-    const Real h = (Real)(1. / 128);
-    const Real iw = (Real)(1. / (smooth_sup * h));
     const Real tic[3] = {(Real)a.tic[0], (Real)a.tic[1], (Real)a.tic[2]};
     Real *o_pw = (Real *)a.pw, *o_pg = (Real *)a.pg, *o_csf = (Real *)a.pcsf;
     Real *o_phi = (Real *)a.phi, *o_t = (Real *)a.tissue;
@@ -122,8 +157,8 @@ void map_planes(const MapArgs &a, int z0, int z1)
         for (int iy = 0; iy < n; iy++)
             for (int ix = 0; ix < n; ix++) {
                 const int64_t c = ix + (int64_t)n * (iy + (int64_t)n * iz);
-                // BlockInfo::pos: origin + h * i, exact multiples of the spacing
-                const Real x[3] = {(Real)(ix * a.inv_extent), (Real)(iy * a.inv_extent), (Real)(iz * a.inv_extent)};
+                const Real x[3] = {cell_pos<Real>(ix, a.inv_extent), cell_pos<Real>(iy, a.inv_extent),
+                                   cell_pos<Real>(iz, a.inv_extent)};
                 const int mx = (int)floor((double)x[0] / brainH);
                 const int my = (int)floor((double)x[1] / brainH);
                 const int mz = (int)floor((double)x[2] / brainH);
@@ -142,14 +177,13 @@ void map_planes(const MapArgs &a, int z0, int z1)
                     g = (tissue > 0.) ? (Real)((double)pGM / tissue) : (Real)0.;
                     f = pCSF;
                     t = (Real)(pGM + pWM);
-                    // :155-164
-                    const Real p[3] = {(Real)(x[0] - tic[0]), (Real)(x[1] - tic[1]), (Real)(x[2] - tic[2])};
-                    const Real dist = std::sqrt((Real)((Real)(p[0] * p[0]) + (Real)(p[1] * p[1])) + (Real)(p[2] * p[2]));
-                    const Real psi = (Real)((Real)(dist - tumorRadius) * iw);
-                    if ((psi < (Real)-1) && ((double)t > 0.001))
+                    // :157-164
+                    Real band = 0;
+                    const int zone = ball_zone<Real>(x, tic, &band);
+                    if (zone == 0 && (double)t > 0.001)
                         ph = (Real)1.0;
-                    else if (((Real)-1 <= psi && psi <= (Real)1) && ((double)t > 0))
-                        ph = (Real)(1.0 * 0.5 * ((double)(Real)((Real)1 - psi) - sin(M_PI * (double)psi) / (M_PI)));
+                    else if (zone == 1 && (double)t > 0)
+                        ph = band;
                     else
                         ph = (Real)0.0;
                 }
@@ -181,6 +215,43 @@ void map_all(const MapArgs &a)
 }
 
 }  // namespace
+
+namespace gbfk_host {
+
+template <class Real>
+bool ball_band_cells(int bpd, const double tic_d[3], std::vector<BallCell<Real>> &out)
+{
+    out.clear();
+    const int n = 8 * bpd;
+    const double sp = grid_spacing(bpd);
+    const Real tic[3] = {(Real)tic_d[0], (Real)tic_d[1], (Real)tic_d[2]};
+    // the band ends at radius 0.005 + 1/64; two cells of margin cover the
+    // rounding of the distance in Real
+    const double reach = 0.005 + 1. / 64;
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; d++) {
+        const double c = (double)tic[d];
+        if (!(c == c)) return true;  // NaN centre: every cell is outside
+        const double l = std::floor((c - reach) / sp) - 2, u = std::ceil((c + reach) / sp) + 2;
+        lo[d] = (int)std::max(0.0, std::min((double)n, l));
+        hi[d] = (int)std::max(-1.0, std::min((double)(n - 1), u));
+    }
+    for (int iz = lo[2]; iz <= hi[2]; iz++)
+        for (int iy = lo[1]; iy <= hi[1]; iy++)
+            for (int ix = lo[0]; ix <= hi[0]; ix++) {
+                const Real x[3] = {cell_pos<Real>(ix, sp), cell_pos<Real>(iy, sp), cell_pos<Real>(iz, sp)};
+                Real v = 0;
+                const int zone = ball_zone<Real>(x, tic, &v);
+                if (zone == 0) return false;
+                if (zone == 1) out.push_back(BallCell<Real>{ix, iy, iz, v});
+            }
+    return true;
+}
+
+template bool ball_band_cells<float>(int, const double[3], std::vector<BallCell<float>> &);
+template bool ball_band_cells<double>(int, const double[3], std::vector<BallCell<double>> &);
+
+}  // namespace gbfk_host
 
 extern "C" {
 
@@ -267,12 +338,8 @@ int gbfk_map_anatomy(int precision, int bpd, const int msize[3], const double *g
         a.mmax = std::max(a.mmax, msize[d]);
         a.tic[d] = tumor_ic[d];
     }
-    // MRAG places bpd blocks at level ceil(log2 bpd) (MRAGridHelpers.h:9-17),
-    // block spacing 2^-level (MRAGrid.inl:200-212).
-    int level = 0;
-    while ((1 << level) < bpd) level++;
     a.ncell = 8 * bpd;
-    a.inv_extent = 1.0 / (double)(8 << level);
+    a.inv_extent = grid_spacing(bpd);
     a.gm = gm;
     a.wm = wm;
     a.csf = csf;

@@ -45,8 +45,12 @@ def sample_stage(nsamples: int, p_w: np.ndarray, seed: int = 0, Dw_range=(0.02, 
             for i in range(nsamples)]
 
 
-def to_gbfk_samples(stage, blocks_per_dim: int, precision: str, L_cm: float = 25.6, anatomy=None):
-    """Per-sample schedules in the build's Real, as gbfk_sample records."""
+def to_gbfk_samples(stage, blocks_per_dim: int, precision: str, L_cm: float = 25.6, anatomy=None, ic="gaussian"):
+    """Per-sample schedules in the build's Real, as gbfk_sample records.
+    ``ic``: "gaussian" (c0 = exp(-|x-x0|^2 / (2 (2h)^2)), the synthetic
+    workloads' initial condition) or "ball" (the reference's smoothed-ball
+    tumour of Glioma_ReactionDiffusion::_ic)."""
+    kind = _lib.IC_KINDS[ic]
     n = 8 * blocks_per_dim
     out = (_lib.Sample * len(stage))()
     scheds = []
@@ -58,6 +62,7 @@ def to_gbfk_samples(stage, blocks_per_dim: int, precision: str, L_cm: float = 25
         r.anatomy = 0 if anatomy is None else int(anatomy[i])
         r.x0[0], r.x0[1], r.x0[2] = s.x0
         r.sigma = 2.0 / n
+        r.ic = kind
     return out, scheds
 
 
@@ -311,10 +316,12 @@ class GliomaModel:
     theta = log of (Dw [cm^2/day], rho [1/day], c = Tend^2 rho, x0, y0, z0,
     PET sigma, PET scale, T1c threshold, FLAIR threshold, sigmoid slope)
     rows; every row's forward solve runs in one batch and its likelihood on
-    the device after it."""
+    the device after it.  ``ic="ball"`` starts every row from the
+    reference's smoothed-ball tumour at (x0, y0, z0), as its TumorIC.txt
+    runs do (Glioma_ReactionDiffusion.cpp:39-52,155-164)."""
 
     def __init__(self, p_w, p_g, t1c, flair, pet=None, roi=None, L_cm=25.6, precision="f32", max_samples=4096,
-                 device=0, stream=None, step_pet=1, step_mri=1):
+                 device=0, stream=None, step_pet=1, step_mri=1, ic="gaussian"):
         n = p_w.shape[0]
         if n % 8:
             raise ValueError("the grid must be 8 * blocks per direction")
@@ -323,6 +330,7 @@ class GliomaModel:
         self.L_cm = L_cm
         self.precision = precision
         self.steps = (step_pet, step_mri)
+        self.ic = ic
         self.batch = Batch(self.bpd, max_samples, precision, device=device, stream=stream)
         R = np.float64 if precision == "f64" else np.float32
         self.batch.set_anatomy(0, p_w.astype(R), p_g.astype(R))
@@ -342,7 +350,7 @@ class GliomaModel:
             sl = slice(a, min(a + self.max_samples, len(Dw)))
             stage = [StageSample(float(Dw[i]), float(rho[i]), float(tend[i]), tuple(x0[i])) for i in
                      range(sl.start, sl.stop)]
-            samples, _ = to_gbfk_samples(stage, self.bpd, self.precision, self.L_cm)
+            samples, _ = to_gbfk_samples(stage, self.bpd, self.precision, self.L_cm, ic=self.ic)
             self.batch.set_samples(samples)
             try:
                 self.batch.run(0)

@@ -179,13 +179,24 @@ int gbfk_collapse(gbfk_ctx *ctx, int ncollapse, const int *children, const int *
  * every sample of a stage in GPU memory and advances all samples that have
  * not reached their own horizon with one launch per time step. */
 typedef struct gbfk_batch gbfk_batch;
+/* Initial conditions of a batch sample.  GBFK_IC_BALL is the reference's
+ * tumour of Glioma_ReactionDiffusion::_ic (Glioma_ReactionDiffusion.cpp:
+ * 155-164), the ball of radius 0.005 smoothed over a width of 1/64 around x0
+ * (x0 rounded to Real), where the cell has tissue; its values are computed
+ * on the host in the reference's arithmetic (only the cells near x0) and
+ * scattered into the zeroed state on the device, so they equal
+ * gbfk_map_anatomy's phi bit for bit.  The reference's inner core
+ * (psi < -1) is empty for that radius and width, and its band test
+ * pGM + pWM > 0 is p_w + p_g > 0 for non-negative fractions. */
+enum gbfk_ic { GBFK_IC_GAUSSIAN = 0, GBFK_IC_BALL = 1 };
 typedef struct {
     double Dw, Dg, rho; /* rescaled Real coefficients, as for gbfk_rd_step */
     double dt;          /* time step */
     int nsteps;         /* steps to this sample's horizon */
     int anatomy;        /* which anatomy (gbfk_batch_set_anatomy) */
     double x0[3];       /* tumour origin in the unit cube */
-    double sigma;       /* initial condition: c0 = exp(-|x-x0|^2/(2 sigma^2)) where p_w+p_g > 0 */
+    double sigma;       /* GBFK_IC_GAUSSIAN: c0 = exp(-|x-x0|^2/(2 sigma^2)) where p_w+p_g > 0 */
+    int ic;             /* enum gbfk_ic: the initial condition around x0 */
 } gbfk_sample;
 /* A batch on a uniform periodic bpd^3 grid with room for max_samples samples
  * and max_anatomies anatomies (2 phi buffers + face coefficients per sample). */
