@@ -27,7 +27,8 @@
  * dt = the reference's CFL formula (:304-307) with h of the finest level.
  *
  * Prints one JSON line (blocks and a hash of the sorted (level, index) list
- * after every adaptation, seconds spent stepping) and writes phi sampled on
+ * after every adaptation; seconds spent stepping, uploads included; seconds
+ * of the uploads and of the host refinements) and writes phi sampled on
  * the finest uniform grid (each finest cell takes the value of the leaf cell
  * that covers it) as int32 n + n^3 float64, x fastest.
  */
@@ -176,7 +177,8 @@ int main(int argc, char **argv)
      * timed loop (context creation is not stepping) */
     gbfk_mrag::Device *dev = mode == "gpu" ? new gbfk_mrag::Device((1 << (3 * maxLevel)) + 64) : NULL;
     BlockProcessing ref;
-    double t_step = 0;
+    double t_step = 0, t_upload = 0, t_adapt = 0;
+    int n_uploads = 0, n_refines = 0;
     long long cell_updates = 0;
     for (int done = 0; done < nsteps;) {
         const int k = std::min(every, nsteps - done);
@@ -186,7 +188,12 @@ int main(int argc, char **argv)
         if (mode == "ref") {
             for (int s = 0; s < k; s++) ref_step(grid, ref, Dw, Dg, rho, dt);
         } else {
-            if (!dev->same_leaves(vInfo)) dev->upload(vInfo, grid.getBlockCollection(), grid.getBoundaryInfo());
+            if (!dev->same_leaves(vInfo)) {
+                const double tu = now();
+                dev->upload(vInfo, grid.getBlockCollection(), grid.getBoundaryInfo());
+                t_upload += now() - tu;
+                n_uploads++;
+            }
             gbfk_mrag::check(dev->ctx, gbfk_rd_step(dev->ctx, Dw, Dg, rho, dt, k, 1), "gbfk_rd_step");
             /* AutomaticRefinement refines the blocks below maxlevel whose
              * detail is >= the tolerance (MRAGScienceCore.h:59-84); with
@@ -202,7 +209,12 @@ int main(int argc, char **argv)
         t_step += now() - t0;
         cell_updates += (long long)k * (long long)vInfo.size() * 512;
         done += k;
-        if (refine) Science::AutomaticRefinement<0, 0>(grid, blockfwt, rtol, maxLevel, 1, NULL);
+        if (refine) {
+            const double ta = now();
+            Science::AutomaticRefinement<0, 0>(grid, blockfwt, rtol, maxLevel, 1, NULL);
+            t_adapt += now() - ta;
+            n_refines++;
+        }
         int nb = 0;
         hashes.push_back(leaves_hash(grid, nb));
         nblocks.push_back(nb);
@@ -236,8 +248,10 @@ int main(int argc, char **argv)
     fclose(f);
 
     printf("{\"mode\": \"%s\", \"real_bytes\": %d, \"maxlevel\": %d, \"steps\": %d, \"every\": %d, \"dt\": %.17g, "
-           "\"step_seconds\": %.6f, \"cell_updates\": %lld, \"blocks\": [",
-           mode.c_str(), (int)sizeof(Real), maxLevel, nsteps, every, (double)dt, t_step, cell_updates);
+           "\"step_seconds\": %.6f, \"upload_seconds\": %.6f, \"uploads\": %d, \"adapt_seconds\": %.6f, "
+           "\"refinements\": %d, \"cell_updates\": %lld, \"blocks\": [",
+           mode.c_str(), (int)sizeof(Real), maxLevel, nsteps, every, (double)dt, t_step, t_upload, n_uploads,
+           t_adapt, n_refines, cell_updates);
     for (size_t i = 0; i < nblocks.size(); i++) printf("%s%d", i ? ", " : "", nblocks[i]);
     printf("], \"hashes\": [");
     for (size_t i = 0; i < hashes.size(); i++) printf("%s\"%016llx\"", i ? ", " : "", hashes[i]);
