@@ -96,6 +96,12 @@ struct gbfk_ctx {
     unsigned *d_nan = nullptr;        // [0]: NaN seen in a step, [1]: a pipeline stage wait timed out
     void *d_stage = nullptr;
     size_t stage_bytes = 0;
+    // gbfk_forward_adjoint's device buffers, kept from one call to the next
+    // (freed by gbfk_destroy, or replaced when a call needs other sizes or
+    // more checkpoint buffers)
+    std::vector<void *> adj_mem;
+    size_t adj_fbytes = 0;
+    int adj_nblocks = 0, adj_nsnap = 0;
     double *d_fwt = nullptr;
     int *d_ints = nullptr;
     size_t ints_cap = 0;
@@ -669,6 +675,8 @@ int gbfk_destroy(gbfk_ctx *ctx)
                     ctx->d_t1c, ctx->d_flair, ctx->d_pet, ctx->d_roi, ctx->d_model, ctx->d_partial, ctx->d_lik};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    for (void *p : ctx->adj_mem)
+        if (p) cudaFree(p);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return GBFK_OK;
@@ -1185,34 +1193,48 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     A.rho = (Real)p->rho;
     A.dt = p->dt;
     A.Dw = (double)(Real)p->Dw;
-    std::vector<void *> owned;
-    auto alloc = [&](size_t bytes, void **out) {
-        cudaError_t e = cudaMalloc(out, bytes);
-        if (e == cudaSuccess) owned.push_back(*out);
-        return e;
-    };
-    auto cleanup = [&]() {
-        cudaStreamSynchronize(ctx->stream);
-        for (void *q : owned) cudaFree(q);
-    };
-    Real *X0 = nullptr, *F = nullptr;
-    double *xpart = nullptr;
+    // buffers: X0, F, T0, T1, T2, LAM, MU, cell flags + block tails, gradient
+    // partials, x0-gradient partials, then the checkpoints; kept in the
+    // context between calls
     const int xparts = 148 * 4;
+    const size_t sizes[10] = {A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes,
+                              (size_t)nb * kAdjFlagBytesPerBlock, (size_t)nb * kGradSlots * sizeof(double),
+                              (size_t)xparts * 6 * sizeof(double)};
+    auto release = [&]() {
+        cudaStreamSynchronize(ctx->stream);
+        for (void *q : ctx->adj_mem)
+            if (q) cudaFree(q);
+        ctx->adj_mem.clear();
+        ctx->adj_fbytes = 0;
+        ctx->adj_nblocks = ctx->adj_nsnap = 0;
+    };
     cudaError_t e = cudaSuccess;
-    void **bufs[] = {(void **)&X0, (void **)&F, (void **)&A.T0, (void **)&A.T1, (void **)&A.T2, (void **)&A.LAM,
-                     (void **)&A.MU};
-    for (void **b : bufs)
-        if (e == cudaSuccess) e = alloc(A.fbytes, b);
-    if (e == cudaSuccess) e = alloc((size_t)nb * kBS3 + nb, (void **)&A.FL);  // per-cell flags + per-block tail
-    if (e == cudaSuccess) e = alloc((size_t)nb * kGradSlots * sizeof(double), (void **)&A.grad_acc);
-    if (e == cudaSuccess) e = alloc((size_t)xparts * 6 * sizeof(double), (void **)&xpart);
-    A.slots.assign(p->nsnapshots, nullptr);
-    for (int i = 0; i < p->nsnapshots && e == cudaSuccess; i++) e = alloc(A.fbytes, (void **)&A.slots[i]);
-    if (e != cudaSuccess) {
-        cleanup();
-        cudaGetLastError();
-        return fail(ctx, GBFK_E_OOM, "forward_adjoint: %s", cudaGetErrorString(e));
+    if (ctx->adj_fbytes != A.fbytes || ctx->adj_nblocks != nb || ctx->adj_nsnap < p->nsnapshots) {
+        release();
+        ctx->adj_mem.assign(10 + p->nsnapshots, nullptr);
+        for (size_t i = 0; i < ctx->adj_mem.size() && e == cudaSuccess; i++)
+            e = cudaMalloc(&ctx->adj_mem[i], i < 10 ? sizes[i] : A.fbytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            release();
+            return fail(ctx, GBFK_E_OOM, "forward_adjoint: %s", cudaGetErrorString(e));
+        }
+        ctx->adj_fbytes = A.fbytes;
+        ctx->adj_nblocks = nb;
+        ctx->adj_nsnap = p->nsnapshots;
     }
+    auto cleanup = [&]() { cudaStreamSynchronize(ctx->stream); };
+    Real *X0 = (Real *)ctx->adj_mem[0], *F = (Real *)ctx->adj_mem[1];
+    A.T0 = (Real *)ctx->adj_mem[2];
+    A.T1 = (Real *)ctx->adj_mem[3];
+    A.T2 = (Real *)ctx->adj_mem[4];
+    A.LAM = (Real *)ctx->adj_mem[5];
+    A.MU = (Real *)ctx->adj_mem[6];
+    A.FL = (unsigned char *)ctx->adj_mem[7];
+    A.grad_acc = (double *)ctx->adj_mem[8];
+    double *xpart = (double *)ctx->adj_mem[9];
+    A.slots.assign(p->nsnapshots, nullptr);
+    for (int i = 0; i < p->nsnapshots; i++) A.slots[i] = (Real *)ctx->adj_mem[10 + i];
     e = cudaMemsetAsync(A.grad_acc, 0, (size_t)nb * kGradSlots * sizeof(double), ctx->stream);
     // forward steps on the pipelined kernel where it applies (bit-identical)
     A.X0 = X0;
@@ -1279,11 +1301,17 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     if (e == cudaSuccess) {
         e = launch_loss_grad<Real>(bpd, F, ctx->d_t1c, ctx->d_flair, p->t1_uc, p->t2_uc, p->slope, A.LAM, ctx->stream);
         ctx->launches++;
+        // dL/dphi at the horizon is written in every block
+        if (e == cudaSuccess) e = cudaMemsetAsync(A.FL + (size_t)nb * (kBS3 + 1), 0, (size_t)nb, ctx->stream);
     }
-    // reverse sweep
+    // reverse sweep; then the zeros of the blocks where dL/dphi_0 vanishes
     if (e == cudaSuccess) {
         A.reverse(0, p->nsteps, p->nsnapshots, X0);
         e = A.err;
+    }
+    if (e == cudaSuccess) {
+        e = launch_adjoint_unsparse<Real>(A.v, A.FL, A.LAM, ctx->stream);
+        ctx->launches++;
     }
     // parameter gradients
     std::vector<double> acc((size_t)nb * kGradSlots);

@@ -503,6 +503,16 @@ cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigne
 // cell has mu = lambda' [0 < phi <= 1], no gradient terms and, unless a face
 // neighbour has a domain cell, lambda = mu: both kernels take that short
 // path without the halo, the coefficients or the reductions.
+// lambda and mu are block-sparse: mu (and so lambda) vanishes wherever
+// pre = 0, i.e. outside the tumour's support, so after the first adjoint
+// step most blocks are zero.  A block whose lambda' is zero in every cell
+// (lam_zero) has mu = 0 without a look at the forward state; a block whose
+// mu is zero records kAdjMuZero and writes neither mu nor flags; lambda of a
+// block is zero when its mu is and no face neighbour contributes, which
+// adj_lambda records in lam_zero instead of writing the cells.  Every value
+// equals the dense computation's (a zero block's cells are +0 where the
+// dense kernels could produce -0: a sign of zero that no later product or
+// sum turns into a different number).
 
 __device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
 {
@@ -512,16 +522,34 @@ __device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
     s = t;
 }
 
+// Per-block status of an adjoint step, written by adj_mu: exactly one of
+// 0 (mu not zero, no domain cell), kAdjDom (mu not zero, a domain cell) and
+// kAdjMuZero (mu is zero in every cell; its mu values and cell flags are not
+// written, and the block contributes nothing to any lambda).
+constexpr unsigned char kAdjDom = 1;
+constexpr unsigned char kAdjMuZero = 2;
+
+template <typename Real>
+__device__ __forceinline__ bool nonzero4(const Vec4<Real> &a)
+{
+    return a.v[0] != (Real)0 || a.v[1] != (Real)0 || a.v[2] != (Real)0 || a.v[3] != (Real)0;
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(128)
 adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
               const double *__restrict__ ih2blk, const Real *__restrict__ phi, const Real *__restrict__ lam_next,
-              Real *__restrict__ mu, unsigned char *__restrict__ flags, unsigned char *__restrict__ blk_dom,
-              Real rho, double dt, double inv_Dw, double *__restrict__ grad_acc)
+              const unsigned char *__restrict__ lam_zero, Real *__restrict__ mu, unsigned char *__restrict__ flags,
+              unsigned char *__restrict__ status, Real rho, double dt, double inv_Dw, double *__restrict__ grad_acc)
 {
     __shared__ __align__(16) Real ph[kStepLab];
     __shared__ double red[4][4];
     const int blk = blockIdx.x, t = threadIdx.x;
+    if (lam_zero[blk]) {
+        // lambda' = 0 in the block: mu = 0 whatever the step does, no gradient terms
+        if (t == 0) status[blk] = kAdjMuZero;
+        return;
+    }
     const int64_t base = slot_of(v, blk) * kBS3;
     const int x4 = (t & 1) * 4, y = (t >> 1) & 7, z = t >> 4;
     const int c0 = x4 + kBS * (y + kBS * z);
@@ -559,12 +587,15 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
             const Real pre = to_real<Real>(__dadd_rn((double)p.v[i], __dmul_rn(dt, 0.)));
             out.v[i] = (pre > (Real)0 && pre <= (Real)1) ? lam.v[i] : (Real)0;
         }
+        if (!__syncthreads_or(nonzero4(out))) {
+            if (t == 0) status[blk] = kAdjMuZero;
+            return;
+        }
         out.store(mu + base + c0);
         *reinterpret_cast<uchar4 *>(flags + base + c0) = make_uchar4(0, 0, 0, 0);
-        if (t == 0) blk_dom[blk] = 0;
+        if (t == 0) status[blk] = 0;
         return;
     }
-    if (t == 0) blk_dom[blk] = 1;
     p.store(ph + l0);
 #pragma unroll
     for (int i = 0; i < 3; i++) {
@@ -644,8 +675,13 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
             neumaier_add(gdw, gdw_c, (double)m * dt * flux_diff * inv_Dw);
         }
     }
-    out.store(mu + base + c0);
-    *reinterpret_cast<uchar4 *>(flags + base + c0) = make_uchar4(fl[0], fl[1], fl[2], fl[3]);
+    // a block whose mu is zero everywhere writes neither mu nor its flags
+    const bool written = __syncthreads_or(nonzero4(out));
+    if (written) {
+        out.store(mu + base + c0);
+        *reinterpret_cast<uchar4 *>(flags + base + c0) = make_uchar4(fl[0], fl[1], fl[2], fl[3]);
+    }
+    if (t == 0) status[blk] = written ? kAdjDom : kAdjMuZero;
     // CTA partials (warp shuffles, then the 4 warps in order), accumulated
     // into this CTA's own slot (deterministic: one writer per slot and
     // launches are ordered on the stream)
@@ -680,30 +716,49 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
     }
 }
 
+// lambda of a block from the mu and cell flags of the block and of its face
+// neighbours.  Only kAdjDom neighbours contribute (the others have no domain
+// cell or mu = 0); a kAdjMuZero block with no contributing neighbour has
+// lambda = 0 and records that in lam_zero instead of writing its cells.
 template <typename Real>
 __global__ void __launch_bounds__(128)
 adj_lambda_kernel(PoolView<Real> v, const Real *__restrict__ H, const double *__restrict__ ih2blk,
                   const Real *__restrict__ phi, const Real *__restrict__ mu, const unsigned char *__restrict__ flags,
-                  const unsigned char *__restrict__ blk_dom, Real *__restrict__ lam, Real rho, double dt)
+                  const unsigned char *__restrict__ status, Real *__restrict__ lam, unsigned char *__restrict__ lam_zero,
+                  Real rho, double dt)
 {
     __shared__ __align__(16) Real smu[kStepLab];
     __shared__ unsigned char sfl[kStepLab];
+    __shared__ unsigned char sst[8];
     const int blk = blockIdx.x, t = threadIdx.x;
+    // threads 0..5: the face neighbours, thread 6: the block itself
+    if (t < 7) sst[t] = status[t == 6 ? blk : face_neighbour(v, blk, t)];
+    __syncthreads();
+    const unsigned self = sst[6];
+    bool contrib = false;
+#pragma unroll
+    for (int f = 0; f < 6; f++) contrib |= sst[f] == kAdjDom;
+    if ((self & kAdjMuZero) && !contrib) {
+        if (t == 0) lam_zero[blk] = 1;
+        return;
+    }
+    if (t == 0) lam_zero[blk] = 0;
     const int64_t base = slot_of(v, blk) * kBS3;
     const int x4 = (t & 1) * 4, y = (t >> 1) & 7, z = t >> 4;
     const int c0 = x4 + kBS * (y + kBS * z);
     const int l0 = lab_p(x4, y, z);
+    const bool own = !(self & kAdjMuZero);
     Vec4<Real> m;
-    m.load(mu + base + c0);
-    // threads 0..5: the face neighbours, thread 6: the block itself
-    const int d = t < 7 ? blk_dom[t == 6 ? blk : face_neighbour(v, blk, t)] : 0;
-    if (!__syncthreads_or(d)) {
-        // no domain cell in the block or its face neighbours: lambda = mu
+    if (own) m.load(mu + base + c0);
+    else m.v[0] = m.v[1] = m.v[2] = m.v[3] = (Real)0;
+    if (!(self & kAdjDom) && !contrib) {
+        // no domain cell in the block and no contribution from its neighbours: lambda = mu
         m.store(lam + base + c0);
         return;
     }
     m.store(smu + l0);
-    const uchar4 f4 = *reinterpret_cast<const uchar4 *>(flags + base + c0);
+    uchar4 f4 = make_uchar4(0, 0, 0, 0);
+    if (own) f4 = *reinterpret_cast<const uchar4 *>(flags + base + c0);
     sfl[l0] = f4.x; sfl[l0 + 1] = f4.y; sfl[l0 + 2] = f4.z; sfl[l0 + 3] = f4.w;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
@@ -711,13 +766,19 @@ adj_lambda_kernel(PoolView<Real> v, const Real *__restrict__ H, const double *__
         const int f = q >> 6, pc = q & 63;
         int lx, ly, lz, sc;
         face_cell(f, pc, lx, ly, lz, sc);
-        const int nb = face_neighbour(v, blk, f);
         const int l = lab_p(lx, ly, lz);
-        smu[l] = mu[(int64_t)nb * kBS3 + sc];
-        sfl[l] = flags[(int64_t)nb * kBS3 + sc];
+        if (sst[f] == kAdjDom) {
+            const int nb = face_neighbour(v, blk, f);
+            smu[l] = mu[(int64_t)nb * kBS3 + sc];
+            sfl[l] = flags[(int64_t)nb * kBS3 + sc];
+        } else {
+            smu[l] = (Real)0;
+            sfl[l] = 0;
+        }
     }
     Vec4<Real> p;
-    p.load(phi + base + c0);
+    if (self & kAdjDom) p.load(phi + base + c0);
+    else p.v[0] = p.v[1] = p.v[2] = p.v[3] = (Real)0;  // no cell has the domain flag
     __syncthreads();
     const Real *Hb = H + (int64_t)blk * kFacesPerBlock;
     const double ih2 = ih2blk[blk];
@@ -753,16 +814,37 @@ adj_lambda_kernel(PoolView<Real> v, const Real *__restrict__ H, const double *__
     out.store(lam + base + c0);
 }
 
+// zeros into the cells of the lam_zero blocks
+template <typename Real>
+__global__ void __launch_bounds__(128)
+adj_unsparse_kernel(PoolView<Real> v, const unsigned char *__restrict__ lam_zero, Real *__restrict__ lam)
+{
+    const int blk = blockIdx.x;
+    if (!lam_zero[blk]) return;
+    Vec4<Real> z;
+    z.v[0] = z.v[1] = z.v[2] = z.v[3] = (Real)0;
+    z.store(lam + slot_of(v, blk) * kBS3 + threadIdx.x * 4);
+}
+
 template <typename Real>
 cudaError_t launch_adjoint_step(const PoolView<Real> &v, const Real *H, const unsigned short *meta, const double *ih2,
                                 const Real *phi, Real *lam, Real *mu, unsigned char *flags, Real rho, double dt,
                                 double Dw, double *grad_acc, cudaStream_t s)
 {
     if (v.nblocks <= 0) return cudaSuccess;
-    unsigned char *blk_dom = flags + (int64_t)v.nblocks * kBS3;  // the flag buffer's per-block tail
-    adj_mu_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, meta, ih2, phi, lam, mu, flags, blk_dom, rho, dt, 1. / Dw,
-                                                   grad_acc);
-    adj_lambda_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, ih2, phi, mu, flags, blk_dom, lam, rho, dt);
+    unsigned char *status = flags + (int64_t)v.nblocks * kBS3;  // the flag buffer's per-block tail
+    unsigned char *lam_zero = status + v.nblocks;
+    adj_mu_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, meta, ih2, phi, lam, lam_zero, mu, flags, status, rho, dt,
+                                                   1. / Dw, grad_acc);
+    adj_lambda_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, ih2, phi, mu, flags, status, lam, lam_zero, rho, dt);
+    return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_adjoint_unsparse(const PoolView<Real> &v, const unsigned char *flags, Real *lam, cudaStream_t s)
+{
+    if (v.nblocks <= 0) return cudaSuccess;
+    adj_unsparse_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, flags + (int64_t)v.nblocks * (kBS3 + 1), lam);
     return cudaGetLastError();
 }
 
@@ -1141,6 +1223,8 @@ cudaError_t upload_ghost_table()
     template cudaError_t launch_adjoint_step<Real>(const PoolView<Real> &, const Real *, const unsigned short *,  \
                                                    const double *, const Real *, Real *, Real *, unsigned char *, \
                                                    Real, double, double, double *, cudaStream_t);            \
+    template cudaError_t launch_adjoint_unsparse<Real>(const PoolView<Real> &, const unsigned char *, Real *,      \
+                                                       cudaStream_t);                                             \
     template cudaError_t launch_loss_grad<Real>(int, const Real *, const unsigned char *, const unsigned char *, \
                                                 double, double, double, Real *, cudaStream_t);               \
     template cudaError_t launch_gaussian_ic<Real>(int, const Real *, const Real *, const double *, double, Real *, \

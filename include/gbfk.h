@@ -266,7 +266,10 @@ int gbfk_batch_log_likelihood(gbfk_batch *b, const gbfk_likelihood_params *param
  * of the state at the horizon against the observations (gbfk_set_observations,
  * without ROI).  dt and the step count are held fixed; the piecewise-constant
  * switches of the step (domain test, no-flux doubling, clamp) are held fixed.
- * States are kept with binomial checkpointing in nsnapshots device buffers. */
+ * States are kept with binomial checkpointing in nsnapshots device buffers;
+ * these and seven work fields stay allocated in the context until
+ * gbfk_destroy, so that later calls on the same grid with at most as many
+ * checkpoints allocate nothing. */
 typedef struct {
     double Dw, Dg, rho, dt; /* rescaled Real coefficients and the time step */
     int nsteps;             /* steps to the horizon */

@@ -25,6 +25,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <map>
 #include <vector>
 
@@ -39,7 +40,7 @@ template <> struct precision_of<float> { static const int value = GBFK_F32; };
  * (MRAG/MRAGcore/MRAGBlockLab.h:256-279). */
 struct Topology {
     std::vector<gbfk_blockinfo> blocks;
-    std::map<int, int> slot_of; /* blockID -> slot */
+    std::vector<int> slot_of; /* blockID -> slot (-1: not a leaf) */
     std::vector<int64_t> row_ptr, src;
     std::vector<double> w0, w1, w2;
     gbfk_ghost_csr csr() const
@@ -59,6 +60,15 @@ template <typename BlockInfoT, typename BoundaryInfoT>
 Topology flatten(const std::vector<BlockInfoT> &vInfo, BoundaryInfoT &boundaryInfo)
 {
     Topology t;
+    int max_id = -1;
+    for (size_t i = 0; i < vInfo.size(); i++) max_id = std::max(max_id, vInfo[i].blockID);
+    t.slot_of.assign((size_t)(max_id + 1), -1);
+    t.blocks.reserve(vInfo.size());
+    t.row_ptr.reserve(vInfo.size() * GBFK_LAB_GHOSTS + 1);
+    t.src.reserve(vInfo.size() * GBFK_LAB_GHOSTS * 2);
+    t.w0.reserve(t.src.capacity());
+    t.w1.reserve(t.src.capacity());
+    t.w2.reserve(t.src.capacity());
     for (int i = 0; i < (int)vInfo.size(); i++) {
         gbfk_blockinfo b;
         b.slot = i;
@@ -88,7 +98,13 @@ Topology flatten(const std::vector<BlockInfoT> &vInfo, BoundaryInfoT &boundaryIn
                 const std::vector<MRAG::IndexWP> &row = ghosts[bb.boundary[icode].start + g];
                 for (size_t k = 0; k < row.size(); k++) {
                     const MRAG::PointIndex &p = pool[row[k].point_index];
-                    t.src.push_back((int64_t)t.slot_of[p.blockID] * GBFK_BLOCK_CELLS + p.index);
+                    const int slot = p.blockID >= 0 && p.blockID <= max_id ? t.slot_of[p.blockID] : -1;
+                    if (slot < 0) {
+                        fprintf(stderr, "gbfk_mrag: a ghost of block %d reads block %d, not a leaf\n",
+                                vInfo[i].blockID, p.blockID);
+                        abort();
+                    }
+                    t.src.push_back((int64_t)slot * GBFK_BLOCK_CELLS + p.index);
                     t.w0.push_back(bb.weightsPool[row[k].weights_index[0]]);
                     t.w1.push_back(bb.weightsPool[row[k].weights_index[1]]);
                     t.w2.push_back(bb.weightsPool[row[k].weights_index[2]]);
