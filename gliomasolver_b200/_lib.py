@@ -41,6 +41,7 @@ EXPORTS = (
     "gbfk_set_observations", "gbfk_uq_dump", "gbfk_log_likelihood",
     "gbfk_batch_create", "gbfk_batch_destroy", "gbfk_batch_last_error", "gbfk_batch_launch_count",
     "gbfk_batch_set_anatomy", "gbfk_batch_set_samples", "gbfk_batch_run", "gbfk_batch_samples_per_cta",
+    "gbfk_batch_tile_shape", "gbfk_batch_graph_count",
     "gbfk_batch_download", "gbfk_batch_set_observations", "gbfk_batch_log_likelihood",
     "gbfk_forward_adjoint",
     "gbfk_host_last_error", "gbfk_matrix_info", "gbfk_matrix_read", "gbfk_matrix_write", "gbfk_map_anatomy",
@@ -175,6 +176,8 @@ def load(path: Path | str | None = None):
         "gbfk_batch_set_samples": (I, [P, I, ctypes.POINTER(Sample)]),
         "gbfk_batch_run": (I, [P, I]),
         "gbfk_batch_samples_per_cta": (I, [P]),
+        "gbfk_batch_tile_shape": (I, [P, ctypes.POINTER(I * 3)]),
+        "gbfk_batch_graph_count": (I, [P]),
         "gbfk_batch_download": (I, [P, I, P]),
         "gbfk_batch_set_observations": (I, [P, P, P, P, P, I]),
         "gbfk_batch_log_likelihood": (I, [P, ctypes.POINTER(LikelihoodParams), I, P]),

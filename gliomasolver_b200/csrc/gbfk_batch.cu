@@ -72,6 +72,8 @@ struct gbfk_batch {
     CUtensorMap maps[2][3];
     bool maps_ready = false;
     int chosen_spc = 0;          // block kernel: samples per CTA; -1: the pipelined kernel
+    int chosen_shape = -1;       // pipelined kernel: launch shape code (-1: the default)
+    int graph_launches = 0;      // CUDA graphs the last run replayed
     bool ran = false;            // the samples hold their final states
     // observations of the likelihood step (n^3 grid) and its scratch
     unsigned char *d_t1c = nullptr, *d_flair = nullptr;
@@ -351,14 +353,15 @@ int batch_prepare(gbfk_batch *b)
 // One step of the batch with the chosen kernel: the pipelined step
 // (spc == -1) or the per-block kernel with spc samples per CTA.
 template <typename Real>
-cudaError_t batch_step(gbfk_batch *b, const BatchView<Real> &bv, int nactive, int step, int spc)
+cudaError_t batch_step(gbfk_batch *b, const BatchView<Real> &bv, int nactive, int step, int spc, int shape)
 {
     if (spc > 0) return launch_rd_batch_step<Real>(bv, nactive, step, spc, b->stream);
     const int par = step & 1;
     return launch_rd_batch_step_tma<Real>(
         b->bl, nactive, nactive * b->nblocks, b->log2_bpd, b->nblocks, (const Real *)b->phi_all[par],
         (Real *)b->phi_all[par ^ 1], (const Real *)b->H_all, (const Real *)b->pw_all, (const Real *)b->pg_all,
-        b->meta_all, (const Real *)b->d_rho, b->d_dt, b->ih2, step > 0, b->d_nan, b->d_err, b->maps[par], b->stream);
+        b->meta_all, (const Real *)b->d_rho, b->d_dt, b->ih2, step > 0, b->d_nan, b->d_err, b->maps[par], shape,
+        b->stream);
 }
 
 template <typename Real>
@@ -388,25 +391,34 @@ int batch_run(gbfk_batch *b, int spc)
         return nactive;
     };
     int step = 0;
-    // autotuner: the pipelined step (power-of-two grids) and the per-block
-    // kernel with 1, 2 or 4 samples per CTA, each timed on 3 real steps
-    // after 1 warm-up (every choice gives the same bits), the fastest kept
+    // autotuner: the pipelined step (power-of-two grids) in each of its
+    // launch shapes (consumer warps, heavy and empty ring slots) and the
+    // per-block kernel with 1, 2 or 4 samples per CTA, each timed on 3 real
+    // steps after 1 warm-up (every choice gives the same bits), the fastest
+    // kept
+    int shape = -1;
     if (spc == 0) {
-        std::vector<int> cands;
-        if (b->log2_bpd >= 0) cands.push_back(-1);
-        cands.push_back(1);
-        cands.push_back(2);
-        cands.push_back(4);
+        std::vector<std::pair<int, int>> cands;  // (samples per CTA, shape)
+        if (b->log2_bpd >= 0) {
+            int codes[16];
+            const int nc = tma_batch_shapes(codes, 16);
+            cands.push_back({-1, -1});
+            for (int i = 0; i < nc; i++) cands.push_back({-1, codes[i]});
+        }
+        cands.push_back({1, -1});
+        cands.push_back({2, -1});
+        cands.push_back({4, -1});
         float best = 1e30f;
-        int best_spc = cands[0];
+        std::pair<int, int> best_c = cands[0];
         cudaEvent_t e0, e1;
         BK(cudaEventCreate(&e0));
         BK(cudaEventCreate(&e1));
         for (size_t ci = 0; ci < cands.size() && step + 4 <= maxsteps; ci++) {
-            BK(batch_step<Real>(b, bv, active_at(step), step, cands[ci]));
+            const int cs = cands[ci].first, csh = cands[ci].second;
+            BK(batch_step<Real>(b, bv, active_at(step), step, cs, csh));
             step++;
             BK(cudaEventRecord(e0, b->stream));
-            for (int r = 0; r < 3; r++, step++) BK(batch_step<Real>(b, bv, active_at(step), step, cands[ci]));
+            for (int r = 0; r < 3; r++, step++) BK(batch_step<Real>(b, bv, active_at(step), step, cs, csh));
             BK(cudaEventRecord(e1, b->stream));
             BK(cudaEventSynchronize(e1));
             float ms = 0;
@@ -414,20 +426,59 @@ int batch_run(gbfk_batch *b, int spc)
             b->launches += 4;
             if (ms < best) {
                 best = ms;
-                best_spc = cands[ci];
+                best_c = cands[ci];
             }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        spc = best_spc;
+        spc = best_c.first;
+        shape = best_c.second;
     }
     b->chosen_spc = spc;
+    b->chosen_shape = spc == -1 ? shape : 0;
     b->ran = false;
-    for (; step < maxsteps; step++) {
-        BK(batch_step<Real>(b, bv, active_at(step), step, spc));
+    // the remaining steps: the first one directly, the rest captured as CUDA
+    // graphs of up to kGraphSteps launches each and replayed on the batch's
+    // stream (a stream that cannot be captured, such as the legacy default
+    // stream, runs them directly)
+    if (step < maxsteps) {
+        BK(batch_step<Real>(b, bv, active_at(step), step, spc, shape));
         b->launches++;
+        step++;
     }
-    BK(cudaStreamSynchronize(b->stream));
+    constexpr int kGraphSteps = 512;
+    std::vector<cudaGraphExec_t> execs;
+    bool graphs = true;
+    while (step < maxsteps) {
+        const int end = std::min(maxsteps, step + kGraphSteps);
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        if (graphs && cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            graphs = false;
+        }
+        cudaError_t le = cudaSuccess;
+        for (int k = step; k < end && le == cudaSuccess; k++) le = batch_step<Real>(b, bv, active_at(k), k, spc, shape);
+        if (graphs) {
+            const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+            if (le == cudaSuccess) le = ce;
+            if (le == cudaSuccess) le = cudaGraphInstantiate(&ge, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (le == cudaSuccess) le = cudaGraphLaunch(ge, b->stream);
+            if (ge) execs.push_back(ge);
+        }
+        if (le != cudaSuccess) {
+            cudaStreamSynchronize(b->stream);
+            for (cudaGraphExec_t x : execs) cudaGraphExecDestroy(x);
+            return bfail(b, GBFK_E_CUDA, "batch_run: steps %d..%d: %s", step, end, cudaGetErrorString(le));
+        }
+        b->launches += end - step;
+        step = end;
+    }
+    b->graph_launches = (int)execs.size();
+    const cudaError_t se = cudaStreamSynchronize(b->stream);
+    for (cudaGraphExec_t x : execs) cudaGraphExecDestroy(x);
+    BK(se);
     unsigned err = 0;
     BK(cudaMemcpy(&err, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (err) return bfail(b, GBFK_E_TIMEOUT, "batch_run: a wait of the pipelined step timed out (1 s)");
@@ -640,6 +691,22 @@ int gbfk_batch_run(gbfk_batch *b, int samples_per_cta)
 }
 
 int gbfk_batch_samples_per_cta(const gbfk_batch *b) { return b ? b->chosen_spc : 0; }
+
+int gbfk_batch_tile_shape(const gbfk_batch *b, int shape[3])
+{
+    if (!b || !shape) return GBFK_E_INVALID;
+    if (b->chosen_spc != -1) {
+        shape[0] = shape[1] = shape[2] = 0;
+        return GBFK_OK;
+    }
+    const int code = tma_shape_effective(b->chosen_shape, (int)b->rsize);
+    shape[0] = code / 1000;
+    shape[1] = (code / 100) % 10;
+    shape[2] = code % 100;
+    return GBFK_OK;
+}
+
+int gbfk_batch_graph_count(const gbfk_batch *b) { return b ? b->graph_launches : 0; }
 
 int gbfk_batch_download(gbfk_batch *b, int sample, void *dense_out)
 {

@@ -125,7 +125,12 @@ cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int tota
                                      int nblocks, const Real *phi_in, Real *phi_out, const Real *H, const Real *pw,
                                      const Real *pg, const unsigned short *meta, const Real *rho, const double *dt,
                                      double ih2, bool clamped, unsigned *nan_flags, unsigned *err_flag,
-                                     const CUtensorMap *maps, cudaStream_t s);
+                                     const CUtensorMap *maps, int shape, cudaStream_t s);
+// launch shapes of the pipelined step a batch may use: codes
+// consumer warps * 1000 + heavy slots * 100 + empty slots (shape -1 above:
+// the default, or GBFK_TMA_SHAPE); returns how many were written
+int tma_batch_shapes(int *codes, int max_codes);
+int tma_shape_effective(int code, int real_bytes);
 
 template <typename Real>
 cudaError_t launch_fill_ghosts(const int *rows, int64_t nrows, const int64_t *row_ptr, const int *src,

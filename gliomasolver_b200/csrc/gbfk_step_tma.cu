@@ -854,18 +854,26 @@ int tma_shape_code()
     X(4, 2, 8)             \
     X(16, 2, 16)
 
+// the shape of a code (consumer warps * 1000 + heavy slots * 100 + empty
+// slots), or the default for any code not in the list
 template <typename Real, typename F>
-cudaError_t with_shape(F &&f)
+cudaError_t with_shape_code(int code, F &&f)
 {
 #define GBFK_TMA_CASE(W, HV, EM) \
     case (W * 10 + HV) * 100 + EM: return f(Shape<Real, W, HV, EM>());
-    switch (tma_shape_code()) {
+    switch (code) {
         GBFK_TMA_SHAPES(GBFK_TMA_CASE)
     default:
         if constexpr (sizeof(Real) == 4) return f(Shape<Real, 8, 2, 8>());
         else return f(Shape<Real, 8, 1, 8>());
     }
 #undef GBFK_TMA_CASE
+}
+
+template <typename Real, typename F>
+cudaError_t with_shape(F &&f)
+{
+    return with_shape_code<Real>(tma_shape_code(), f);
 }
 
 }  // namespace
@@ -938,7 +946,7 @@ cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int tota
                                      int nblocks, const Real *phi_in, Real *phi_out, const Real *H, const Real *pw,
                                      const Real *pg, const unsigned short *meta, const Real *rho, const double *dt,
                                      double ih2, bool clamped, unsigned *nan_flags, unsigned *err_flag,
-                                     const CUtensorMap *maps, cudaStream_t s)
+                                     const CUtensorMap *maps, int shape, cudaStream_t s)
 {
     if (nactive <= 0 || total_items <= 0) return cudaSuccess;
     if (log2_bpd < 0) return cudaErrorInvalidValue;
@@ -960,9 +968,37 @@ cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int tota
     src.L = log2_bpd;
     src.nblocks = nblocks;
     src.nan_flags = nan_flags;
-    return with_shape<Real>([&](auto sh) {
+    return with_shape_code<Real>(shape < 0 ? tma_shape_code() : shape, [&](auto sh) {
         return decltype(sh)::template launch<BatchSource<Real>>(src, total_items, ih2, clamped, err_flag, maps, s);
     });
+}
+
+// the shape code a launch with `code` uses (-1: GBFK_TMA_SHAPE, else the
+// default of the Real type; a code outside the list: the default)
+int tma_shape_effective(int code, int real_bytes)
+{
+    static const int all[] = {
+#define GBFK_TMA_CODE(W, HV, EM) (W * 10 + HV) * 100 + EM,
+        GBFK_TMA_SHAPES(GBFK_TMA_CODE)
+#undef GBFK_TMA_CODE
+    };
+    if (code < 0) code = tma_shape_code();
+    for (int c : all)
+        if (c == code) return code;
+    return real_bytes == 4 ? 8208 : 8108;
+}
+
+// the launch shapes a batch autotuner may try (codes as for with_shape_code)
+int tma_batch_shapes(int *codes, int max_codes)
+{
+    static const int all[] = {
+#define GBFK_TMA_CODE(W, HV, EM) (W * 10 + HV) * 100 + EM,
+        GBFK_TMA_SHAPES(GBFK_TMA_CODE)
+#undef GBFK_TMA_CODE
+    };
+    const int n = (int)(sizeof(all) / sizeof(all[0]));
+    for (int i = 0; i < n && i < max_codes; i++) codes[i] = all[i];
+    return n < max_codes ? n : max_codes;
 }
 
 template bool tma_step_eligible<float>(const PoolView<float> &);
@@ -977,11 +1013,12 @@ template cudaError_t launch_rd_step_tma<double>(const PoolView<double> &, const 
 template cudaError_t launch_rd_batch_step_tma<float>(const BatchLists &, int, int, int, int, const float *, float *,
                                                      const float *, const float *, const float *,
                                                      const unsigned short *, const float *, const double *, double,
-                                                     bool, unsigned *, unsigned *, const CUtensorMap *, cudaStream_t);
+                                                     bool, unsigned *, unsigned *, const CUtensorMap *, int,
+                                                     cudaStream_t);
 template cudaError_t launch_rd_batch_step_tma<double>(const BatchLists &, int, int, int, int, const double *,
                                                       double *, const double *, const double *, const double *,
                                                       const unsigned short *, const double *, const double *, double,
-                                                      bool, unsigned *, unsigned *, const CUtensorMap *,
+                                                      bool, unsigned *, unsigned *, const CUtensorMap *, int,
                                                       cudaStream_t);
 
 }  // namespace gbfk

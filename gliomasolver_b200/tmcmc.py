@@ -114,6 +114,19 @@ class Batch:
     def samples_per_cta(self) -> int:
         return int(self.lib.gbfk_batch_samples_per_cta(self.b))
 
+    @property
+    def tile_shape(self) -> tuple:
+        """(consumer warps, heavy slots, empty slots) of the pipelined step the
+        last run used; (0, 0, 0) for the per-block kernel."""
+        sh = (ctypes.c_int * 3)()
+        self._check(self.lib.gbfk_batch_tile_shape(self.b, ctypes.byref(sh)))
+        return tuple(sh)
+
+    @property
+    def graph_count(self) -> int:
+        """CUDA graphs the last run replayed."""
+        return int(self.lib.gbfk_batch_graph_count(self.b))
+
     def set_anatomy(self, index: int, p_w: np.ndarray, p_g: np.ndarray):
         a = np.ascontiguousarray(p_w, dtype=self.dtype)
         g = np.ascontiguousarray(p_g, dtype=self.dtype)

@@ -217,6 +217,17 @@ int gbfk_batch_set_samples(gbfk_batch *b, int nsamples, const gbfk_sample *sampl
 int gbfk_batch_run(gbfk_batch *b, int samples_per_cta);
 /* The samples_per_cta choice the last run used (-1: the pipelined step). */
 int gbfk_batch_samples_per_cta(const gbfk_batch *b);
+/* The launch shape of the pipelined step the last run used: consumer warps
+ * per CTA, heavy-block ring slots, empty-block ring slots (all 0 when it
+ * used the per-block kernel).  With samples_per_cta 0 the autotuner times
+ * every compiled shape; otherwise the shape is the default (or the
+ * GBFK_TMA_SHAPE="warps,heavy,empty" environment variable). */
+int gbfk_batch_tile_shape(const gbfk_batch *b, int shape[3]);
+/* gbfk_batch_run replays its steps after the autotuner and the first step as
+ * CUDA graphs of up to 512 launches captured on the batch's stream; this is
+ * how many the last run replayed (0 when the stream could not be captured,
+ * e.g. the legacy default stream). */
+int gbfk_batch_graph_count(const gbfk_batch *b);
 /* phi of one sample after the run, dense n^3 Real. */
 int gbfk_batch_download(gbfk_batch *b, int sample, void *dense_out);
 

@@ -58,7 +58,12 @@ def test_batch_equals_sequential_solves(gbfk_lib, prec):
             b.run(spc)
             results[spc] = [b.download(i) for i in range(10)]
             if spc == 0:
+                # the autotuner ran every candidate (each launch shape of the
+                # pipelined step, 1/2/4 samples per CTA) on real steps
                 assert b.samples_per_cta in (-1, 1, 2, 4)
+            assert (b.tile_shape == (0, 0, 0)) == (b.samples_per_cta != -1)
+            if max(s.nsteps for s in scheds) > 60:
+                assert b.graph_count >= 1   # the steps after the autotuner replay as CUDA graphs
 
     for i in range(10):
         pw, pg = anat[which[i]]
