@@ -926,6 +926,45 @@ int gbfk_rd_rhs(gbfk_ctx *ctx, double Dw, double Dg, double rho, void *host)
                                       : rd_rhs_impl<float>(ctx, Dw, Dg, rho, host);
 }
 
+}  // extern "C"
+
+template <typename Real>
+static int cfl_impl(gbfk_ctx *ctx, double Dw, double Dg, double *out)
+{
+    const int nparts = 148 * 4;
+    if (!ctx->d_partial) CK(cudaMalloc(&ctx->d_partial, (size_t)148 * 4 * 7 * sizeof(double)));
+    const Real dw = (Real)Dw, dg = (Real)Dg;
+    CK(launch_cfl<Real>(view<Real>(ctx), dw, dg, ctx->d_partial, nparts, ctx->stream));
+    ctx->launches++;
+    std::vector<double> part(2 * (size_t)nparts);
+    CK(cudaMemcpyAsync(part.data(), ctx->d_partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double dmax = 0, hmin = INFINITY;
+    for (int i = 0; i < nparts; i++) {
+        dmax = std::fmax(dmax, part[2 * i]);
+        hmin = std::fmin(hmin, part[2 * i + 1]);
+    }
+    // Glioma_ReactionDiffusion.cpp:306-307 in Real, with h the finest leaf's
+    const Real h = (Real)hmin;
+    const Real mx = dw >= dg ? dw : dg;
+    out[0] = (double)(Real)(0.99 * (double)h * (double)h / (2. * 3 * (double)mx));
+    out[1] = hmin;
+    out[2] = dmax;
+    return GBFK_OK;
+}
+
+extern "C" {
+
+int gbfk_cfl(gbfk_ctx *ctx, double Dw, double Dg, double out[3])
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!ctx->have_topology) return fail(ctx, GBFK_E_STATE, "cfl: no topology");
+    if (!out) return fail(ctx, GBFK_E_INVALID, "cfl: null output");
+    CK(cudaSetDevice(ctx->device));
+    return ctx->precision == GBFK_F64 ? cfl_impl<double>(ctx, Dw, Dg, out) : cfl_impl<float>(ctx, Dw, Dg, out);
+}
+
 int gbfk_fwt_details(gbfk_ctx *ctx, double *out)
 {
     if (!ctx) return GBFK_E_INVALID;

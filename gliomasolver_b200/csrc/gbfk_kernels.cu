@@ -1177,6 +1177,57 @@ __global__ void dense_scatter_kernel(const Real *__restrict__ src, Real *__restr
     }
 }
 
+// CFL data of the current leaves: the largest local diffusion coefficient
+// df_loc = p_w * Dw + p_g * Dg of any cell (formed in Real as
+// ReactionDiffusionOperator.h:105 forms it) and the smallest block spacing
+// h, reduced by warp shuffles and then across the CTA's warps;
+// partial[2c] = max df_loc, partial[2c + 1] = min h of CTA c.  A NaN
+// coefficient is skipped (fmax/fmin), like the reference's max, which keeps
+// the first argument when a comparison is false.
+template <typename Real>
+__global__ void __launch_bounds__(256)
+cfl_kernel(PoolView<Real> v, Real Dw, Real Dg, double *__restrict__ partial)
+{
+    __shared__ double sm[2][8];
+    double dmax = 0, hmin = INFINITY;
+    const int64_t ncells = (int64_t)v.nblocks * kBS3;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncells;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int blk = (int)(i >> 9), c = (int)(i & 511);
+        const int64_t g = slot_of(v, blk) * kBS3 + c;
+        const Real df = radd(rmul(v.pw[g], Dw), rmul(v.pg[g], Dg));
+        dmax = fmax(dmax, (double)df);
+        if (c == 0) hmin = fmin(hmin, (double)v.hblk[blk]);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        dmax = fmax(dmax, __shfl_down_sync(0xffffffffu, dmax, off));
+        hmin = fmin(hmin, __shfl_down_sync(0xffffffffu, hmin, off));
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        sm[0][w] = dmax;
+        sm[1][w] = hmin;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++) {
+            dmax = fmax(dmax, sm[0][k]);
+            hmin = fmin(hmin, sm[1][k]);
+        }
+        partial[2 * blockIdx.x] = dmax;
+        partial[2 * blockIdx.x + 1] = hmin;
+    }
+}
+
+template <typename Real>
+cudaError_t launch_cfl(const PoolView<Real> &v, Real Dw, Real Dg, double *partial, int nparts, cudaStream_t s)
+{
+    if (v.nblocks <= 0 || nparts <= 0) return cudaErrorInvalidValue;
+    cfl_kernel<Real><<<nparts, 256, 0, s>>>(v, Dw, Dg, partial);
+    return cudaGetLastError();
+}
+
 template <typename Real>
 cudaError_t launch_dense_scatter(const Real *src, Real *dst, int n, bool to_pool, cudaStream_t s)
 {
@@ -1238,7 +1289,8 @@ cudaError_t upload_ghost_table()
                                             Real *, Real *, cudaStream_t);                                    \
     template cudaError_t launch_collapse<Real>(int, const int *, const int *, Real *, Real *, Real *,        \
                                                cudaStream_t);                                                 \
-    template cudaError_t launch_dense_scatter<Real>(const Real *, Real *, int, bool, cudaStream_t);
+    template cudaError_t launch_dense_scatter<Real>(const Real *, Real *, int, bool, cudaStream_t); \
+    template cudaError_t launch_cfl<Real>(const PoolView<Real> &, Real, Real, double *, int, cudaStream_t);
 
 GBFK_INSTANTIATE(float)
 GBFK_INSTANTIATE(double)

@@ -189,5 +189,9 @@ cudaError_t launch_x0_grad(int bpd, const Real *c0, const Real *lam0, const doub
 
 template <typename Real>
 cudaError_t launch_dense_scatter(const Real *dense, Real *pool, int n, bool to_pool, cudaStream_t s);
+// per-CTA partials of the largest p_w * Dw + p_g * Dg and the smallest block
+// spacing (partial: 2 * nparts doubles)
+template <typename Real>
+cudaError_t launch_cfl(const PoolView<Real> &v, Real Dw, Real Dg, double *partial, int nparts, cudaStream_t s);
 
 }  // namespace gbfk

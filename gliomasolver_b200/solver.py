@@ -160,6 +160,13 @@ class BlockPool:
         self._check(self.lib.gbfk_rd_rhs(self.ctx, float(Dw), float(Dg), float(rho), _ptr(out)))
         return out
 
+    def cfl(self, Dw, Dg) -> dict:
+        """The reference's CFL step at the finest leaf spacing, the smallest
+        spacing and the largest local coefficient p_w Dw + p_g Dg (gbfk_cfl)."""
+        out = np.empty(3, dtype=np.float64)
+        self._check(self.lib.gbfk_cfl(self.ctx, float(Dw), float(Dg), _ptr(out)))
+        return {"dt": float(out[0]), "h_min": float(out[1]), "max_diffusion": float(out[2])}
+
     # -- adaptivity -------------------------------------------------------
     def fwt_details(self) -> np.ndarray:
         out = np.empty(self.num_blocks, dtype=np.float64)

@@ -154,6 +154,15 @@ int gbfk_step_kernel(const gbfk_ctx *ctx);
 /* The operator alone: writes dphidt (Real, pool order, nblocks*512 cells) to
  * host memory; phi is unchanged.  (ReactionDiffusionOperator.h:47-138.) */
 int gbfk_rd_rhs(gbfk_ctx *ctx, double Dw, double Dg, double rho, void *host_dphidt);
+/* CFL time step of the current leaves: the reference's
+ *   dt = 0.99 * h*h / (2 * 3 * max(Dw, Dg))   (Glioma_ReactionDiffusion.cpp:306-307)
+ * in Real, with h the smallest block spacing of the leaves (the reference's
+ * driver takes h of the initial grid, which exceeds the stable step once
+ * blocks are refined).  A device reduction (warp shuffles, then per CTA)
+ * also finds the largest local coefficient p_w * Dw + p_g * Dg of any cell.
+ * out[0] = dt, out[1] = the smallest h, out[2] = the largest coefficient.
+ * Dw, Dg: the rescaled coefficients, as for gbfk_rd_step.  Synchronises. */
+int gbfk_cfl(gbfk_ctx *ctx, double Dw, double Dg, double out[3]);
 
 /* --- adaptivity ------------------------------------------------------- */
 /* Per block of the topology (in upload order) the max |detail| of the

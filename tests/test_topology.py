@@ -116,3 +116,38 @@ def test_split_and_collapse_match_oracle(gbfk_lib, prec):
         assert np.array_equal(back[f], want_parent)
         # injection of an interpolated block returns the parent's own values
         assert np.array_equal(back[f], src.reshape(-1, 512)[5])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_cfl_step_on_the_device(gbfk_lib, prec):
+    """gbfk_cfl: the reference's dt formula at the finest leaf spacing (the
+    schedule's dt on a uniform grid, bit for bit) and the largest local
+    diffusion coefficient, against numpy in the same Real."""
+    from gliomasolver_b200 import BlockPool
+
+    R = np.float64 if prec == "f64" else np.float32
+    n, bpd = 32, 4
+    rng = np.random.default_rng(3)
+    slots = rng.permutation(bpd ** 3 + 6)[: bpd ** 3]
+    pw, pg, c0, (pwp, pgp, php) = _pool_inputs(n, 3, R, slots)
+    s = make_schedule(0.3, 0.1, 150.0, 25.6, bpd, prec)
+    want_d = (R(pw) * R(s.Dw) + R(pg) * R(s.Dg)).astype(R).max()
+    blocks, csr = uniform_topology(bpd, slots)
+    with BlockPool(bpd ** 3 + 6, prec) as pool:
+        pool.set_topology(blocks, csr)
+        pool.upload("p_w", pwp)
+        pool.upload("p_g", pgp)
+        c = pool.cfl(s.Dw, s.Dg)
+        assert c["dt"] == s.dt and c["h_min"] == float(R(1.0 / n))
+        assert c["max_diffusion"] == float(want_d)
+        # a refined block: the step follows the finest spacing
+        blocks[5] = (blocks[5][0], 1, blocks[5][2], 0.5 / n)
+        pool.set_topology(blocks, csr)
+        pool.upload("p_w", pwp)
+        pool.upload("p_g", pgp)
+        c = pool.cfl(s.Dw, s.Dg)
+        h = R(0.5 / n)
+        mx = max(R(s.Dw), R(s.Dg))
+        assert c["h_min"] == float(h)
+        assert c["dt"] == float(R(0.99 * np.float64(h) * np.float64(h) / (6.0 * np.float64(mx))))
