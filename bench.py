@@ -320,15 +320,18 @@ def adjoint_sample(stream, local, bpd=16, nsnap=64):
     }
 
 
-def adjoint_batch(stream, local, nsamples=16, bpd=32, nsnap=64, seed=5):
+def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9):
     """Config 5: forward + discrete adjoint for 16 samples at 256^3, FP32 state,
     each sample with its own seeded anatomy (brain scale U[0.8, 1.2]) and
     parameters sampled as in config 3 (Dw log-U[0.02,0.3], rho
     log-U[0.002,0.2], T U[30,300] d, x0 in white matter).  Observations: the
     sample's own forward run thresholded at 0.7 / 0.25 with 2% label noise;
     gradients at Dw * 1.1, rho * 0.9.  The samples run one after the other
-    (one gbfk_forward_adjoint call each; 64 checkpoint buffers of 67 MB).
-    Sample 0 is repeated in FP64 for the FP32-vs-FP64 gradient error."""
+    (one gbfk_forward_adjoint call each, on one context whose buffers are
+    allocated before the timed calls).  The checkpoint budget is admitted by
+    a 160 GB HBM cap (less what the device has free beside the other
+    buffers): min(steps, cap / 67 MB) checkpoints per sample.  Sample 0 is
+    repeated in FP64 for the FP32-vs-FP64 gradient error."""
     import torch
 
     from gliomasolver_b200 import BlockPool
@@ -338,54 +341,93 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, nsnap=64, seed=5):
     n = 8 * bpd
     rng = np.random.default_rng(seed)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-    t_total, steps_total, recs = 0.0, 0, []
+    t_total, steps_total, fwd_total, recs = 0.0, 0, 0, []
     peak, _ = measured_peak()
 
-    def one(prec, p_w, p_g, st, masks=None):
+    def open_pool(prec):
+        R = np.float32 if prec == "f32" else np.float64
+        pool = BlockPool(bpd ** 3, prec, device=local, stream=stream.cuda_stream)
+        pool.set_uniform(bpd)
+        z = np.zeros((n, n, n), dtype=R)
+        pool.upload_dense("p_w", z)
+        pool.upload_dense("p_g", z)
+        pool.upload_dense("phi", z)
+        pool.set_observations(z.astype(float), z.astype(float))
+        torch.cuda.synchronize()
+        free, _total = torch.cuda.mem_get_info(local)
+        fbytes = n ** 3 * np.dtype(R).itemsize
+        cap = min(hbm_cap, free - 8 * fbytes - 4e9)
+        cap_snap = max(1, int(cap // fbytes))
+        # allocate the checkpoints (and the work fields) once, outside the timed
+        # calls; halve the budget if the device refuses it
+        from gliomasolver_b200 import GbfkError
+        from gliomasolver_b200._lib import STATUS_CODES
+        while True:
+            try:
+                pool.forward_adjoint(1e-4, 1e-5, 0.01, 1e-3, 2, nsnapshots=cap_snap)
+                break
+            except GbfkError as e:
+                if e.code != STATUS_CODES["GBFK_E_OOM"] or cap_snap <= 64:
+                    raise
+                cap_snap //= 2
+        torch.cuda.synchronize()
+        return pool, cap_snap
+
+    def one(pool, cap_snap, prec, p_w, p_g, st, masks=None):
         R = np.float32 if prec == "f32" else np.float64
         s = make_schedule(st.Dw_cm2_day, st.rho_day, st.tend_day, L_CM, bpd, prec)
-        with BlockPool(bpd ** 3, prec, device=local, stream=stream.cuda_stream) as pool:
-            pool.set_uniform(bpd)
-            pool.upload_dense("p_w", p_w.astype(R))
-            pool.upload_dense("p_g", p_g.astype(R))
-            if masks is None:
-                pool.upload_dense("phi", tumor_ic(n, st.x0, p_w, p_g).astype(R))
-                pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, s.nsteps)
-                u = pool.download_dense("phi").astype(np.float64)
-                masks = [(u > 0.7).astype(float), (u > 0.25).astype(float)]
-                for m in masks:
-                    flip = rng.random(m.shape) < 0.02
-                    m[flip] = 1 - m[flip]
-            pool.set_observations(*masks)
-            Dw = float(R(R(st.Dw_cm2_day * 1.1) / R(L_CM * L_CM)))
-            Dg = float(R(0.1 * Dw))
-            torch.cuda.synchronize()
-            e0, e1 = ev(), ev()
-            e0.record(stream)
-            res = pool.forward_adjoint(Dw, Dg, st.rho_day * 0.9, s.dt, s.nsteps, x0=st.x0, sigma=2.0 / n,
-                                       nsnapshots=nsnap)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            return res, e0.elapsed_time(e1) / 1e3, s.nsteps, masks
+        pool.upload_dense("p_w", p_w.astype(R))
+        pool.upload_dense("p_g", p_g.astype(R))
+        if masks is None:
+            pool.upload_dense("phi", tumor_ic(n, st.x0, p_w, p_g).astype(R))
+            pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, s.nsteps)
+            u = pool.download_dense("phi").astype(np.float64)
+            masks = [(u > 0.7).astype(float), (u > 0.25).astype(float)]
+            for m in masks:
+                flip = rng.random(m.shape) < 0.02
+                m[flip] = 1 - m[flip]
+        pool.set_observations(*masks)
+        Dw = float(R(R(st.Dw_cm2_day * 1.1) / R(L_CM * L_CM)))
+        Dg = float(R(0.1 * Dw))
+        nsnap = min(s.nsteps, cap_snap)
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        res = pool.forward_adjoint(Dw, Dg, st.rho_day * 0.9, s.dt, s.nsteps, x0=st.x0, sigma=2.0 / n,
+                                   nsnapshots=max(1, nsnap))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return res, e0.elapsed_time(e1) / 1e3, s.nsteps, masks, nsnap
 
     first = None
-    for i in range(nsamples):
-        p_w, p_g, _ = make_anatomy(n, seed + 100 + i, scale=float(rng.uniform(0.8, 1.2)))
-        st = sample_stage(1, p_w, seed=seed + 200 + i)[0]
-        res, t, k, masks = one("f32", p_w, p_g, st)
-        t_total += t
-        steps_total += k
-        recs.append({"steps": k, "seconds": t, "loss": res["loss"], "dDw": res["dDw"], "drho": res["drho"]})
-        if first is None:
-            first = (p_w, p_g, st, res, masks)
+    pool, cap32 = open_pool("f32")
+    try:
+        for i in range(nsamples):
+            p_w, p_g, _ = make_anatomy(n, seed + 100 + i, scale=float(rng.uniform(0.8, 1.2)))
+            st = sample_stage(1, p_w, seed=seed + 200 + i)[0]
+            res, t, k, masks, nsnap = one(pool, cap32, "f32", p_w, p_g, st)
+            t_total += t
+            steps_total += k
+            fwd_total += res["forward_steps"]
+            recs.append({"steps": k, "checkpoints": nsnap, "forward_steps_run": res["forward_steps"], "seconds": t,
+                         "loss": res["loss"], "dDw": res["dDw"], "drho": res["drho"]})
+            if first is None:
+                first = (p_w, p_g, st, res, masks)
+    finally:
+        pool.close()
     p_w, p_g, st, r32, masks = first
-    r64 = one("f64", p_w, p_g, st, masks)[0]
+    pool, cap64 = open_pool("f64")
+    try:
+        r64 = one(pool, cap64, "f64", p_w, p_g, st, masks)[0]
+    finally:
+        pool.close()
     rel = {k: abs(r32[k] - r64[k]) / max(abs(r64[k]), 1e-300) for k in ("loss", "dDw", "drho")}
     alg = 9 * 4 * (n ** 3) * steps_total  # (4 forward + 5 adjoint) words per cell and step, FP32
     return {
         "workload": f"{nsamples} samples, forward + discrete adjoint at {n}^3, FP32 state, own anatomy each "
-                    f"(scale U[0.8,1.2]), config-3 parameter sampling, {nsnap} checkpoint buffers, one sample per call",
-        "samples": nsamples, "steps_total": steps_total, "seconds": t_total,
+                    f"(scale U[0.8,1.2]), config-3 parameter sampling, checkpoints admitted by a "
+                    f"{hbm_cap / 1e9:.0f} GB HBM cap (up to {cap32} of 67 MB), one sample per call",
+        "samples": nsamples, "steps_total": steps_total, "forward_steps_run": fwd_total, "seconds": t_total,
         "gradient_samples_per_s": nsamples / t_total,
         "roofline": {"achieved": alg / t_total / 1e9, "peak": peak, "unit": "GB/s", "frac": alg / t_total / 1e9 / peak,
                      "algorithmic_bytes": "9 words (forward 4 + adjoint 5) x cells x steps; recomputation not counted"},

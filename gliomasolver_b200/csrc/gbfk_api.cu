@@ -12,6 +12,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace gbfk {
@@ -1130,18 +1131,19 @@ struct Adjoint {
         CUtensorMap m[3];
     };
     std::vector<Maps> maps;
+    std::unordered_map<const void *, size_t> map_index;
 
     cudaError_t add_maps(const void *buf)
     {
         maps.emplace_back();
         maps.back().buf = buf;
+        map_index[buf] = maps.size() - 1;
         return make_pool_tensor_maps(const_cast<void *>(buf), ctx->max_blocks, (int)sizeof(Real), maps.back().m);
     }
     const CUtensorMap *maps_of(const void *buf) const
     {
-        for (const Maps &m : maps)
-            if (m.buf == buf) return m.m;
-        return nullptr;
+        const auto it = map_index.find(buf);
+        return it == map_index.end() ? nullptr : maps[it->second].m;
     }
 
     void step(const Real *in, Real *out)
@@ -1181,11 +1183,12 @@ struct Adjoint {
         asteps++;
         ctx->launches += 2;
     }
-    static double beta(int c, int r)  // C(c + r, c), capped
+    static double beta(int c, int r)  // C(c + r, c) = C(c + r, r), capped
     {
+        const int k = std::min(c, r), m = std::max(c, r);
         double b = 1;
-        for (int i = 1; i <= c; i++) {
-            b = b * (r + i) / i;
+        for (int i = 1; i <= k; i++) {
+            b = b * (m + i) / i;
             if (b > 1e18) return 1e18;
         }
         return b;
@@ -1250,9 +1253,10 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     cudaError_t e = cudaSuccess;
     if (ctx->adj_fbytes != A.fbytes || ctx->adj_nblocks != nb || ctx->adj_nsnap < p->nsnapshots) {
         release();
-        ctx->adj_mem.assign(10 + p->nsnapshots, nullptr);
-        for (size_t i = 0; i < ctx->adj_mem.size() && e == cudaSuccess; i++)
-            e = cudaMalloc(&ctx->adj_mem[i], i < 10 ? sizes[i] : A.fbytes);
+        // the work fields one by one, the checkpoints in one allocation
+        ctx->adj_mem.assign(11, nullptr);
+        for (size_t i = 0; i < 11 && e == cudaSuccess; i++)
+            e = cudaMalloc(&ctx->adj_mem[i], i < 10 ? sizes[i] : A.fbytes * (size_t)p->nsnapshots);
         if (e != cudaSuccess) {
             cudaGetLastError();
             release();
@@ -1273,7 +1277,7 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     A.grad_acc = (double *)ctx->adj_mem[8];
     double *xpart = (double *)ctx->adj_mem[9];
     A.slots.assign(p->nsnapshots, nullptr);
-    for (int i = 0; i < p->nsnapshots; i++) A.slots[i] = (Real *)ctx->adj_mem[10 + i];
+    for (int i = 0; i < p->nsnapshots; i++) A.slots[i] = (Real *)((char *)ctx->adj_mem[10] + A.fbytes * (size_t)i);
     e = cudaMemsetAsync(A.grad_acc, 0, (size_t)nb * kGradSlots * sizeof(double), ctx->stream);
     // forward steps on the pipelined kernel where it applies (bit-identical)
     A.X0 = X0;
