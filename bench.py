@@ -556,6 +556,7 @@ def gpu_arm(args):
     adj5 = None
     if not args.no_batch:
         batch = batched_stage(args, stream, local)
+    if not args.no_batch or args.adjoint_sample:
         adj = adjoint_sample(stream, local)
     if args.adjoint_batch:
         adj5 = adjoint_batch(stream, local)
@@ -594,6 +595,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched TMCMC-stage measurement")
+    ap.add_argument("--adjoint-sample", action="store_true",
+                    help="run the config-4 gradient sample even with --no-batch")
     ap.add_argument("--adjoint-batch", action="store_true",
                     help="also run config 5 (16 gradient samples at 256^3, a few minutes)")
     ap.add_argument("--step-kernel", default="auto", choices=["auto", "block", "pipelined"],
