@@ -514,6 +514,31 @@ cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigne
 // dense kernels could produce -0: a sign of zero that no later product or
 // sum turns into a different number).
 
+// Programmatic dependent launch (kernels launched by launch_pdl): wait until
+// the previous grid on the stream has completed and its writes are visible,
+// then let the next grid be scheduled as this one's CTAs finish.  Without
+// the launch attribute both instructions return at once.
+__device__ __forceinline__ void pdl_wait_then_release()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename K, typename... Args>
+cudaError_t launch_pdl(K kernel, int grid, int threads, cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 __device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
 {
     const double t = s + x;
@@ -544,6 +569,7 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
 {
     __shared__ __align__(16) Real ph[kStepLab];
     __shared__ double red[4][4];
+    pdl_wait_then_release();
     const int blk = blockIdx.x, t = threadIdx.x;
     if (lam_zero[blk]) {
         // lambda' = 0 in the block: mu = 0 whatever the step does, no gradient terms
@@ -730,6 +756,7 @@ adj_lambda_kernel(PoolView<Real> v, const Real *__restrict__ H, const double *__
     __shared__ __align__(16) Real smu[kStepLab];
     __shared__ unsigned char sfl[kStepLab];
     __shared__ unsigned char sst[8];
+    pdl_wait_then_release();
     const int blk = blockIdx.x, t = threadIdx.x;
     // threads 0..5: the face neighbours, thread 6: the block itself
     if (t < 7) sst[t] = status[t == 6 ? blk : face_neighbour(v, blk, t)];
@@ -834,10 +861,11 @@ cudaError_t launch_adjoint_step(const PoolView<Real> &v, const Real *H, const un
     if (v.nblocks <= 0) return cudaSuccess;
     unsigned char *status = flags + (int64_t)v.nblocks * kBS3;  // the flag buffer's per-block tail
     unsigned char *lam_zero = status + v.nblocks;
-    adj_mu_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, meta, ih2, phi, lam, lam_zero, mu, flags, status, rho, dt,
-                                                   1. / Dw, grad_acc);
-    adj_lambda_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, H, ih2, phi, mu, flags, status, lam, lam_zero, rho, dt);
-    return cudaGetLastError();
+    cudaError_t e = launch_pdl(adj_mu_kernel<Real>, v.nblocks, 128, s, v, H, meta, ih2, phi, (const Real *)lam,
+                               (const unsigned char *)lam_zero, mu, flags, status, rho, dt, 1. / Dw, grad_acc);
+    if (e != cudaSuccess) return e;
+    return launch_pdl(adj_lambda_kernel<Real>, v.nblocks, 128, s, v, H, ih2, phi, (const Real *)mu,
+                      (const unsigned char *)flags, (const unsigned char *)status, lam, lam_zero, rho, dt);
 }
 
 template <typename Real>

@@ -473,6 +473,13 @@ __global__ void __launch_bounds__((kWarps + 1) * 32, kWarps == 8 ? (sizeof(Real)
 rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __grid_constant__ CUtensorMap map_x,
                    const __grid_constant__ CUtensorMap map_y, const __grid_constant__ CUtensorMap map_z)
 {
+    // Programmatic dependent launch: a step launched with it may be scheduled
+    // while the previous grid on the stream still runs; it waits here until
+    // that grid has completed and its writes are visible, then allows the
+    // next step's grid to be scheduled as this one's CTAs finish.  Without
+    // the launch attribute both instructions return at once.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     using Lay = SmemLayout<Real, kHeavySlots, kEmptySlots>;
     constexpr int kThreads = kWarps * 32;  // consumer threads
     constexpr int kCells = kBS3 / kThreads;
@@ -825,8 +832,19 @@ struct Shape {
         const int nctas = items < g ? items : g;
         auto k = clamped ? rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true, Source>
                          : rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false, Source>;
-        k<<<nctas, kThreads, kSmem, s>>>(src, ih2, err_flag, maps[0], maps[1], maps[2]);
-        return cudaGetLastError();
+        // one pool: launched with programmatic dependent launch, so that the
+        // next step's launch overlaps this step's tail
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(nctas);
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = kSmem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = Source::kSamples ? 0 : 1;
+        return cudaLaunchKernelEx(&cfg, k, src, ih2, err_flag, maps[0], maps[1], maps[2]);
     }
 };
 
