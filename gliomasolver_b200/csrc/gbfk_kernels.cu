@@ -5,6 +5,32 @@
 
 namespace gbfk {
 
+// Programmatic dependent launch (kernels launched by launch_pdl): wait until
+// the previous grid on the stream has completed and its writes are visible,
+// then let the next grid be scheduled as this one's CTAs finish.  Without
+// the launch attribute both instructions return at once.
+__device__ __forceinline__ void pdl_wait_then_release()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename K, typename... Args>
+cudaError_t launch_pdl(K kernel, int grid, int threads, cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+
 // Position of lab cell (x, y, z) in [-1, 9)^3 among a block's 488 ghosts, in
 // BlockLab::load's visiting order (MRAG/MRAGcore/MRAGBlockLab.h:256-279);
 // -1 for the interior.  Filled by init_ghost_table() at library load.
@@ -420,6 +446,7 @@ rd_step_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned shor
                Real *__restrict__ dphidt_out, Real rho, double dt, int dt_finite, unsigned *nan_flag)
 {
     __shared__ __align__(16) Real ph[kStepLab];
+    pdl_wait_then_release();
     step_block<Real, kWriteRhs>(v, blockIdx.x, ph, H, meta, ih2blk, phi_in, phi_out, dphidt_out, rho, dt, dt_finite,
                                 nan_flag);
 }
@@ -475,12 +502,10 @@ cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigne
     if (v.nblocks <= 0) return cudaSuccess;
     const int dt_finite = isfinite(dt) ? 1 : 0;
     if (dphidt_out)
-        rd_step_kernel<Real, true><<<v.nblocks, 128, 0, s>>>(v, H, meta, ih2, phi_in, phi_out, dphidt_out, rho, dt,
-                                                             dt_finite, nan_flag);
-    else
-        rd_step_kernel<Real, false><<<v.nblocks, 128, 0, s>>>(v, H, meta, ih2, phi_in, phi_out, dphidt_out, rho,
-                                                              dt, dt_finite, nan_flag);
-    return cudaGetLastError();
+        return launch_pdl(rd_step_kernel<Real, true>, v.nblocks, 128, s, v, H, meta, ih2, phi_in, phi_out,
+                          dphidt_out, rho, dt, dt_finite, nan_flag);
+    return launch_pdl(rd_step_kernel<Real, false>, v.nblocks, 128, s, v, H, meta, ih2, phi_in, phi_out, dphidt_out,
+                      rho, dt, dt_finite, nan_flag);
 }
 
 // ---------------------------------------------------------------------------
@@ -513,31 +538,6 @@ cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigne
 // equals the dense computation's (a zero block's cells are +0 where the
 // dense kernels could produce -0: a sign of zero that no later product or
 // sum turns into a different number).
-
-// Programmatic dependent launch (kernels launched by launch_pdl): wait until
-// the previous grid on the stream has completed and its writes are visible,
-// then let the next grid be scheduled as this one's CTAs finish.  Without
-// the launch attribute both instructions return at once.
-__device__ __forceinline__ void pdl_wait_then_release()
-{
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
-template <typename K, typename... Args>
-cudaError_t launch_pdl(K kernel, int grid, int threads, cudaStream_t s, Args... args)
-{
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(threads);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, args...);
-}
 
 __device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
 {
@@ -999,6 +999,7 @@ __global__ void fill_ghosts_kernel(const int *__restrict__ rows, int64_t nrows,
                                    const Real *__restrict__ w, const Real *__restrict__ field,
                                    Real *__restrict__ ghosts)
 {
+    pdl_wait_then_release();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrows;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int r = rows[i];
@@ -1015,8 +1016,7 @@ cudaError_t launch_fill_ghosts(const int *rows, int64_t nrows, const int64_t *ro
     if (nrows <= 0) return cudaSuccess;
     int64_t nb = (nrows + 255) / 256;
     if (nb > 148 * 32) nb = 148 * 32;
-    fill_ghosts_kernel<Real><<<(int)nb, 256, 0, s>>>(rows, nrows, row_ptr, src, w, field, ghosts);
-    return cudaGetLastError();
+    return launch_pdl(fill_ghosts_kernel<Real>, (int)nb, 256, s, rows, nrows, row_ptr, src, w, field, ghosts);
 }
 
 // ---------------------------------------------------------------------------
