@@ -500,7 +500,11 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
     const int c = blockIdx.x, G = gridDim.x;
     const int NH = src.total_heavy(), NE = src.total_empty();
     const int nh = NH > c ? (NH - 1 - c) / G + 1 : 0;
-    const int ne = NE > c ? (NE - 1 - c) / G + 1 : 0;
+    // empty items: one pool counts them from the other end (CTA c takes
+    // G - 1 - c, 2G - 1 - c, ...), so that the CTAs that get one more heavy
+    // item than others get no more empty ones; a batch: c, c + G, ...
+    const int ce = Source::kSamples ? c : G - 1 - c;
+    const int ne = NE > ce ? (NE - 1 - ce) / G + 1 : 0;
     if (nh + ne == 0) return;  // uniform across the CTA
     // one pool: the CTA's items staged in shared memory, issued by lane 0
     // alone; a batch: decoded 32 at a time by the producer warp
@@ -513,7 +517,7 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
         }
         int unused;
         for (int i = t; i < nh; i += blockDim.x) src.heavy_item(c + i * G, unused, items[i]);
-        for (int i = t; i < ne; i += blockDim.x) src.empty_item(c + i * G, unused, items[nh + i]);
+        for (int i = t; i < ne; i += blockDim.x) src.empty_item(ce + i * G, unused, items[nh + i]);
     }
     if (t == 0) {
         for (int i = 0; i < kHeavySlots; i++) {
