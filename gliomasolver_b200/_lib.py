@@ -36,7 +36,7 @@ EXPORTS = (
     "gbfk_set_uniform", "gbfk_set_topology", "gbfk_num_blocks",
     "gbfk_upload_field", "gbfk_download_field", "gbfk_upload_dense", "gbfk_download_dense",
     "gbfk_rd_step", "gbfk_set_step_kernel", "gbfk_step_kernel",
-    "gbfk_rd_rhs", "gbfk_cfl", "gbfk_fwt_details", "gbfk_split", "gbfk_collapse",
+    "gbfk_rd_rhs", "gbfk_cfl", "gbfk_rd_step_host", "gbfk_join_copies", "gbfk_fwt_details", "gbfk_split", "gbfk_collapse",
     "gbfk_rd_step_static",
     "gbfk_set_observations", "gbfk_uq_dump", "gbfk_log_likelihood",
     "gbfk_batch_create", "gbfk_batch_destroy", "gbfk_batch_last_error", "gbfk_batch_launch_count",
@@ -162,6 +162,8 @@ def load(path: Path | str | None = None):
         "gbfk_step_kernel": (I, [P]),
         "gbfk_rd_rhs": (I, [P, D, D, D, P]),
         "gbfk_cfl": (I, [P, D, D, P]),
+        "gbfk_rd_step_host": (I, [P, P, P, D, D, D, D, I]),
+        "gbfk_join_copies": (I, [P]),
         "gbfk_fwt_details": (I, [P, P]),
         "gbfk_split": (I, [P, I, P, P]),
         "gbfk_collapse": (I, [P, I, P, P]),

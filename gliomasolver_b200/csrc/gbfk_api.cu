@@ -103,6 +103,14 @@ struct gbfk_ctx {
     std::vector<void *> adj_mem;
     size_t adj_fbytes = 0;
     int adj_nblocks = 0, adj_nsnap = 0;
+    // gbfk_rd_step_host: an input and an output copy stream, two sets of
+    // staging buffers and their events (set k & 1 serves call k)
+    cudaStream_t io_in_stream = nullptr, io_out_stream = nullptr;
+    void *io_in[2] = {nullptr, nullptr}, *io_out[2] = {nullptr, nullptr};
+    size_t io_bytes = 0;
+    cudaEvent_t io_ev[4][2] = {};  // in ready, in free, out ready, out free
+    bool io_ready = false;
+    int64_t io_calls = 0;
     double *d_fwt = nullptr;
     int *d_ints = nullptr;
     size_t ints_cap = 0;
@@ -678,6 +686,17 @@ int gbfk_destroy(gbfk_ctx *ctx)
         if (p) cudaFree(p);
     for (void *p : ctx->adj_mem)
         if (p) cudaFree(p);
+    if (ctx->io_ready) {
+        cudaStreamSynchronize(ctx->io_in_stream);
+        cudaStreamSynchronize(ctx->io_out_stream);
+        for (int j = 0; j < 2; j++) {
+            cudaFree(ctx->io_in[j]);
+            cudaFree(ctx->io_out[j]);
+            for (int k = 0; k < 4; k++) cudaEventDestroy(ctx->io_ev[k][j]);
+        }
+        cudaStreamDestroy(ctx->io_in_stream);
+        cudaStreamDestroy(ctx->io_out_stream);
+    }
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return GBFK_OK;
@@ -685,10 +704,22 @@ int gbfk_destroy(gbfk_ctx *ctx)
 
 const char *gbfk_last_error(const gbfk_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+int gbfk_join_copies(gbfk_ctx *ctx)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (ctx->io_calls == 0) return GBFK_OK;
+    CK(cudaSetDevice(ctx->device));
+    // the output stream runs its copies in order: its last event covers them all
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->io_ev[3][(ctx->io_calls - 1) & 1], 0));
+    return GBFK_OK;
+}
+
 int gbfk_sync(gbfk_ctx *ctx)
 {
     if (!ctx) return GBFK_E_INVALID;
     CK(cudaSetDevice(ctx->device));
+    int rc = gbfk_join_copies(ctx);
+    if (rc) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return check_stage_timeout(ctx);
 }
@@ -906,6 +937,76 @@ int gbfk_upload_dense(gbfk_ctx *ctx, int field, const void *host, int n)
 }
 
 int gbfk_download_dense(gbfk_ctx *ctx, int field, void *host, int n) { return dense_io(ctx, field, host, n, false); }
+
+int gbfk_rd_step_host(gbfk_ctx *ctx, const void *host_in, void *host_out, double Dw, double Dg, double rho,
+                      double dt, int nsteps)
+{
+    if (!ctx) return GBFK_E_INVALID;
+    if (!ctx->have_topology || !ctx->uniform) return fail(ctx, GBFK_E_STATE, "rd_step_host: needs a uniform grid");
+    if (!host_in || !host_out || nsteps < 0) return fail(ctx, GBFK_E_INVALID, "rd_step_host: bad arguments");
+    CK(cudaSetDevice(ctx->device));
+    const int n = 8 * ctx->bpd;
+    const size_t bytes = (size_t)n * n * n * ctx->rsize;
+    if (!ctx->io_ready || ctx->io_bytes < bytes) {
+        if (ctx->io_ready) {
+            CK(cudaStreamSynchronize(ctx->io_in_stream));
+            CK(cudaStreamSynchronize(ctx->io_out_stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            for (int j = 0; j < 2; j++) {
+                cudaFree(ctx->io_in[j]);
+                cudaFree(ctx->io_out[j]);
+                ctx->io_in[j] = ctx->io_out[j] = nullptr;
+            }
+        } else {
+            CK(cudaStreamCreateWithFlags(&ctx->io_in_stream, cudaStreamNonBlocking));
+            CK(cudaStreamCreateWithFlags(&ctx->io_out_stream, cudaStreamNonBlocking));
+            for (int j = 0; j < 2; j++)
+                for (int k = 0; k < 4; k++) CK(cudaEventCreateWithFlags(&ctx->io_ev[k][j], cudaEventDisableTiming));
+            ctx->io_ready = true;
+        }
+        ctx->io_bytes = 0;
+        ctx->io_calls = 0;
+        for (int j = 0; j < 2; j++) {
+            CK(cudaMalloc(&ctx->io_in[j], bytes));
+            CK(cudaMalloc(&ctx->io_out[j], bytes));
+        }
+        ctx->io_bytes = bytes;
+    }
+    const int j = (int)(ctx->io_calls & 1);
+    cudaEvent_t *ev_in_ready = ctx->io_ev[0], *ev_in_free = ctx->io_ev[1], *ev_out_ready = ctx->io_ev[2],
+                *ev_out_free = ctx->io_ev[3];
+    // input: H2D on the input stream once call k - 2 has scattered this staging buffer
+    if (ctx->io_calls >= 2) CK(cudaStreamWaitEvent(ctx->io_in_stream, ev_in_free[j], 0));
+    CK(cudaMemcpyAsync(ctx->io_in[j], host_in, bytes, cudaMemcpyHostToDevice, ctx->io_in_stream));
+    CK(cudaEventRecord(ev_in_ready[j], ctx->io_in_stream));
+    // the context's stream: scatter into the blocks, the steps, gather
+    CK(cudaStreamWaitEvent(ctx->stream, ev_in_ready[j], 0));
+    void *phi = field_ptr(ctx, GBFK_PHI);
+    if (ctx->precision == GBFK_F64)
+        CK(launch_dense_scatter<double>((const double *)ctx->io_in[j], (double *)phi, n, true, ctx->stream));
+    else
+        CK(launch_dense_scatter<float>((const float *)ctx->io_in[j], (float *)phi, n, true, ctx->stream));
+    CK(cudaEventRecord(ev_in_free[j], ctx->stream));
+    ctx->launches++;
+    ctx->phi_clamped = false;
+    const int rc = ctx->precision == GBFK_F64 ? rd_step_impl<double>(ctx, Dw, Dg, rho, dt, nsteps, 0)
+                                              : rd_step_impl<float>(ctx, Dw, Dg, rho, dt, nsteps, 0);
+    if (rc) return rc;
+    if (ctx->io_calls >= 2) CK(cudaStreamWaitEvent(ctx->stream, ev_out_free[j], 0));
+    phi = field_ptr(ctx, GBFK_PHI);
+    if (ctx->precision == GBFK_F64)
+        CK(launch_dense_scatter<double>((const double *)phi, (double *)ctx->io_out[j], n, false, ctx->stream));
+    else
+        CK(launch_dense_scatter<float>((const float *)phi, (float *)ctx->io_out[j], n, false, ctx->stream));
+    CK(cudaEventRecord(ev_out_ready[j], ctx->stream));
+    ctx->launches++;
+    // output: D2H on the output stream, overlapping the next call's input copy
+    CK(cudaStreamWaitEvent(ctx->io_out_stream, ev_out_ready[j], 0));
+    CK(cudaMemcpyAsync(host_out, ctx->io_out[j], bytes, cudaMemcpyDeviceToHost, ctx->io_out_stream));
+    CK(cudaEventRecord(ev_out_free[j], ctx->io_out_stream));
+    ctx->io_calls++;
+    return GBFK_OK;
+}
 
 int gbfk_rd_step(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int nsteps, int check_nan)
 {

@@ -51,6 +51,7 @@ class BlockPool:
         self.lib = _lib.load()
         self.precision = precision
         self.dtype = np.float64 if precision == "f64" else np.float32
+        self._io_keep = []  # host buffers of rd_step_host calls not yet synced
         cfg = _lib.Config(_lib.GBFK_F64 if precision == "f64" else _lib.GBFK_F32, int(max_blocks),
                           int(device), stream)
         h = ctypes.c_void_p()
@@ -94,6 +95,7 @@ class BlockPool:
 
     def sync(self):
         self._check(self.lib.gbfk_sync(self.ctx))
+        self._io_keep.clear()
 
     # -- topology ---------------------------------------------------------
     def set_uniform(self, blocks_per_dim: int):
@@ -159,6 +161,21 @@ class BlockPool:
         out = np.empty(self.num_blocks * BLOCK_CELLS, dtype=self.dtype)
         self._check(self.lib.gbfk_rd_rhs(self.ctx, float(Dw), float(Dg), float(rho), _ptr(out)))
         return out
+
+    def rd_step_host(self, phi_in: np.ndarray, phi_out: np.ndarray, Dw, Dg, rho, dt, nsteps: int = 1):
+        """Asynchronous host-to-host steps (gbfk_rd_step_host): phi_in (dense
+        n^3) in, nsteps steps, phi out into phi_out.  Both arrays are kept
+        alive here and must stay untouched until sync()."""
+        for a in (phi_in, phi_out):
+            if a.dtype != self.dtype or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError("phi_in and phi_out must be C-contiguous arrays of the pool's Real")
+        self._io_keep.extend((phi_in, phi_out))
+        self._check(self.lib.gbfk_rd_step_host(self.ctx, _ptr(phi_in), _ptr(phi_out), float(Dw), float(Dg),
+                                               float(rho), float(dt), int(nsteps)))
+
+    def join_copies(self):
+        """Make the pool's stream wait for the copies of rd_step_host."""
+        self._check(self.lib.gbfk_join_copies(self.ctx))
 
     def cfl(self, Dw, Dg) -> dict:
         """The reference's CFL step at the finest leaf spacing, the smallest

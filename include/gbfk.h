@@ -163,6 +163,21 @@ int gbfk_rd_rhs(gbfk_ctx *ctx, double Dw, double Dg, double rho, void *host_dphi
  * out[0] = dt, out[1] = the smallest h, out[2] = the largest coefficient.
  * Dw, Dg: the rescaled coefficients, as for gbfk_rd_step.  Synchronises. */
 int gbfk_cfl(gbfk_ctx *ctx, double Dw, double Dg, double out[3]);
+/* Host-to-host stepping for solves whose state lives in host memory between
+ * calls (one sample after the other, each from its own initial state): phi
+ * is copied in from host_in (dense n^3 Real, x fastest, n = 8*bpd, uniform
+ * grids only), advanced nsteps steps as by gbfk_rd_step, and copied out to
+ * host_out.  Asynchronous: the copies run on two internal streams with two
+ * sets of staging buffers, so that the output copy of one call overlaps the
+ * input copy of the next (PCIe carries both directions at once).  host_in
+ * and host_out must stay untouched until gbfk_sync (pinned buffers give the
+ * overlap; pageable ones are copied synchronously).  gbfk_join_copies makes
+ * the context's stream wait for every copy issued so far, so that work or
+ * events recorded on it afterwards follow them; gbfk_sync joins and waits.
+ * NaN is not checked here (use gbfk_rd_step with check_nan). */
+int gbfk_rd_step_host(gbfk_ctx *ctx, const void *host_in, void *host_out, double Dw, double Dg, double rho,
+                      double dt, int nsteps);
+int gbfk_join_copies(gbfk_ctx *ctx);
 
 /* --- adaptivity ------------------------------------------------------- */
 /* Per block of the topology (in upload order) the max |detail| of the

@@ -227,3 +227,31 @@ def test_pipelined_step_kernel_selection(gbfk_lib):
         pool.rd_step(1e-3, 1e-4, 0.1, 0.5, 2, check_nan=True)
         assert pool.step_kernel == "pipelined"
         pool.sync()
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_host_to_host_steps_equal_upload_step_download(gbfk_lib, prec):
+    """gbfk_rd_step_host (asynchronous, two copy streams, two staging sets):
+    five calls in a row from different initial states, each output equal to
+    upload + gbfk_rd_step + download of the same state."""
+    R = np.float64 if prec == "f64" else np.float32
+    n = 32
+    pw, pg, c0, _ = make_case(n, 4)
+    s = make_schedule(0.2, 0.05, 150.0, 25.6, n // 8, prec)
+    rng = np.random.default_rng(9)
+    ins = [np.ascontiguousarray((c0 * rng.uniform(0.2, 1.0)).astype(R)) for _ in range(5)]
+    steps = [1, 3, 0, 7, 2]
+    with _pool(n, prec, pw.astype(R), pg.astype(R), ins[0]) as a, _pool(n, prec, pw.astype(R), pg.astype(R),
+                                                                        ins[0]) as b:
+        want = []
+        for x, k in zip(ins, steps):
+            b.upload_dense("phi", x)
+            b.rd_step(s.Dw, s.Dg, s.rho, s.dt, k)
+            want.append(b.download_dense("phi"))
+        outs = [np.empty_like(x) for x in ins]
+        for x, o, k in zip(ins, outs, steps):
+            a.rd_step_host(x, o, s.Dw, s.Dg, s.rho, s.dt, k)
+        a.sync()
+        for i in range(5):
+            assert np.array_equal(outs[i], want[i]), i
+        assert np.array_equal(a.download_dense("phi"), want[-1])
