@@ -65,6 +65,8 @@ struct gbfk_batch {
     // pipelined step: work lists, per-position parameters, tensor maps
     int *d_lists = nullptr;      // lists, list_off, hpref, epref, anatomy (one allocation)
     size_t lists_cap = 0;
+    int2 *d_dec = nullptr;       // decoded heavy items, then decoded empty items
+    size_t dec_cap = 0;
     BatchLists bl{};
     void *d_rho = nullptr;
     double *d_dt = nullptr;
@@ -232,6 +234,27 @@ int batch_lists(gbfk_batch *b)
     b->bl.hpref = b->bl.list_off + off.size();
     b->bl.epref = b->bl.hpref + ns + 1;
     b->bl.anatomy = b->bl.epref + ns + 1;
+    // every item decoded once: (position, entry) in global item order
+    const size_t nitems = (size_t)hpref[ns] + (size_t)epref[ns];
+    if (b->dec_cap < nitems) {
+        if (b->d_dec) cudaFree(b->d_dec);
+        b->d_dec = nullptr;
+        b->dec_cap = 0;
+        BK(cudaMalloc(&b->d_dec, std::max<size_t>(nitems, 1) * sizeof(int2)));
+        b->dec_cap = nitems;
+    }
+    std::vector<int2> dec(nitems);
+    for (int k = 0; k < ns; k++) {
+        const int a = anat[k];
+        for (int i = 0; i < nh[a]; i++) dec[(size_t)hpref[k] + i] = make_int2(k, lists[off[2 * a] + i]);
+        for (int i = 0; i < ne[a]; i++)
+            dec[(size_t)hpref[ns] + epref[k] + i] = make_int2(k, lists[off[2 * a + 1] + i] * 4);
+    }
+    if (nitems)
+        BK(cudaMemcpyAsync(b->d_dec, dec.data(), nitems * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
+    BK(cudaStreamSynchronize(b->stream));
+    b->bl.hdec = b->d_dec;
+    b->bl.edec = b->d_dec + hpref[ns];
     return GBFK_OK;
 }
 
@@ -619,7 +642,7 @@ int gbfk_batch_destroy(gbfk_batch *b)
     void *ptrs[] = {b->d_nbr,       b->d_ih2,    b->d_views, b->d_nan,      b->d_err,     b->d_rho, b->d_dt,
                     b->d_lists,     b->pw_all,   b->pg_all,  b->meta_all,   b->btype_all, b->phi_all[0],
                     b->phi_all[1],  b->H_all,    b->d_t1c,   b->d_flair,    b->d_pet,     b->d_roi, b->d_model,
-                    b->d_partial,   b->d_lik,    b->d_ball};
+                    b->d_partial,   b->d_lik,    b->d_ball,  b->d_dec};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);

@@ -119,6 +119,9 @@ struct BatchLists {
     const int *hpref;     // [positions + 1]: heavy blocks of positions before p
     const int *epref;     // [positions + 1]: empty blocks of positions before p
     const int *anatomy;   // [positions]
+    // the items decoded once per run: heavy item g is (position, block * 4 +
+    // type) = hdec[g], empty item g is (position, block * 4) = edec[g]
+    const int2 *hdec, *edec;
 };
 template <typename Real>
 cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int total_items, int log2_bpd,

@@ -305,15 +305,18 @@ struct BatchSource {
         }
         return lo;
     }
+    const int2 *hdec, *edec;  // the items decoded once per run (BatchLists)
     __device__ void heavy_item(int g, int &p, int &e) const
     {
-        p = position(hpref, nactive, g);
-        e = lists[list_off[2 * anatomy[p]] + (g - hpref[p])];
+        const int2 d = hdec[g];
+        p = d.x;
+        e = d.y;
     }
     __device__ void empty_item(int g, int &p, int &e) const
     {
-        p = position(epref, nactive, g);
-        e = lists[list_off[2 * anatomy[p] + 1] + (g - epref[p])] * 4;
+        const int2 d = edec[g];
+        p = d.x;
+        e = d.y;
     }
     __device__ void params(int p, double &r, double &d) const { r = (double)rho[p]; d = dt[p]; }
     __device__ const unsigned short *meta_of(int p) const { return meta + (int64_t)anatomy[p] * nblocks * kBS3; }
@@ -978,6 +981,8 @@ cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int tota
     src.hpref = bl.hpref;
     src.epref = bl.epref;
     src.anatomy = bl.anatomy;
+    src.hdec = bl.hdec;
+    src.edec = bl.edec;
     src.nactive = nactive;
     src.phi_in = phi_in;
     src.phi_out = phi_out;
