@@ -270,15 +270,14 @@ struct PoolSource {
 };
 
 // Work source of a TMCMC batch step: the active samples (positions
-// 0 .. nactive-1, longest horizon first) with their per-anatomy block lists;
-// hpref / epref are prefix sums of the heavy / empty block counts over the
-// positions.  Sample p's pool starts at block p * nblocks of the phi buffers
-// and of the face coefficients.
+// 0 .. nactive-1, longest horizon first); hpref / epref are prefix sums of
+// the heavy / empty block counts over the positions, and the items of every
+// position are decoded once per run (hdec, edec: global item g -> (position,
+// entry)), so that the active ones are a prefix.  Sample p's pool starts at
+// block p * nblocks of the phi buffers and of the face coefficients.
 template <typename Real>
 struct BatchSource {
     static constexpr bool kSamples = true;
-    const int *lists;       // per anatomy a: heavy entries at list_off[2a], empty entries at list_off[2a + 1]
-    const int *list_off;
     const int *hpref, *epref;
     const int *anatomy;     // per position
     int nactive;
@@ -294,18 +293,7 @@ struct BatchSource {
 
     __device__ int total_heavy() const { return hpref[nactive]; }
     __device__ int total_empty() const { return epref[nactive]; }
-    // position p with pref[p] <= g < pref[p + 1]
-    __device__ static int position(const int *pref, int n, int g)
-    {
-        int lo = 0, hi = n - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (pref[mid] <= g) lo = mid;
-            else hi = mid - 1;
-        }
-        return lo;
-    }
-    const int2 *hdec, *edec;  // the items decoded once per run (BatchLists)
+    const int2 *hdec, *edec;
     __device__ void heavy_item(int g, int &p, int &e) const
     {
         const int2 d = hdec[g];
@@ -976,8 +964,6 @@ cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int tota
     if (nactive <= 0 || total_items <= 0) return cudaSuccess;
     if (log2_bpd < 0) return cudaErrorInvalidValue;
     BatchSource<Real> src;
-    src.lists = bl.lists;
-    src.list_off = bl.list_off;
     src.hpref = bl.hpref;
     src.epref = bl.epref;
     src.anatomy = bl.anatomy;
