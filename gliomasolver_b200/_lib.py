@@ -44,6 +44,7 @@ EXPORTS = (
     "gbfk_batch_tile_shape", "gbfk_batch_graph_count",
     "gbfk_batch_download", "gbfk_batch_set_observations", "gbfk_batch_log_likelihood",
     "gbfk_forward_adjoint",
+    "gbfk_probe_bounded_wait",
     "gbfk_host_last_error", "gbfk_matrix_info", "gbfk_matrix_read", "gbfk_matrix_write", "gbfk_map_anatomy",
 )
 
@@ -185,6 +186,7 @@ def load(path: Path | str | None = None):
         "gbfk_batch_set_observations": (I, [P, P, P, P, P, I]),
         "gbfk_batch_log_likelihood": (I, [P, ctypes.POINTER(LikelihoodParams), I, P]),
         "gbfk_forward_adjoint": (I, [P, ctypes.POINTER(AdjointParams), ctypes.POINTER(AdjointResult), P]),
+        "gbfk_probe_bounded_wait": (I, [I, ctypes.POINTER(D)]),
         "gbfk_host_last_error": (ctypes.c_char_p, []),
         "gbfk_matrix_info": (I, [ctypes.c_char_p, ctypes.POINTER(I), ctypes.POINTER(I * 3), ctypes.POINTER(I)]),
         "gbfk_matrix_read": (I, [ctypes.c_char_p, P, I64]),

@@ -44,6 +44,7 @@
 #include <cstdlib>
 #include <mutex>
 
+#include "gbfk.h"
 #include "gbfk_exact.cuh"
 #include "gbfk_kernels.cuh"
 
@@ -1035,3 +1036,46 @@ template cudaError_t launch_rd_batch_step_tma<double>(const BatchLists &, int, i
                                                       cudaStream_t);
 
 }  // namespace gbfk
+
+// The bounded wait of the pipelined step, made to give up: one thread waits
+// for the completion of an mbarrier phase that nothing arrives on.  The wait
+// ends after its limit and the kernel records that in *err, as the step
+// records a copy that never landed, instead of hanging.
+namespace gbfk {
+__global__ void bounded_wait_probe_kernel(unsigned *err)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (!mbar_wait(&bar, 0)) atomicOr(err, 1u);
+    }
+}
+}  // namespace gbfk
+
+extern "C" int gbfk_probe_bounded_wait(int device, double *seconds)
+{
+    if (cudaSetDevice(device) != cudaSuccess) return GBFK_E_CUDA;
+    unsigned *d_err = nullptr, err = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float ms = 0;
+    cudaError_t e = cudaMalloc(&d_err, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(d_err, 0, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, 0);
+    if (e == cudaSuccess) {
+        gbfk::bounded_wait_probe_kernel<<<1, 32>>>(d_err);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess) e = cudaMemcpy(&err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (d_err) cudaFree(d_err);
+    if (e != cudaSuccess) return GBFK_E_CUDA;
+    if (seconds) *seconds = ms / 1e3;
+    return err ? GBFK_E_TIMEOUT : GBFK_OK;
+}

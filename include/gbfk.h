@@ -370,6 +370,16 @@ int gbfk_map_anatomy(int precision, int bpd, const int msize[3], const double *g
                      const double *csf, const double tumor_ic[3], void *pw, void *pg, void *pcsf, void *phi,
                      void *tissue, double *L);
 
+/* --- failure detection ------------------------------------------------ */
+/* No counterpart in the reference.  Checks on `device` that the bounded wait
+ * of the pipelined step gives up instead of hanging: a one-thread kernel
+ * waits for an mbarrier phase that nothing completes, the wait ends after its
+ * limit (1 s of device time) and the kernel records it, as a step records a
+ * copy that never landed.  Returns GBFK_E_TIMEOUT (what gbfk_rd_step reports
+ * for such a step) with the seconds the kernel took; GBFK_OK would mean the
+ * phase completed, GBFK_E_CUDA a failed CUDA call.  The device stays usable. */
+int gbfk_probe_bounded_wait(int device, double *seconds);
+
 /* --- allocation-free step -------------------------------------------- */
 /* No counterpart in the reference.  One fused RD step (the operator and the
  * update of gbfk_rd_step) on a uniform periodic bpd^3 grid, for callers that

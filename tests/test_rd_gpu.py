@@ -255,3 +255,24 @@ def test_host_to_host_steps_equal_upload_step_download(gbfk_lib, prec):
         for i in range(5):
             assert np.array_equal(outs[i], want[i]), i
         assert np.array_equal(a.download_dense("phi"), want[-1])
+
+
+def test_bounded_wait_gives_up_and_the_device_stays_usable(gbfk_lib):
+    """Failure detection without a fault: a wait on an mbarrier phase that
+    nothing completes (the bounded wait of the pipelined step) gives up after
+    its 1 s limit and is reported as GBFK_E_TIMEOUT; the device keeps working."""
+    import ctypes
+
+    from gliomasolver_b200._lib import STATUS_CODES
+
+    secs = ctypes.c_double(0)
+    rc = gbfk_lib.gbfk_probe_bounded_wait(0, ctypes.byref(secs))
+    assert rc == STATUS_CODES["GBFK_E_TIMEOUT"]
+    assert 0.9 < secs.value < 10.0
+    n = 16
+    pw, pg, c0, _ = make_case(n, 2)
+    s = make_schedule(0.13, 0.025, 150.0, 25.6, n // 8, "f64")
+    with _pool(n, "f64", pw, pg, c0) as pool:
+        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 4, check_nan=True)
+        got = pool.download_dense("phi")
+    assert np.array_equal(got, O.rd_steps_dense(pw, pg, c0, s.Dw, s.Dg, s.rho, s.h, s.dt, 4))
