@@ -466,11 +466,12 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
                    const __grid_constant__ CUtensorMap map_y, const __grid_constant__ CUtensorMap map_z)
 {
     // Programmatic dependent launch: a step launched with it may be scheduled
-    // while the previous grid on the stream still runs; it waits here until
-    // that grid has completed and its writes are visible, then allows the
-    // next step's grid to be scheduled as this one's CTAs finish.  Without
-    // the launch attribute both instructions return at once.
-    asm volatile("griddepcontrol.wait;" ::: "memory");
+    // while the previous grid on the stream still runs.  It lets the next
+    // step's grid be scheduled as this one's CTAs finish, stages its work
+    // items (host-written lists, complete before any later kernel starts) and
+    // sets up its barriers, and only then waits until the previous grid has
+    // completed and its writes are visible, before any other global access.
+    // Without the launch attribute both instructions return at once.
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     using Lay = SmemLayout<Real, kHeavySlots, kEmptySlots>;
     constexpr int kThreads = kWarps * 32;  // consumer threads
@@ -523,6 +524,7 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();  // the only CTA-wide barrier
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 
     const int L = src.L;
     const int lane = t & 31;
