@@ -279,9 +279,8 @@ void face_positions(int f, int p, int &lx, int &ly, int &lz, int &src_cell)
 inline int lab_idx(int x, int y, int z) { return (x + 1) + kLab * ((y + 1) + kLab * (z + 1)); }
 
 template <typename Real>
-int set_csr(gbfk_ctx *ctx, const std::vector<int64_t> &row_ptr, const std::vector<int> &src,
-            const std::vector<double> &w0, const std::vector<double> &w1, const std::vector<double> &w2,
-            bool detect_direct)
+int set_csr(gbfk_ctx *ctx, const int64_t *row_ptr, const std::vector<int> &src, const double *w0, const double *w1,
+            const double *w2, bool detect_direct)
 {
     const int nb = ctx->nblocks;
     const int64_t nrows = (int64_t)nb * kLabGhosts;
@@ -334,7 +333,7 @@ int set_csr(gbfk_ctx *ctx, const std::vector<int64_t> &row_ptr, const std::vecto
     CK(cudaMalloc(&ctx->d_gpw, nrows * sizeof(Real)));
     CK(cudaMalloc(&ctx->d_gpg, nrows * sizeof(Real)));
     CK(cudaMalloc(&ctx->d_gphi, nrows * sizeof(Real)));
-    CK(cudaMemcpy(ctx->d_row_ptr, row_ptr.data(), (nrows + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_row_ptr, row_ptr, (nrows + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
     if (nnz) {
         CK(cudaMemcpy(ctx->d_src, src.data(), nnz * sizeof(int), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(ctx->d_w, w.data(), nnz * sizeof(Real), cudaMemcpyHostToDevice));
@@ -380,8 +379,9 @@ int build_uniform_csr(gbfk_ctx *ctx)
                         }
             }
     if (ctx->d_nbr) { cudaFree(ctx->d_nbr); ctx->d_nbr = nullptr; }
-    return ctx->precision == GBFK_F64 ? set_csr<double>(ctx, row_ptr, src, ones, ones, ones, true)
-                                      : set_csr<float>(ctx, row_ptr, src, ones, ones, ones, true);
+    return ctx->precision == GBFK_F64
+               ? set_csr<double>(ctx, row_ptr.data(), src, ones.data(), ones.data(), ones.data(), true)
+               : set_csr<float>(ctx, row_ptr.data(), src, ones.data(), ones.data(), ones.data(), true);
 }
 
 template <typename Real>
@@ -847,10 +847,8 @@ int gbfk_set_topology(gbfk_ctx *ctx, const gbfk_blockinfo *blocks, int nblocks, 
         for (int i = 0; i < nblocks; i++) hv[i] = (float)ctx->h_h[i];
         CK(cudaMemcpy(ctx->d_h, hv.data(), nblocks * sizeof(float), cudaMemcpyHostToDevice));
     }
-    std::vector<int64_t> row_ptr(g->row_ptr, g->row_ptr + g->nrows + 1);
-    std::vector<double> w0(g->w0, g->w0 + nnz), w1(g->w1, g->w1 + nnz), w2(g->w2, g->w2 + nnz);
-    int rc = ctx->precision == GBFK_F64 ? set_csr<double>(ctx, row_ptr, src, w0, w1, w2, true)
-                                        : set_csr<float>(ctx, row_ptr, src, w0, w1, w2, true);
+    int rc = ctx->precision == GBFK_F64 ? set_csr<double>(ctx, g->row_ptr, src, g->w0, g->w1, g->w2, true)
+                                        : set_csr<float>(ctx, g->row_ptr, src, g->w0, g->w1, g->w2, true);
     if (rc) return rc;
     rc = upload_ih2(ctx);
     if (rc) return rc;
