@@ -43,12 +43,18 @@ def needs_build() -> bool:
 def build_library(force: bool = False, verbose: bool = False) -> Path:
     if not force and not needs_build():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-I", str(ROOT / "include"), *[str(HERE / s) for s in SOURCES],
-           "-o", str(OUT) + ".tmp"]
+    # a temporary name per process: ranks that build at the same time each
+    # replace the library atomically with a complete file
+    tmp = f"{OUT}.tmp{os.getpid()}"
+    cmd = [nvcc(), *NVCC_FLAGS, "-I", str(ROOT / "include"), *[str(HERE / s) for s in SOURCES], "-o", tmp]
     if verbose:
         print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
-    os.replace(str(OUT) + ".tmp", OUT)
+    try:
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, OUT)
+    finally:
+        if os.path.exists(tmp):
+            os.remove(tmp)
     return OUT
 
 
