@@ -73,6 +73,8 @@ def _declare(L):
     L.orc_collapse_blocks_f32.argtypes = [P, P]
     L.orc_uq_dump_f64.argtypes = [I, P, P, P, P, I, P]
     L.orc_uq_dump_f32.argtypes = [I, P, P, P, P, I, P]
+    L.orc_adjoint_step_dense_f64.argtypes = [I, P, P, P, D, D, D, D, D, P, P, P]
+    L.orc_loss_grad_f64.argtypes = [I64, P, P, P, D, D, D, P]
     L.orc_map_anatomy_f64.argtypes = [I, I, I, I, P, P, P, P, P, P, P, P, P]
     L.orc_map_anatomy_f32.argtypes = [I, I, I, I, P, P, P, P, P, P, P, P, P]
     L.orc_log_likelihood.argtypes = [I, P, P, P, P, P, I, D, D, D, D, D, I, I, P]
@@ -175,6 +177,33 @@ def log_likelihood(model, t1c, flair, pet=None, roi=None, pet_sigma2=0.000361, p
                              None if ro is None else _p(ro), 0 if ro is None else ro.size // 3,
                              pet_sigma2, pet_scale, t1_uc, t2_uc, slope, step_pet, step_mri, out)
     return np.array([float(out[0]), float(out[1]), float(out[2])])
+
+
+def adjoint_dense(pw, pg, phi0, Dw, Dg, rho, h, dt, nsteps, lam_final):
+    """The discrete adjoint of nsteps FP64 steps (orc_adjoint_step_dense_f64,
+    every state stored): returns (dL/dphi0, dL/drho, dL/dDw) for a loss whose
+    gradient with respect to the final state is lam_final."""
+    L = lib()
+    n = phi0.shape[0]
+    pw, pg = (np.ascontiguousarray(a, dtype=np.float64) for a in (pw, pg))
+    states = [np.ascontiguousarray(phi0, dtype=np.float64)]
+    for _ in range(nsteps):
+        states.append(rd_steps_dense(pw, pg, states[-1], Dw, Dg, rho, h, dt, 1))
+    lam = np.array(lam_final, dtype=np.float64, copy=True)
+    grad = np.zeros(2)
+    scratch = np.empty(8 * n ** 3)
+    for k in range(nsteps - 1, -1, -1):
+        L.orc_adjoint_step_dense_f64(n, _p(pw), _p(pg), _p(states[k]), float(Dw), float(Dg), float(rho), float(h),
+                                     float(dt), _p(lam), _p(grad), _p(scratch))
+    return lam, float(grad[0]), float(grad[1])
+
+
+def loss_grad(u, t1c, flair, t1uc=0.7, t2uc=0.25, slope=2.0):
+    """d(-(L_T1c + L_FLAIR))/du (orc_loss_grad_f64)."""
+    u, t1c, flair = (np.ascontiguousarray(a, dtype=np.float64) for a in (u, t1c, flair))
+    out = np.empty_like(u)
+    lib().orc_loss_grad_f64(u.size, _p(u), _p(t1c), _p(flair), float(t1uc), float(t2uc), float(slope), _p(out))
+    return out
 
 
 def map_anatomy(gm, wm, csf, bpd, tumor_ic, precision="f64"):

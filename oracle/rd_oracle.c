@@ -479,3 +479,111 @@ void orc_log_likelihood(int n, const double *model, const double *t1c, const dou
     }
 ORC_MAP_ANATOMY(f64, double, sqrt)
 ORC_MAP_ANATOMY(f32, float, sqrtf)
+
+/* ------------------------------------------------------------------------ */
+/* The discrete adjoint of one fused step on a dense periodic grid, FP64: the
+ * derivative of the step of orc_rd_steps_dense_f64 (ReactionDiffusionOperator
+ * + UpdateTumor, ReactionDiffusionOperator.h:97-138,189-226) with its
+ * piecewise-constant switches held fixed: the domain test, the no-flux
+ * doubling of the coefficient opposite a neighbour with chf < 0.1, the clamp
+ * (derivative 1 where 0 < phi + dt*dphidt <= 1).  With
+ *   r_i = ih2 sum_k df_ik phi_k - ih2 (sum_k df_ik) phi_i + rho phi_i (1 - phi_i)
+ * (df_ik the doubled harmonic mean towards neighbour k, 0 outside the domain):
+ *   mu_i     = lam'_i [0 < pre_i <= 1]
+ *   lam_j    = mu_j + dt ( dom_j mu_j (-ih2 sum_k df_jk + rho (1 - 2 phi_j))
+ *                         + ih2 sum_{k} dom_i mu_i df_i,k^1 ),  i = j + e_k
+ *   grad[0] += sum_i dom_i mu_i dt phi_i (1 - phi_i)             (d / d rho)
+ *   grad[1] += sum_i dom_i mu_i dt (diffusive part of r_i) / Dw   (d / d Dw, Dg = 0.1 Dw:
+ *              the coefficients are homogeneous of degree 1 in Dw)
+ * phi is the state the step maps forward; lam holds dL/dphi' on entry and
+ * dL/dphi on exit; scratch holds 8 n^3 doubles. */
+void orc_adjoint_step_dense_f64(int n, const double *pw, const double *pg, const double *phi, double Dw,
+                                double Dg, double rho, double h, double dt, double *lam, double grad[2],
+                                double *scratch)
+{
+    const int64_t nn = n, N = nn * nn * nn;
+    const double ih2 = 1. / (h * h);
+    double *mu = scratch, *dom = scratch + N, *dfs = scratch + 2 * N; /* dfs: 6 per cell */
+    for (int iz = 0; iz < n; iz++)
+        for (int iy = 0; iy < n; iy++)
+            for (int ix = 0; ix < n; ix++) {
+                const int xm = (ix + n - 1) % n, xp = (ix + 1) % n;
+                const int ym = (iy + n - 1) % n, yp = (iy + 1) % n;
+                const int zm = (iz + n - 1) % n, zp = (iz + 1) % n;
+                const int64_t id[7] = {ix + nn * (iy + nn * iz), xm + nn * (iy + nn * iz), xp + nn * (iy + nn * iz),
+                                       ix + nn * (ym + nn * iz), ix + nn * (yp + nn * iz), ix + nn * (iy + nn * zm),
+                                       ix + nn * (iy + nn * zp)};
+                const int64_t c = id[0];
+                double a[7], b[7], p[7], df[6] = {0, 0, 0, 0, 0, 0};
+                for (int k = 0; k < 7; k++) {
+                    a[k] = pw[id[k]];
+                    b[k] = pg[id[k]];
+                    p[k] = phi[id[k]];
+                }
+                const int d = a[0] + b[0] + p[0] > 0.;
+                double dphidt = 0., diff = 0.;
+                if (d) {
+                    const double df_loc = a[0] * Dw + b[0] * Dg;
+                    for (int k = 0; k < 6; k++) {
+                        const double dn = a[k + 1] * Dw + b[k + 1] * Dg;
+                        df[k] = (dn + df_loc < 1.0e-08) ? 0. : 2. * dn * df_loc / (dn + df_loc);
+                    }
+                    for (int k = 0; k < 6; k++)
+                        if (p[k + 1] + a[k + 1] + b[k + 1] < 0.1) df[k ^ 1] *= 2.0;
+                    const double in = ih2 * (df[0] * p[1] + df[1] * p[2] + df[2] * p[3] + df[3] * p[4] +
+                                             df[4] * p[5] + df[5] * p[6]);
+                    const double out = -((df[0] + df[1] + df[2] + df[3] + df[4] + df[5]) * p[0] * ih2);
+                    dphidt = out + in + rho * p[0] * (1. - p[0]);
+                    diff = out + in;
+                }
+                const double pre = p[0] + dt * dphidt;
+                const int pass = pre > 0. && pre <= 1.;
+                mu[c] = pass ? lam[c] : 0.;
+                dom[c] = d;
+                for (int k = 0; k < 6; k++) dfs[6 * c + k] = df[k];
+                if (d && pass) {
+                    grad[0] += mu[c] * dt * p[0] * (1. - p[0]);
+                    grad[1] += mu[c] * dt * diff / Dw;
+                }
+            }
+    for (int iz = 0; iz < n; iz++)
+        for (int iy = 0; iy < n; iy++)
+            for (int ix = 0; ix < n; ix++) {
+                const int xm = (ix + n - 1) % n, xp = (ix + 1) % n;
+                const int ym = (iy + n - 1) % n, yp = (iy + 1) % n;
+                const int zm = (iz + n - 1) % n, zp = (iz + 1) % n;
+                const int64_t c = ix + nn * (iy + nn * iz);
+                const int64_t nb[6] = {xm + nn * (iy + nn * iz), xp + nn * (iy + nn * iz), ix + nn * (ym + nn * iz),
+                                       ix + nn * (yp + nn * iz), ix + nn * (iy + nn * zm), ix + nn * (iy + nn * zp)};
+                double acc = 0.;
+                if (dom[c]) {
+                    double sdf = 0.;
+                    for (int k = 0; k < 6; k++) sdf += dfs[6 * c + k];
+                    acc += mu[c] * (-ih2 * sdf + rho * (1. - 2. * phi[c]));
+                }
+                for (int k = 0; k < 6; k++)
+                    if (dom[nb[k]]) acc += ih2 * dfs[6 * nb[k] + (k ^ 1)] * mu[nb[k]];
+                lam[c] = mu[c] + dt * acc;
+            }
+}
+
+/* d loss / du of loss = -(L_T1c + L_FLAIR) (HGG_Likelihood.cpp:136-156): the
+ * Bernoulli term with alpha = 1/2 + 1/2 sgn(u - uc) (1 - exp(-w2 / slope)),
+ * w2 = 1 above uc and (u - uc)^2 below, differentiated: above uc the terms are
+ * constant; below, with d = u - uc and e = exp(-d^2 / slope),
+ * d log(alpha) / du = -2 d / slope and d log(1 - alpha) / du = e d / slope / (1 - e/2). */
+void orc_loss_grad_f64(int64_t ncells, const double *u, const double *t1c, const double *flair, double t1uc,
+                       double t2uc, double slope, double *lam)
+{
+    for (int64_t i = 0; i < ncells; i++) {
+        double g = 0.;
+        for (int t = 0; t < 2; t++) {
+            const double d = u[i] - (t ? t2uc : t1uc);
+            const int y = (t ? flair[i] : t1c[i]) == 1.;
+            if (!(d < -0.0)) continue;
+            const double e = exp(-d * d / slope);
+            g += y ? -2. * d / slope : e * d / slope / (1. - 0.5 * e);
+        }
+        lam[i] = -g;
+    }
+}

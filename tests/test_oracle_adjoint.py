@@ -1,0 +1,62 @@
+"""The oracle's restatement of the discrete adjoint (orc_adjoint_step_dense_f64)
+and of the loss gradient (orc_loss_grad_f64), checked on the CPU against
+central differences of the oracle's own forward steps and likelihood: the
+reference for the device adjoint beside finite differences."""
+import numpy as np
+
+from gliomasolver_b200.anatomy import make_case
+from gliomasolver_b200.schedule import make_schedule
+from oracle import oracle as O
+
+
+def _case():
+    n = 16
+    pw, pg, _, _ = make_case(n, 2)
+    s = make_schedule(0.3, 0.1, 150.0, 25.6, n // 8, "f64")
+    x = np.arange(n) / n
+    zz, yy, xx = np.meshgrid(x, x, x, indexing="ij")
+    r2 = (xx - 0.5) ** 2 + (yy - 0.5) ** 2 + (zz - 0.5) ** 2
+    c0 = np.where(pw + pg > 0, 0.45 * np.exp(-r2 / 0.02), 0.0)
+    return pw, pg, c0, s
+
+
+def test_adjoint_matches_central_differences():
+    pw, pg, c0, s = _case()
+    nsteps = 12
+    w = np.random.default_rng(0).standard_normal(c0.shape)
+
+    def loss(phi0, Dw=s.Dw, rho=s.rho):
+        u = O.rd_steps_dense(pw, pg, phi0, Dw, 0.1 * Dw, rho, s.h, s.dt, nsteps)
+        return float(np.sum(w * u))
+
+    lam0, drho, ddw = O.adjoint_dense(pw, pg, c0, s.Dw, 0.1 * s.Dw, s.rho, s.h, s.dt, nsteps, w)
+    cells = np.argwhere((c0 > 0.05) & (c0 < 0.4))[::7][:8]
+    assert len(cells) == 8
+    for c in map(tuple, cells):
+        e = np.zeros_like(c0)
+        e[c] = 1e-6
+        fd = (loss(c0 + e) - loss(c0 - e)) / 2e-6
+        assert abs(fd - lam0[c]) <= 1e-6 * abs(fd) + 1e-9, c
+    er, ed = 1e-6 * s.rho, 1e-6 * s.Dw
+    fd_rho = (loss(c0, rho=s.rho + er) - loss(c0, rho=s.rho - er)) / (2 * er)
+    fd_dw = (loss(c0, Dw=s.Dw + ed) - loss(c0, Dw=s.Dw - ed)) / (2 * ed)
+    assert abs(drho - fd_rho) <= 1e-6 * abs(fd_rho)
+    assert abs(ddw - fd_dw) <= 1e-6 * abs(fd_dw)
+
+
+def test_loss_gradient_matches_central_differences():
+    rng = np.random.default_rng(4)
+    n = 8
+    u = rng.uniform(0, 1, (n, n, n))
+    t1c = (rng.uniform(0, 1, u.shape) > 0.6).astype(float)
+    flair = (rng.uniform(0, 1, u.shape) > 0.4).astype(float)
+    g = O.loss_grad(u, t1c, flair, 0.7, 0.25, 2.0)
+    for c in map(tuple, rng.integers(0, n, (12, 3))):
+        if min(abs(u[c] - 0.7), abs(u[c] - 0.25)) < 1e-3:
+            continue  # the likelihood is discontinuous at the thresholds
+        e = np.zeros_like(u)
+        e[c] = 1e-6
+        lp = O.log_likelihood(u + e, t1c, flair)
+        lm = O.log_likelihood(u - e, t1c, flair)
+        fd = -((lp[1] + lp[2]) - (lm[1] + lm[2])) / 2e-6
+        assert abs(fd - g[c]) <= 1e-5 * max(abs(fd), 1e-3), (c, fd, g[c])
