@@ -60,3 +60,31 @@ def test_loss_gradient_matches_central_differences():
         lm = O.log_likelihood(u - e, t1c, flair)
         fd = -((lp[1] + lp[2]) - (lm[1] + lm[2])) / 2e-6
         assert abs(fd - g[c]) <= 1e-5 * max(abs(fd), 1e-3), (c, fd, g[c])
+
+
+def test_origin_gradient_through_the_initial_condition():
+    """dL/dx0 = sum_i lambda0_i dc0_i/dx0 with c0 = exp(-|x - x0|^2 / (2 sigma^2))
+    where there is tissue (the Gaussian initial condition of the workloads),
+    against central differences of x0."""
+    from gliomasolver_b200.anatomy import tumor_ic
+
+    pw, pg, _, s = _case()
+    n, nsteps = pw.shape[0], 10
+    w = np.random.default_rng(1).standard_normal(pw.shape)
+    x0 = np.array([0.47, 0.52, 0.49])
+    sigma = 2.0 / n
+    x = np.arange(n) / n
+    zz, yy, xx = np.meshgrid(x, x, x, indexing="ij")
+
+    def loss(p):
+        c0 = tumor_ic(n, p, pw, pg)
+        return float(np.sum(w * O.rd_steps_dense(pw, pg, c0, s.Dw, s.Dg, s.rho, s.h, s.dt, nsteps)))
+
+    c0 = tumor_ic(n, x0, pw, pg)
+    lam0, _, _ = O.adjoint_dense(pw, pg, c0, s.Dw, s.Dg, s.rho, s.h, s.dt, nsteps, w)
+    grad = [float(np.sum(lam0 * c0 * (g - x0[d]) / sigma ** 2)) for d, g in enumerate((xx, yy, zz))]
+    for d in range(3):
+        e = np.zeros(3)
+        e[d] = 1e-7
+        fd = (loss(x0 + e) - loss(x0 - e)) / 2e-7
+        assert abs(fd - grad[d]) <= 1e-5 * abs(fd) + 1e-6, (d, fd, grad[d])
