@@ -12,7 +12,7 @@ Glioma_ReactionDiffusion.cpp:300-321).
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 
 import numpy as np
 
@@ -198,7 +198,7 @@ class Batch:
 @dataclass
 class TMCMCOptions:
     pop_size: int = 512
-    max_stages: int = 100
+    max_stages: int = 100         # MaxStages: generations, the prior one included
     tol_cov: float = 1.0          # TolCOV
     bbeta: float = 0.2            # proposal covariance scale
     min_chain: int = 0            # MinChainLength
@@ -215,6 +215,19 @@ class TMCMCResult:
     log_evidence: float
     acceptance: list              # per stage: accepted proposals / proposals
     evaluations: int
+    # Per generation g = 0 .. len(p) - 1, the quantities the reference keeps
+    # in its run record (engine_tmcmc.c:334-365, tmcmc_stats.c
+    # calculate_statistics): the population and its log-likelihoods, the
+    # distinct points among them, the COV of the weights that lead to
+    # generation g + 1, log of the evidence increment, the weighted mean and
+    # the weighted (unscaled) sample covariance.
+    stages: list = field(default_factory=list)          # [(theta, F)]
+    uniques: list = field(default_factory=list)
+    coef_var: list = field(default_factory=list)
+    log_selection: list = field(default_factory=list)
+    mean_theta: list = field(default_factory=list)
+    ss: np.ndarray = None                                # of the last generation
+    p_next: float = 1.0                                  # exponent after the last generation
 
 
 def _cov_of_weights(F, dp):
@@ -236,6 +249,18 @@ def next_exponent(F, p, tol_cov):
         else:
             lo = mid
     return max(lo, p + 1e-12)
+
+
+def _distinct_points(theta, tol=1e-6):
+    """How many points of the population differ from every earlier distinct
+    one in some coordinate by more than tol (engine_tmcmc.c:795-835)."""
+    table = np.empty_like(theta)
+    un = 0
+    for x in theta:
+        if un == 0 or not np.any(np.all(np.abs(table[:un] - x) <= tol, axis=1)):
+            table[un] = x
+            un += 1
+    return un
 
 
 def _posdef(S):
@@ -269,17 +294,30 @@ def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions()):
     p = [0.0]
     log_ev = 0.0
     acc = []
-    for _ in range(opts.max_stages):
+    rec = TMCMCResult(None, None, p, 0.0, acc, 0)
+
+    def record(theta, F, q, log_sel, mean, ss):
+        rec.stages.append((theta.copy(), F.copy()))
+        rec.uniques.append(_distinct_points(theta))
+        rec.coef_var.append(float(q.std(ddof=1) / q.mean()))
+        rec.log_selection.append(float(log_sel))
+        rec.mean_theta.append(mean)
+        rec.ss = _posdef(ss)
+
+    for _ in range(opts.max_stages - 1):
         pj = p[-1]
         pn = next_exponent(F, pj, opts.tol_cov)
         flcp = F * (pn - pj)
         w = np.exp(flcp - flcp.max())
-        log_ev += np.log(w.sum()) + flcp.max() - np.log(len(F))
+        log_sel = np.log(w.sum()) + flcp.max() - np.log(len(F))
+        log_ev += log_sel
         q = w / w.sum()
         sel = rng.multinomial(opts.pop_size, q)
         mean = q @ theta
         dev = theta - mean
-        cov = _posdef(opts.bbeta * (dev.T * q) @ dev)
+        ss = (dev.T * q) @ dev
+        cov = _posdef(opts.bbeta * ss)
+        record(theta, F, q, log_sel, mean, ss)
         # leaders with chain lengths (split at max_chain, raised to min_chain)
         chains = []
         for i in np.flatnonzero(sel):
@@ -320,7 +358,19 @@ def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions()):
         acc.append(naccept / max(nprop, 1))
         if pn >= 1.0:
             break
-    return TMCMCResult(theta, F, p, float(log_ev), acc, nevals)
+    # The last generation's own statistics, toward the exponent that would
+    # follow it (1 after the final stage, so uniform weights), as the
+    # reference computes them after its last stage.
+    pj = p[-1]
+    rec.p_next = 1.0 if pj >= 1.0 else next_exponent(F, pj, opts.tol_cov)
+    flcp = F * (rec.p_next - pj)
+    w = np.exp(flcp - flcp.max())
+    q = w / w.sum()
+    mean = q @ theta
+    dev = theta - mean
+    record(theta, F, q, np.log(w.sum()) + flcp.max() - np.log(len(F)), mean, (dev.T * q) @ dev)
+    rec.theta, rec.loglik, rec.log_evidence, rec.evaluations = theta, F, float(log_ev), nevals
+    return rec
 
 
 class GliomaModel:
