@@ -338,3 +338,38 @@ def ref_map_anatomy(prefix, bpd, tumor_ic, precision="f64"):
     for k, name in enumerate(("p_w", "p_g", "p_csf", "phi")):
         res[name] = raw[1 + k * n3:1 + (k + 1) * n3].reshape(n, n, n)
     return res
+
+
+def ref_topology_available(precision: str = "f64") -> bool:
+    return (REF_DIR / f"topo_harness_{precision}").exists()
+
+
+def read_topology_dump(path) -> dict:
+    """The records of oracle/_ref/topo_harness_*: int32 name length, name,
+    int32 kind (0 int64, 1 float64), int64 count, data."""
+    out = {}
+    with open(path, "rb") as f:
+        while True:
+            head = f.read(4)
+            if not head:
+                break
+            name = f.read(int(np.frombuffer(head, np.int32)[0])).decode()
+            kind = int(np.frombuffer(f.read(4), np.int32)[0])
+            count = int(np.frombuffer(f.read(8), np.int64)[0])
+            out[name] = np.frombuffer(f.read(8 * count), np.int64 if kind == 0 else np.float64).copy()
+    return out
+
+
+def ref_topology(base_bpd, maxlevel, refine_tol, every, precision="f64"):
+    """The reference's wavelet details, block split and collapse on an
+    adapted grid (oracle/_ref/topo_harness_*, one host thread so that the
+    grid is reproducible): a dict of the dump's arrays and the JSON summary
+    under "summary"."""
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "topo.bin")
+        r = subprocess.run([str(REF_DIR / f"topo_harness_{precision}"), str(int(base_bpd)), str(int(maxlevel)),
+                            _fmt(refine_tol), str(int(every)), out], check=True, capture_output=True, text=True,
+                           env=dict(os.environ, GBFK_ORACLE_THREADS="1"))
+        res = read_topology_dump(out)
+    res["summary"] = json.loads(r.stdout.strip().splitlines()[-1])
+    return res
