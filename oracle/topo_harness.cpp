@@ -8,9 +8,13 @@
  *
  * A grid of base_bpd^3 blocks (periodic, stencil [-1,2), as the RD operator
  * needs) is refined with Science::AutomaticRefinement up to maxlevel - 1 on
- * analytic fields (a Gaussian tumour and smooth tissue fractions, each value
- * rounded to a multiple of 2^-10 so that the dump compresses; resampled after
- * every refinement).  Then, on that grid:
+ * analytic fields (a Gaussian tumour, smooth tissue fractions and a ball of
+ * CSF without tissue, each value rounded to a multiple of 2^-10 so that the
+ * dump compresses; resampled after every refinement).  Then, on that grid:
+ *  - rhs: one sweep of the reference's ReactionDiffusionOperator through
+ *    BlockProcessing::pipeline_process (Glioma_ReactionDiffusion.cpp:176-183;
+ *    Dw = 0.2 cm^2/day on L = 25.6 cm, Dg = Dw/10, rho = 0.05/day): dphidt of
+ *    every leaf, with each leaf's h and the three coefficients in Real;
  *  - detail: BlockFWT::multichannel_fwt<0,0> (MRAG/MRAGcore/MRAGBlockFWT.h,
  *    the per-block detail AutomaticRefinement compares with its tolerance,
  *    MRAG/MRAGscience/MRAGScienceCore.h:68-79) of every leaf;
@@ -22,7 +26,8 @@
  *    back, its cells.
  * The dump holds, for the grid before the split: the leaves (level, index)
  * in vInfo order, the ghost lists flattened by include/gbfk_mrag.hpp, p_w,
- * p_g, phi slot-major (512 per leaf, x fastest), the details; then the split
+ * p_g, phi slot-major (512 per leaf, x fastest), rhs, h, the coefficients,
+ * the details; then the split
  * parents' slots with their children's fields, and the collapsed parents
  * (their positions in the split list) with their fields.  Format: records of
  * int32 name length, name, int32 kind (0 int64, 1 float64), int64 count,
@@ -61,8 +66,11 @@ static void fill(Grid<W, B> &grid)
                     const double r2 = (x[0] - 0.42) * (x[0] - 0.42) + (x[1] - 0.55) * (x[1] - 0.55) +
                                       (x[2] - 0.5) * (x[2] - 0.5);
                     const double pw = 0.5 + 0.45 * sin(2 * pi * x[0]) * cos(2 * pi * x[2]);
-                    block(ix, iy, iz).p_w = (Real)q10(pw);
-                    block(ix, iy, iz).p_g = (Real)q10(0.95 - pw);
+                    const double c2 = (x[0] - 0.62) * (x[0] - 0.62) + (x[1] - 0.5) * (x[1] - 0.5) +
+                                      (x[2] - 0.45) * (x[2] - 0.45);
+                    const bool csf = c2 < 0.09 * 0.09; /* a ventricle: no tissue, no flux */
+                    block(ix, iy, iz).p_w = csf ? (Real)0 : (Real)q10(pw);
+                    block(ix, iy, iz).p_g = csf ? (Real)0 : (Real)q10(0.95 - pw);
                     block(ix, iy, iz).phi = (Real)q10(exp(-r2 / (2 * 0.07 * 0.07)));
                     block(ix, iy, iz).dphidt = 0;
                 }
@@ -92,6 +100,10 @@ static void put_d(FILE *f, const char *name, const std::vector<double> &v)
 }
 
 typedef B::ElementType Cell;
+
+struct get_dphidt {
+    Real operator()(const Cell &c) const { return c.dphidt; }
+};
 
 static void put_fields(FILE *f, const std::string &prefix, Grid<W, B> &grid, const std::vector<BlockInfo> &blocks)
 {
@@ -150,6 +162,26 @@ int main(int argc, char **argv)
     put_d(f, "w1", t.w1);
     put_d(f, "w2", t.w2);
     put_fields(f, "", grid, vInfo);
+
+    /* one ReactionDiffusionOperator sweep (Glioma_ReactionDiffusion.cpp:176-183):
+     * dphidt of every leaf, with its spacing and the coefficients */
+    {
+        const Real L = (Real)25.6;
+        const Real Dw = (Real)((Real)0.2 / (L * L)), Dg = (Real)(0.1 * Dw), rho = (Real)0.05;
+        ReactionDiffusionOperator<_DIM> rhs(Dw, Dg, rho);
+        BlockProcessing bp;
+        bp.pipeline_process(vInfo, grid.getBlockCollection(), grid.getBoundaryInfo(), rhs);
+        std::vector<Real> a;
+        gbfk_mrag::gather_into(a, grid.getBlockCollection(), vInfo, get_dphidt());
+        put_d(f, "rhs", std::vector<double>(a.begin(), a.end()));
+        std::vector<double> h(nb), coeffs(3);
+        for (size_t i = 0; i < nb; i++) h[i] = (double)vInfo[i].h[0];
+        coeffs[0] = (double)Dw;
+        coeffs[1] = (double)Dg;
+        coeffs[2] = (double)rho;
+        put_d(f, "h", h);
+        put_d(f, "coeffs", coeffs);
+    }
 
     std::vector<FWTReport<1> > rep =
         BlockFWT<W, B, RD_Projector_Wavelets>::multichannel_fwt<0, 0>(vInfo, grid.getBlockCollection(),

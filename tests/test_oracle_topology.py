@@ -1,10 +1,13 @@
-"""The oracle's grid-adaptation functions pinned to the reference: per-block
+"""The oracle's adaptive-grid functions pinned to the reference: the RD
+right-hand side through the ghost lists (fill_ghosts + rd_rhs_pool), per-block
 wavelet details (fwt_detail_pool), block split (split_block) and collapse
-(collapse_blocks) on an adapted grid with coarse-fine ghosts, bit for bit
-against the reference's own BlockFWT, Grid::refine and Grid::compress
+(collapse_blocks) on an adapted grid with coarse-fine ghosts and a ball of CSF,
+bit for bit against the reference's own ReactionDiffusionOperator sweep,
+BlockFWT, Grid::refine and Grid::compress
 (oracle/topo_harness.cpp): from the committed fixtures
 (tests/golden/make_golden_topology.py) and, where the harness is built, live
 on a larger grid for all three fields.  CPU only."""
+import hashlib
 from pathlib import Path
 
 import numpy as np
@@ -19,6 +22,13 @@ REALS = {"f64": np.float64, "f32": np.float32}
 def _csr(row_ptr, src, w0, w1, w2):
     return {"row_ptr": np.ascontiguousarray(row_ptr, dtype=np.int64), "src": np.ascontiguousarray(src, dtype=np.int64),
             "w0": np.ascontiguousarray(w0), "w1": np.ascontiguousarray(w1), "w2": np.ascontiguousarray(w2)}
+
+
+def _rhs(csr, fields, h, coeffs, R):
+    pw, pg, phi = (fields[k].astype(R) for k in ("p_w", "p_g", "phi"))
+    ghosts = [O.fill_ghosts(csr, a) for a in (pw, pg, phi)]
+    assert np.any(pw + pg == 0)                      # no-flux cells present
+    return O.rd_rhs_pool(h.astype(R), pw, pg, phi, *ghosts, *(R(c) for c in coeffs))
 
 
 def _check(csr, fields, detail, parents, kids, collapsed, parent_fields, R):
@@ -51,6 +61,10 @@ def test_topology_functions_match_the_reference_fixture(prec):
     # the grid has two levels, and some ghosts are interpolated across them
     assert len(set(g["level"].tolist())) == 2 and row_ptr[-1] > row_ptr.size - 1
     assert g["split_parent"].size == 8 and g["collapse_parent"].size > 0
+    R = REALS[prec]
+    rhs = _rhs(csr, {k: g[k] for k in ("p_w", "p_g", "phi")}, g["h"], g["coeffs"], R)
+    assert np.array_equal(rhs.astype(np.float64)[::997], g["rhs_sample"])
+    assert hashlib.sha256(rhs.tobytes()).digest() == g["rhs_sha256"].tobytes()
     _check(csr, {"phi": g["phi"]}, g["detail"], g["split_parent"], {"phi": g["split_phi"]}, g["collapse_parent"],
            {"phi": g["collapse_phi"]}, REALS[prec])
 
@@ -62,6 +76,9 @@ def test_topology_functions_match_the_reference_live(prec):
     d = O.ref_topology(2, 5, 2e-2, 5, precision=prec)
     assert len(set(d["level"].tolist())) >= 3 and d["summary"]["split"] > 8
     names = ("p_w", "p_g", "phi")
-    _check(_csr(d["row_ptr"], d["src"], d["w0"], d["w1"], d["w2"]), {n: d[n] for n in names}, d["detail"],
+    csr = _csr(d["row_ptr"], d["src"], d["w0"], d["w1"], d["w2"])
+    rhs = _rhs(csr, d, d["h"], d["coeffs"], REALS[prec])
+    assert np.array_equal(rhs, d["rhs"].astype(REALS[prec])) and np.abs(rhs).max() > 0
+    _check(csr, {n: d[n] for n in names}, d["detail"],
            d["split_parent"], {n: d["split_" + n] for n in names}, d["collapse_parent"],
            {n: d["collapse_" + n] for n in names}, REALS[prec])
