@@ -373,3 +373,35 @@ def ref_topology(base_bpd, maxlevel, refine_tol, every, precision="f64"):
         res = read_topology_dump(out)
     res["summary"] = json.loads(r.stdout.strip().splitlines()[-1])
     return res
+
+
+def read_matrix3d(path) -> np.ndarray:
+    """A Matrix .dat of doubles as written by MatrixD3D::dump (the layout of
+    write_matrix3d): shape (nz, ny, nx)."""
+    raw = Path(path).read_bytes()
+    head = np.frombuffer(raw[:24], dtype=np.int32)
+    if head[0] != 1234 or head[1] != 3 or head[5] != 0:
+        raise ValueError(f"{path}: not a 3-D Matrix of doubles")
+    nx, ny, nz = (int(v) for v in head[2:5])
+    return np.frombuffer(raw[24:], dtype=np.float64, count=nx * ny * nz).reshape(nz, ny, nx).copy()
+
+
+def ref_uq_available(precision: str = "f64") -> bool:
+    return (REF_DIR / f"uq_harness_{precision}").exists()
+
+
+def ref_uq_dump(prefix, tumor_ic, refine_tol, compress_tol, precision="f64", sigma=0.0):
+    """The reference's _dumpUQoutput of its own grid after _ic on
+    {prefix}GM.dat, WM.dat, CSF.dat (phi replaced by a Gaussian of width
+    sigma at the tumour centre when sigma > 0) and one AutomaticRefinement
+    and AutomaticCompression (oracle/_ref/uq_harness_*).  Returns the leaves
+    (level, index, h, phi in block order), the dump as (gpd, gpd, gpd) and
+    the JSON summary."""
+    with tempfile.TemporaryDirectory() as td:
+        r = subprocess.run([str(REF_DIR / f"uq_harness_{precision}"), os.fspath(prefix),
+                            *(_fmt(v) for v in tumor_ic), _fmt(refine_tol), _fmt(compress_tol), td, _fmt(sigma)],
+                           check=True, capture_output=True, text=True, env=dict(os.environ, GBFK_ORACLE_THREADS="1"))
+        res = read_topology_dump(os.path.join(td, "leaves.bin"))
+        res["dump"] = read_matrix3d(os.path.join(td, "HGG_data.dat"))
+    res["summary"] = json.loads(r.stdout.strip().splitlines()[-1])
+    return res
