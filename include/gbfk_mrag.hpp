@@ -38,13 +38,15 @@ template <typename R> struct precision_of;
 template <> struct precision_of<double> { static const int value = GBFK_F64; };
 template <> struct precision_of<float> { static const int value = GBFK_F32; };
 
-/* Host threads for the per-block loops below: GBFK_HOST_THREADS if set, else
- * the online processors; 1 to 64.  (The adapter is compiled as C++98 with the
- * reference's sources, hence pthreads.) */
+/* Host threads for the per-block loops below: GBFK_HOST_THREADS if set (1 to
+ * 64), else the online processors up to 16 (the loops are memory-bound copies
+ * and run once per step in the drop-in policy, where thread start-up counts).
+ * (The adapter is compiled as C++98 with the reference's sources, hence
+ * pthreads.) */
 inline int host_threads()
 {
     const char *e = getenv("GBFK_HOST_THREADS");
-    long n = e && *e ? atol(e) : sysconf(_SC_NPROCESSORS_ONLN);
+    const long n = e && *e ? atol(e) : std::min(sysconf(_SC_NPROCESSORS_ONLN), 16L);
     return (int)std::max(1L, std::min(n, 64L));
 }
 
