@@ -4,8 +4,6 @@ import ctypes
 import re
 from pathlib import Path
 
-import pytest
-
 from gliomasolver_b200 import _lib
 from gliomasolver_b200.build import build_library
 

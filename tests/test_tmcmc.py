@@ -57,7 +57,7 @@ def test_glioma_model_calibration_runs_on_the_batch(gbfk_lib):
     the population's forward solves and likelihoods in batches; the
     ground truth scores higher than a far-off parameter set, and the
     posterior concentrates around the truth's Dw*T and rho*T."""
-    from gliomasolver_b200.anatomy import make_anatomy, tumor_ic
+    from gliomasolver_b200.anatomy import make_anatomy
     from gliomasolver_b200.tmcmc import GliomaModel
 
     n = 32
