@@ -1,7 +1,7 @@
-"""The reference arm of bench.py (`--impl reference`) on the CPU, alone and under
-torchrun with two ranks: one JSON
-line with the metric, unit and config of the GPU arm, `impl`, a
-`cpu_baseline` that describes the run and an `e2e` without copies."""
+"""The reference arm of bench.py (`--impl reference`) on the CPU, alone and
+under torchrun with two ranks: one JSON line with the metric, unit and config
+of the GPU arm, `impl`, a `cpu_baseline` that describes the run and an `e2e`
+without copies."""
 import json
 import subprocess
 import sys
