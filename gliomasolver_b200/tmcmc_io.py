@@ -229,8 +229,11 @@ def write_reference_outputs(result: TMCMCResult, directory, par: TMCMCPar = None
     """Write curgen_db_000.txt .. curgen_db_<Gen>.txt, runinfo.txt and
     fitness.txt into ``directory`` (created if missing); with ``posterior``
     and a run that reached exponent 1, also posterior.txt and
-    statistics.txt as extractInferenceOutput.sh makes them."""
-    par = par if par is not None else TMCMCPar(max_stages=max(len(result.stages), 20))
+    statistics.txt as extractInferenceOutput.sh makes them.  Without ``par``
+    the run record has max(generations, 20) entries and the population size
+    is the first generation's."""
+    if par is None:
+        par = TMCMCPar(max_stages=max(len(result.stages), 20), pop_size=len(result.stages[0][1]))
     os.makedirs(directory, exist_ok=True)
     for g, (theta, F) in enumerate(result.stages):
         with open(os.path.join(directory, "curgen_db_%03d.txt" % g), "w") as f:

@@ -193,3 +193,10 @@ def test_write_reference_outputs(tmp_path, run):
     assert len(last.splitlines()[0].split()) - 1 == 3
     assert (tmp_path / "out" / "fitness.txt").read_text() == "%f\n" % run.log_evidence
     assert (tmp_path / "out" / "runinfo.txt").read_text() == runinfo_text(run, 30, 200)
+
+
+def test_write_reference_outputs_without_a_parameter_file(tmp_path, run):
+    write_reference_outputs(run, tmp_path, posterior=False)
+    gen = len(run.stages) - 1
+    assert (tmp_path / "runinfo.txt").read_text() == runinfo_text(run, max(gen + 1, 20), 200)
+    assert not (tmp_path / "posterior.txt").exists()
