@@ -132,6 +132,16 @@ def read_tumor_ic(path="TumorIC.txt") -> tuple:
     return tuple(float(v) for v in vals[:3])
 
 
+def read_input_parameters(path="InputParameters.txt") -> tuple:
+    """Dw [cm^2/day], rho [1/day] and Tend [day] of a UQ forward run: three
+    numbers (Glioma_ReactionDiffusion.cpp:280-293), for make_schedule."""
+    with open(path) as f:
+        vals = f.read().split()
+    if len(vals) < 3:
+        raise ValueError(f"{path}: expected three numbers")
+    return tuple(float(v) for v in vals[:3])
+
+
 @dataclass
 class Observations:
     """Inputs of the likelihood step, ready for ``set_observations`` and

@@ -201,6 +201,11 @@ def test_load_observations(tmp_path):
     assert obs.params == {"pet_sigma2": 0.000361, "pet_scale": 0.85, "t1_uc": 0.7, "t2_uc": 0.25, "slope": 2.0}
     assert obs.likelihood_kwargs(2, 3)["step_mri"] == 3
     assert patient.read_tumor_ic(tmp_path / "TumorIC.txt") == (0.28, 0.67, 0.35)
+    (tmp_path / "InputParameters.txt").write_text("0.13\n0.025\n150\n")
+    assert patient.read_input_parameters(tmp_path / "InputParameters.txt") == (0.13, 0.025, 150.0)
+    (tmp_path / "short.txt").write_text("0.13 0.025\n")
+    with pytest.raises(ValueError):
+        patient.read_input_parameters(tmp_path / "short.txt")
     obs2 = patient.load_observations(tmp_path, pet=False)
     assert obs2.pet is None and obs2.roi is None
     with pytest.raises(GbfkError):
