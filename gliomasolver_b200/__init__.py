@@ -6,11 +6,14 @@ reference-shaped operator interface (``ReactionDiffusionOperator``,
 ``UpdateTumor``, ``BlockProcessing``), the time-step schedule of the
 reference's driver, the seeded synthetic anatomy, the patient data of the
 reference (``patient``: Matrix files, anatomy and tumour mapping,
-likelihood inputs), batched TMCMC stages and the TMCMC driver (``tmcmc``),
-the adjoint as a ``torch.autograd.Function`` (``autograd``) and the sharding
-of a stage over ranks (``shard``).
+likelihood inputs), batched TMCMC stages and the TMCMC driver (``tmcmc``)
+with the reference's TMCMC files (``tmcmc_io``), host snapshots of a pool so
+that a long run can resume (``snapshot``), the adjoint as a
+``torch.autograd.Function`` (``autograd``) and the sharding of a stage over
+ranks (``shard``).
 """
 from . import patient  # noqa: F401
+from . import snapshot  # noqa: F401
 from .schedule import Schedule, make_schedule  # noqa: F401
 from ._lib import GbfkError  # noqa: F401
 from .solver import (  # noqa: F401
