@@ -81,7 +81,7 @@ def test_glioma_model_calibration_runs_on_the_batch(gbfk_lib):
         lower, upper = truth.copy(), truth.copy()
         lower[:2] -= 1.0
         upper[:2] += 1.0
-        res = tmcmc(model, lower, upper, TMCMCOptions(pop_size=128, max_stages=6, seed=2))
+        res = tmcmc(model, lower, upper, TMCMCOptions(pop_size=128, max_stages=7, seed=2))
         assert len(res.p) >= 2 and np.all(np.isfinite(res.loglik))
         best = res.theta[np.argmax(res.loglik)]
         assert abs(best[1] - truth[1]) < 0.5
