@@ -227,7 +227,15 @@ class TMCMCResult:
     log_selection: list = field(default_factory=list)
     mean_theta: list = field(default_factory=list)
     ss: np.ndarray = None                                # of the last generation
-    p_next: float = 1.0                                  # exponent after the last generation
+    p_next: float = None                                 # exponent after the last generation (set at the end)
+
+
+@dataclass
+class TMCMCCheckpoint:
+    """A run stopped after generation G = len(result.stages) - 1, with the
+    random generator's state at that point (``tmcmc(..., start=...)``)."""
+    result: TMCMCResult
+    rng_state: dict
 
 
 def _cov_of_weights(F, dp):
@@ -273,10 +281,20 @@ def _posdef(S):
     return (V * np.maximum(w, floor)) @ V.T
 
 
-def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions()):
+def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions(), on_generation=None, start=None):
     """Sample the posterior of a uniform prior on the box [lower, upper]
     times exp(loglik).  ``loglik(theta)`` takes an (n, d) array and returns n
-    log-likelihoods (NaN/inf count as ``opts.penalty``)."""
+    log-likelihoods (NaN/inf count as ``opts.penalty``).
+
+    ``on_generation(result, rng_state)`` is called once per generation, after
+    its statistics are recorded (``result.stages[-1]`` is its population,
+    ``result.p[-1]`` its exponent; ``result.p_next`` is None until the last
+    one), with the random generator's state at that point, which is the start
+    of the generation's transition (``tmcmc_io.Checkpointer`` writes the
+    reference's files and the exact state there).  ``start``: a
+    ``TMCMCCheckpoint`` (``tmcmc_io.load_checkpoint``); the run continues
+    from its last generation and, with the same likelihood and options,
+    equals the uninterrupted run."""
     rng = np.random.default_rng(opts.seed)
     lower = np.asarray(lower, dtype=np.float64)
     upper = np.asarray(upper, dtype=np.float64)
@@ -289,12 +307,26 @@ def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions()):
         F = np.asarray(loglik(th), dtype=np.float64)
         return np.where(np.isfinite(F), F, opts.penalty)
 
-    theta = lower + (upper - lower) * rng.random((opts.pop_size, d))
-    F = evaluate(theta)
-    p = [0.0]
     log_ev = 0.0
-    acc = []
-    rec = TMCMCResult(None, None, p, 0.0, acc, 0)
+    if start is None:
+        theta = lower + (upper - lower) * rng.random((opts.pop_size, d))
+        F = evaluate(theta)
+        p = [0.0]
+        acc = []
+        rec = TMCMCResult(None, None, p, 0.0, acc, 0)
+    else:
+        # generations 0..G-1 as recorded; G's statistics are recomputed below
+        old = start.result
+        g = len(old.stages) - 1
+        theta, F = (a.copy() for a in old.stages[g])
+        p, acc = list(old.p[:g + 1]), list(old.acceptance[:g])
+        rec = TMCMCResult(None, None, p, 0.0, acc, 0, stages=list(old.stages[:g]), uniques=list(old.uniques[:g]),
+                          coef_var=list(old.coef_var[:g]), log_selection=list(old.log_selection[:g]),
+                          mean_theta=list(old.mean_theta[:g]))
+        for v in rec.log_selection:
+            log_ev += v
+        nevals = old.evaluations
+        rng.bit_generator.state = start.rng_state
 
     def record(theta, F, q, log_sel, mean, ss):
         rec.stages.append((theta.copy(), F.copy()))
@@ -303,8 +335,12 @@ def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions()):
         rec.log_selection.append(float(log_sel))
         rec.mean_theta.append(mean)
         rec.ss = _posdef(ss)
+        rec.theta, rec.loglik, rec.log_evidence, rec.evaluations = theta, F, float(log_ev), nevals
+        if on_generation is not None:
+            on_generation(rec, rng.bit_generator.state)
 
-    for _ in range(opts.max_stages - 1):
+    done = p[-1] >= 1.0
+    for _ in range(0 if done else opts.max_stages - len(p)):
         pj = p[-1]
         pn = next_exponent(F, pj, opts.tol_cov)
         flcp = F * (pn - pj)
@@ -312,12 +348,15 @@ def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions()):
         log_sel = np.log(w.sum()) + flcp.max() - np.log(len(F))
         log_ev += log_sel
         q = w / w.sum()
-        sel = rng.multinomial(opts.pop_size, q)
         mean = q @ theta
         dev = theta - mean
         ss = (dev.T * q) @ dev
-        cov = _posdef(opts.bbeta * ss)
         record(theta, F, q, log_sel, mean, ss)
+        sel = rng.multinomial(opts.pop_size, q)
+        # the proposal covariance bbeta * SS, bbeta applied to the weighted
+        # deviations before the product (this operand order fixes the run's
+        # rounding, and with it every later generation)
+        cov = _posdef((opts.bbeta * (dev.T * q)) @ dev)
         # leaders with chain lengths (split at max_chain, raised to min_chain)
         chains = []
         for i in np.flatnonzero(sel):
@@ -368,7 +407,9 @@ def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions()):
     q = w / w.sum()
     mean = q @ theta
     dev = theta - mean
-    record(theta, F, q, np.log(w.sum()) + flcp.max() - np.log(len(F)), mean, (dev.T * q) @ dev)
+    log_sel = np.log(w.sum()) + flcp.max() - np.log(len(F))
+    log_ev += log_sel
+    record(theta, F, q, log_sel, mean, (dev.T * q) @ dev)
     rec.theta, rec.loglik, rec.log_evidence, rec.evaluations = theta, F, float(log_ev), nevals
     return rec
 

@@ -19,6 +19,7 @@ This is host-side file handling only (no device work).
 """
 from __future__ import annotations
 
+import json
 import math
 import os
 import re
@@ -26,7 +27,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .tmcmc import TMCMCOptions, TMCMCResult
+from .tmcmc import TMCMCCheckpoint, TMCMCOptions, TMCMCResult
 
 _INT = re.compile(r"[+-]?\d+")
 _FLOAT = re.compile(r"[+-]?(?:\d+\.?\d*|\.\d+)(?:[eE][+-]?\d+)?")
@@ -140,8 +141,9 @@ def runinfo_text(result: TMCMCResult, max_stages: int, pop_size: int = None) -> 
     """``runinfo.txt`` after the last generation, as save_runinfo writes it
     at the end of a run: arrays of length max_stages (zero past the run);
     p[Gen + 1], where it fits, is the exponent after the last generation (1
-    once the run reached it); CoefVar[Gen + 1] is the COV objective at its
-    optimum (0);
+    once the run reached it; 0 while the run goes on, as in the record the
+    reference saves during a run); CoefVar[Gen + 1] is the COV objective at
+    its optimum (0);
     acceptance[g] = distinct points of generation g / population size
     (engine_tmcmc.c:834-835)."""
     gen = len(result.stages) - 1
@@ -159,7 +161,7 @@ def runinfo_text(result: TMCMCResult, max_stages: int, pop_size: int = None) -> 
     mean = np.zeros((max_stages, d))
     coef[:gen + 1] = result.coef_var
     p[:gen + 1] = result.p[:gen + 1]
-    if gen + 1 < max_stages:
+    if gen + 1 < max_stages and result.p_next is not None:
         p[gen + 1] = result.p_next
     un[:gen + 1] = result.uniques
     logsel[:gen + 1] = result.log_selection
@@ -251,3 +253,72 @@ def write_reference_outputs(result: TMCMCResult, directory, par: TMCMCPar = None
             f.write("".join(" ".join(r) + "\n" for r in rows))
         with open(os.path.join(directory, "statistics.txt"), "w") as f:
             f.write(statistics_text(rows))
+
+
+def _atomic_write(path, write):
+    tmp = f"{path}.tmp{os.getpid()}"
+    try:
+        with open(tmp, "wb") as f:
+            write(f)
+        os.replace(tmp, path)
+    finally:
+        if os.path.exists(tmp):
+            os.remove(tmp)
+
+
+STATE_FILE = "tmcmc_state.npz"
+
+
+class Checkpointer:
+    """An ``on_generation`` hook for :func:`~gliomasolver_b200.tmcmc.tmcmc`
+    that writes, after every generation, what the reference writes during a
+    run (curgen_db_<g>.txt, runinfo.txt; engine_tmcmc.c:1176-1184) and
+    tmcmc_state.npz: every generation's population and statistics in binary
+    and the random generator's state, from which ``load_checkpoint`` resumes
+    the run exactly.  After the last generation it also writes fitness.txt
+    (and, with ``posterior``, posterior.txt and statistics.txt)."""
+
+    def __init__(self, directory, par: TMCMCPar = None, posterior: bool = True):
+        self.directory = os.fspath(directory)
+        self.par = par
+        self.posterior = posterior
+        os.makedirs(self.directory, exist_ok=True)
+
+    def __call__(self, result: TMCMCResult, rng_state: dict):
+        g = len(result.stages) - 1
+        par = self.par if self.par is not None else TMCMCPar(max_stages=max(g + 1, 20),
+                                                              pop_size=len(result.stages[0][1]))
+        with open(os.path.join(self.directory, "curgen_db_%03d.txt" % g), "w") as f:
+            f.write(curgen_db_text(*result.stages[g]))
+        text = runinfo_text(result, par.max_stages, par.pop_size)
+        _atomic_write(os.path.join(self.directory, "runinfo.txt"), lambda f: f.write(text.encode()))
+        arrays = {"p": np.asarray(result.p, dtype=np.float64),
+                  "acceptance": np.asarray(result.acceptance, dtype=np.float64),
+                  "uniques": np.asarray(result.uniques, dtype=np.int64),
+                  "coef_var": np.asarray(result.coef_var, dtype=np.float64),
+                  "log_selection": np.asarray(result.log_selection, dtype=np.float64),
+                  "mean_theta": np.asarray(result.mean_theta, dtype=np.float64),
+                  "ss": np.asarray(result.ss, dtype=np.float64),
+                  "evaluations": np.int64(result.evaluations),
+                  "rng_state": np.frombuffer(json.dumps(rng_state).encode(), dtype=np.uint8)}
+        for k, (theta, F) in enumerate(result.stages):
+            arrays["theta_%03d" % k] = theta
+            arrays["F_%03d" % k] = F
+        _atomic_write(os.path.join(self.directory, STATE_FILE), lambda f: np.savez(f, **arrays))
+        if result.p_next is not None:
+            write_reference_outputs(result, self.directory, par, self.posterior)
+
+
+def load_checkpoint(directory) -> TMCMCCheckpoint:
+    """The state a :class:`Checkpointer` left in ``directory``: pass it as
+    ``tmcmc(..., start=...)`` with the same likelihood and options."""
+    with np.load(os.path.join(os.fspath(directory), STATE_FILE)) as z:
+        n = int(z["p"].size)
+        stages = [(z["theta_%03d" % k].copy(), z["F_%03d" % k].copy()) for k in range(n)]
+        res = TMCMCResult(stages[-1][0], stages[-1][1], [float(v) for v in z["p"]], 0.0,
+                          [float(v) for v in z["acceptance"]], int(z["evaluations"]), stages=stages,
+                          uniques=[int(v) for v in z["uniques"]], coef_var=[float(v) for v in z["coef_var"]],
+                          log_selection=[float(v) for v in z["log_selection"]],
+                          mean_theta=[row.copy() for row in z["mean_theta"]], ss=z["ss"].copy())
+        rng_state = json.loads(bytes(z["rng_state"]).decode())
+    return TMCMCCheckpoint(res, rng_state)

@@ -9,8 +9,8 @@ import numpy as np
 import pytest
 
 from gliomasolver_b200.tmcmc import TMCMCOptions, tmcmc
-from gliomasolver_b200.tmcmc_io import (curgen_db_text, parse_par, posterior_rows, runinfo_text, statistics_text,
-                                        write_reference_outputs)
+from gliomasolver_b200.tmcmc_io import (Checkpointer, curgen_db_text, load_checkpoint, parse_par, posterior_rows,
+                                        runinfo_text, statistics_text, write_reference_outputs)
 
 # A parameter file in the reference's syntax: tabs and spaces, comment lines,
 # an inline comment, a commented-out key, B1 before B10, a parameter (B3)
@@ -200,3 +200,42 @@ def test_write_reference_outputs_without_a_parameter_file(tmp_path, run):
     gen = len(run.stages) - 1
     assert (tmp_path / "runinfo.txt").read_text() == runinfo_text(run, max(gen + 1, 20), 200)
     assert not (tmp_path / "posterior.txt").exists()
+
+
+class _Stop(Exception):
+    pass
+
+
+def test_a_resumed_run_equals_the_uninterrupted_run(tmp_path):
+    lower, upper = [-1.0, -1.0, -1.0], [1.0, 1.0, 1.0]
+    opts = TMCMCOptions(pop_size=150, seed=5)
+    full = tmcmc(_gauss, lower, upper, opts, on_generation=Checkpointer(tmp_path / "a"))
+    assert len(full.stages) > 3 and full.p[-1] == 1.0
+    ck = Checkpointer(tmp_path / "b")
+
+    def stop_after_generation_2(rec, rng_state):
+        ck(rec, rng_state)
+        if len(rec.stages) == 3:
+            raise _Stop
+
+    with pytest.raises(_Stop):
+        tmcmc(_gauss, lower, upper, opts, on_generation=stop_after_generation_2)
+    mid = load_checkpoint(tmp_path / "b")
+    assert len(mid.result.stages) == 3 and len(mid.result.p) == 3
+    assert "p[20]=" in (tmp_path / "b" / "runinfo.txt").read_text() and not (tmp_path / "b" / "fitness.txt").exists()
+    resumed = tmcmc(_gauss, lower, upper, opts, on_generation=Checkpointer(tmp_path / "b"), start=mid)
+    assert np.array_equal(resumed.theta, full.theta) and np.array_equal(resumed.loglik, full.loglik)
+    assert resumed.p == full.p and resumed.p_next == full.p_next
+    assert resumed.log_evidence == full.log_evidence and resumed.evaluations == full.evaluations
+    assert resumed.acceptance == full.acceptance and resumed.uniques == full.uniques
+    assert resumed.log_selection == full.log_selection and resumed.coef_var == full.coef_var
+    assert np.array_equal(resumed.ss, full.ss)
+    files = sorted(q.name for q in (tmp_path / "a").iterdir())
+    assert files == sorted(q.name for q in (tmp_path / "b").iterdir())
+    for name in files:
+        if name != "tmcmc_state.npz":
+            assert (tmp_path / "a" / name).read_bytes() == (tmp_path / "b" / name).read_bytes(), name
+    # resuming a finished run evaluates nothing more and gives the same result
+    again = tmcmc(_gauss, lower, upper, opts, start=load_checkpoint(tmp_path / "a"))
+    assert again.evaluations == full.evaluations and np.array_equal(again.theta, full.theta)
+    assert again.log_evidence == full.log_evidence and again.p == full.p
