@@ -264,35 +264,40 @@ def batched_stage(args, stream, local, nsamples=512, bpd=16, seed=1):
 def adjoint_sample(stream, local, bpd=16, nsnap=64):
     """Config 4: forward + discrete adjoint at 128^3, FP32 state, FP64 loss and
     gradient sums, 64 checkpoint buffers, about 10^4 steps (Dw = 0.2, T = 300 d);
-    observations from a seeded ground-truth run (rho = 0.012) thresholded at
-    0.7 / 0.25 with 2% label noise; gradients taken at Dw = 0.18, rho = 0.014.
+    observations from a seeded FP64 ground-truth run (rho = 0.012) thresholded
+    at 0.7 / 0.25 with 2% label noise; gradients taken at Dw = 0.18, rho = 0.014.
     rho*T ~ 4 keeps a tumour front: with rho*T >> 1 the tumour saturates the
     brain (every cell exactly 0 or 1), the loss is locally constant and all
-    gradients are 0.  Timed against one plain forward solve of the same steps."""
+    gradients are 0.  Timed against one plain forward solve of the same steps.
+    Untimed checks: the same problem with FP64 state against central
+    differences of FP64 forward solves (relative step 1e-4 for Dw and rho,
+    1e-7 for x0), and the FP32 gradients against the FP64 ones."""
     import torch
 
     from gliomasolver_b200 import BlockPool
     from gliomasolver_b200.anatomy import make_anatomy, pick_origin, tumor_ic
+    from gliomasolver_b200.gradcheck import check_gradients, synthetic_observations
 
     n = 8 * bpd
     p_w, p_g, _ = make_anatomy(n, SEED)
     s = make_schedule(0.2, 0.012, 300.0, L_CM, bpd, "f32")
+    s64 = make_schedule(0.2, 0.012, 300.0, L_CM, bpd, "f64")
     x_gt = pick_origin(p_w, SEED)[0]
+    x0 = [float(min(1.0, v + 2.0 / n)) for v in x_gt]
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    with BlockPool(bpd ** 3, "f64", device=local, stream=stream.cuda_stream) as pool64:
+        pool64.set_uniform(bpd)
+        pool64.upload_dense("p_w", p_w)
+        pool64.upload_dense("p_g", p_g)
+        masks = synthetic_observations(pool64, tumor_ic(n, x_gt, p_w, p_g), s64.Dw, s64.rho, s64.dt, s64.nsteps,
+                                       seed=SEED + 17)
+        Dw64 = float(np.float64(0.18) / np.float64(L_CM * L_CM))
+        chk = check_gradients(pool64, p_w, p_g, Dw64, 0.014, s.dt, s.nsteps, x0, 2.0 / n, nsnapshots=nsnap)
     with BlockPool(bpd ** 3, "f32", device=local, stream=stream.cuda_stream) as pool:
         pool.set_uniform(bpd)
         pool.upload_dense("p_w", p_w.astype(np.float32))
         pool.upload_dense("p_g", p_g.astype(np.float32))
-        pool.upload_dense("phi", tumor_ic(n, x_gt, p_w, p_g).astype(np.float32))
-        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, s.nsteps)
-        u = pool.download_dense("phi").astype(np.float64)
-        rng = np.random.default_rng(SEED + 17)
-        masks = [(u > 0.7).astype(float), (u > 0.25).astype(float)]
-        for m in masks:
-            flip = rng.random(m.shape) < 0.02
-            m[flip] = 1 - m[flip]
         pool.set_observations(*masks)
-        x0 = np.clip(np.array(x_gt) + 2.0 / n, 0, 1)
         Dw = float(np.float32(np.float32(0.18) / np.float32(L_CM * L_CM)))
         Dg = float(np.float32(0.1 * Dw))
         # warm-up (face coefficients, first allocations)
@@ -312,6 +317,10 @@ def adjoint_sample(stream, local, bpd=16, nsnap=64):
         e1.record(stream)
         torch.cuda.synchronize()
         t_fwd = e0.elapsed_time(e1) / 1e3
+    a64 = chk["adjoint"]
+    rel32 = {k: abs(res[k] - a64[k]) / max(abs(a64[k]), 1e-300) for k in ("dDw", "drho")}
+    rel32["loss"] = abs(res["loss"] - chk["loss"]) / abs(chk["loss"])
+    rel32["dx0"] = float(np.linalg.norm(np.array(res["dx0"]) - np.array(a64["dx0"])) / np.linalg.norm(a64["dx0"]))
     return {
         "workload": f"forward + discrete adjoint, {n}^3 uniform, FP32 state, FP64 loss/gradient sums, "
                     f"{nsnap} checkpoint buffers, {s.nsteps} steps",
@@ -320,6 +329,13 @@ def adjoint_sample(stream, local, bpd=16, nsnap=64):
         "plain_forward_s": t_fwd, "plain_forward_samples_per_s": 1.0 / t_fwd,
         "gradient_cost_in_forward_solves": t_adj / t_fwd,
         "loss": res["loss"], "dDw": res["dDw"], "drho": res["drho"], "dx0": list(res["dx0"]),
+        "fp64_check": {"what": "FP64 state, same problem: adjoint vs central differences of FP64 forward solves "
+                               "(relative step 1e-4 for Dw, rho; 1e-7 for x0); crossings = voxels that cross a "
+                               "likelihood threshold between the two runs of a quotient",
+                       "adjoint": a64, "fd": chk["fd"], "rel_err": chk["rel_err"], "crossings": chk["crossings"],
+                       "fd_resolution": chk["fd_resolution"], "chain_rule_rel_err": chk["chain_rule_rel_err"],
+                       "forward_steps_run": chk["forward_steps"]},
+        "fp32_vs_fp64_rel": rel32,
     }
 
 
@@ -436,6 +452,48 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9):
                      "algorithmic_bytes": "9 words (forward 4 + adjoint 5) x cells x steps; recomputation not counted"},
         "fp32_vs_fp64_rel": rel, "per_sample": recs,
     }
+
+
+def adaptive_forward(steps, precision="f32"):
+    """Config 2 on the resident drop-in (dropin/_build/glioma_adaptive_*): the
+    reference's MRAG grid as the block tree, the leaves on the GPU for the
+    whole run; level 2 to 5 (256^3-equivalent), Dw = 0.2 cm^2/day,
+    rho = 0.05/day, re-adapting every 20 steps (one refinement loop at 1e-3,
+    compression to convergence at 1e-4), ``steps`` steps of the T = 300 d
+    schedule (36364 in all).  Host wall clock around synchronous calls."""
+    import tempfile
+
+    exe = ROOT / "dropin" / "_build" / f"glioma_adaptive_{precision}"
+    if not exe.exists():
+        return {"unavailable": "dropin/_build is built only where the reference sources are"}
+    n = 256
+    pw, pg, c0, _ = make_case(n, SEED)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(np.int32(n).tobytes())
+            for a in (pw, pg, c0):
+                f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+        t0 = time.perf_counter()
+        r = subprocess.run([str(exe), fin, "5", "1e-3", "1e-4", str(steps), "20", fout], capture_output=True,
+                           text=True, timeout=1800)
+        wall = time.perf_counter() - t0
+    if r.returncode != 0:
+        return {"failed": r.stderr[-500:]}
+    rec = json.loads(r.stdout.strip().splitlines()[-1])
+    cu = rec["cell_updates"]
+    keep = ("step_seconds", "adapt_seconds", "first_upload_seconds", "topology_changes", "uploads", "upload_seconds",
+            "detail_sweeps", "details_seconds", "plan_seconds", "splits", "split_seconds", "collapses",
+            "collapse_seconds", "near_decisions", "min_margin_refine", "min_margin_compress")
+    out = {"workload": f"config 2 adaptive forward, levels 2-5 (256^3-equivalent), {precision.upper()} storage, "
+                       f"re-adapt every 20 steps, first {steps} of the 36364 steps of T = 300 d",
+           "steps": steps, "blocks_min": min(rec["blocks"]), "blocks_max": max(rec["blocks"]),
+           "cell_updates": cu, "stepping_cell_updates_per_s": cu / rec["step_seconds"],
+           "run_cell_updates_per_s": cu / (rec["step_seconds"] + rec["adapt_seconds"]), "process_wall_s": wall}
+    out.update({k: rec[k] for k in keep})
+    out["timing"] = ("host wall clock around synchronous calls; adapt = device details + the reference grid's "
+                     "own plan and tree update (plan_seconds) + device split/collapse + ghost-list upload")
+    return out
 
 
 def gpu_arm(args):
@@ -564,6 +622,9 @@ def gpu_arm(args):
     batch = None
     adj = None
     adj5 = None
+    adaptive = None
+    if args.adaptive_steps > 0 and rank == 0:
+        adaptive = adaptive_forward(args.adaptive_steps, prec)
     if not args.no_batch:
         batch = batched_stage(args, stream, local)
     if not args.no_batch or args.adjoint_sample:
@@ -587,6 +648,7 @@ def gpu_arm(args):
             "parallelism": "replicas" if world > 1 else "single",
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
             "batched_stage": batch, "forward_adjoint": adj, "forward_adjoint_16x256": adj5,
+            "adaptive_forward": adaptive,
         }
         print(json.dumps(line), flush=True)
     pool.close()
@@ -610,6 +672,8 @@ def main():
                     help="run the config-4 gradient sample even with --no-batch")
     ap.add_argument("--adjoint-batch", action="store_true",
                     help="also run config 5 (16 gradient samples at 256^3, a few minutes)")
+    ap.add_argument("--adaptive-steps", type=int, default=400,
+                    help="steps of the config-2 adaptive run on the resident drop-in (0: skip)")
     ap.add_argument("--step-kernel", default="auto", choices=["auto", "block", "pipelined"],
                     help="step kernel of the resident solve (auto: pipelined on uniform power-of-two grids)")
     args = ap.parse_args()

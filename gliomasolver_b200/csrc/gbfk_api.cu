@@ -59,6 +59,11 @@ struct gbfk_ctx {
 
     // static per (topology, p_w, p_g): cell classes; per (.., Dw, Dg): face coefficients
     void *d_origin = nullptr;         // nblocks * 3 Real: BlockInfo::origin
+    bool have_origin = false;
+    // capacity in bytes of each topology buffer (keyed by the member's
+    // address): the buffers are kept across topology changes and grown only
+    // when a topology needs more room
+    std::unordered_map<void *, size_t> topo_cap;
 
     // observations for the likelihood (n^3 grid)
     int obs_n = 0;
@@ -154,17 +159,31 @@ int ensure_table(gbfk_ctx *ctx)
     return GBFK_OK;
 }
 
+// A topology buffer of at least `bytes`: the one already held if it is large
+// enough, else a new one (the old contents are not kept).
+template <typename T>
+int topo_alloc(gbfk_ctx *c, T **p, size_t bytes)
+{
+    void **q = (void **)p;
+    bytes = std::max<size_t>(bytes, 1);
+    auto it = c->topo_cap.find((void *)q);
+    if (*q && it != c->topo_cap.end() && it->second >= bytes) return GBFK_OK;
+    if (*q) cudaFree(*q);
+    *q = nullptr;
+    c->topo_cap.erase((void *)q);
+    const cudaError_t e = cudaMalloc(q, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, GBFK_E_OOM, "topology buffer of %zu bytes: %s", bytes, cudaGetErrorString(e));
+    }
+    c->topo_cap[(void *)q] = bytes;
+    return GBFK_OK;
+}
+
+// Forget the current topology; its buffers stay allocated for the next one.
 void free_topology(gbfk_ctx *c)
 {
-    void **ptrs[] = {(void **)&c->d_slot, (void **)&c->d_nbr, &c->d_h, (void **)&c->d_row_ptr, (void **)&c->d_src,
-                     &c->d_w, (void **)&c->d_step_rows, (void **)&c->d_all_rows, &c->d_gpw, &c->d_gpg,
-                     &c->d_gphi, (void **)&c->d_fwt, &c->d_H, (void **)&c->d_ih2, (void **)&c->d_btype, &c->d_origin,
-                     (void **)&c->d_lists};
-    for (void **p : ptrs) {
-        if (*p) cudaFree(*p);
-        *p = nullptr;
-    }
-    c->have_topology = c->have_csr = c->uniform = false;
+    c->have_topology = c->have_csr = c->uniform = c->have_origin = false;
     c->nblocks = 0;
     c->nrows = c->n_step_rows = 0;
     c->h_slot.clear();
@@ -173,6 +192,21 @@ void free_topology(gbfk_ctx *c)
     c->faces_valid = false;
     c->lists_valid = false;
     c->phi_clamped = false;
+}
+
+// Free the topology buffers (context destruction).
+void release_topology(gbfk_ctx *c)
+{
+    free_topology(c);
+    void **ptrs[] = {(void **)&c->d_slot, (void **)&c->d_nbr, &c->d_h, (void **)&c->d_row_ptr, (void **)&c->d_src,
+                     &c->d_w, (void **)&c->d_step_rows, (void **)&c->d_all_rows, &c->d_gpw, &c->d_gpg,
+                     &c->d_gphi, (void **)&c->d_fwt, &c->d_H, (void **)&c->d_ih2, (void **)&c->d_btype, &c->d_origin,
+                     (void **)&c->d_lists};
+    for (void **p : ptrs) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    c->topo_cap.clear();
 }
 
 // Something the face coefficients or classes depend on changed.
@@ -189,13 +223,17 @@ int upload_origin(gbfk_ctx *ctx, const std::vector<int> &level, const std::vecto
     std::vector<double> o(3 * (size_t)nb);
     for (int i = 0; i < nb; i++)
         for (int d = 0; d < 3; d++) o[3 * i + d] = index[3 * i + d] * ldexp(1.0, -level[i]);
-    CK(cudaMalloc(&ctx->d_origin, 3 * (size_t)nb * ctx->rsize));
+    {
+        const int rc = topo_alloc(ctx, &ctx->d_origin, 3 * (size_t)nb * ctx->rsize);
+        if (rc) return rc;
+    }
     if (ctx->precision == GBFK_F64) {
         CK(cudaMemcpy(ctx->d_origin, o.data(), o.size() * sizeof(double), cudaMemcpyHostToDevice));
     } else {
         std::vector<float> f(o.begin(), o.end());
         CK(cudaMemcpy(ctx->d_origin, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
+    ctx->have_origin = true;
     return GBFK_OK;
 }
 
@@ -207,7 +245,10 @@ int upload_ih2(gbfk_ctx *ctx)
         const double h = ctx->precision == GBFK_F64 ? ctx->h_h[i] : (double)(float)ctx->h_h[i];
         v[i] = 1. / (h * h);
     }
-    CK(cudaMalloc(&ctx->d_ih2, ctx->nblocks * sizeof(double)));
+    {
+        const int rc = topo_alloc(ctx, &ctx->d_ih2, ctx->nblocks * sizeof(double));
+        if (rc) return rc;
+    }
     CK(cudaMemcpy(ctx->d_ih2, v.data(), ctx->nblocks * sizeof(double), cudaMemcpyHostToDevice));
     return GBFK_OK;
 }
@@ -324,15 +365,17 @@ int set_csr(gbfk_ctx *ctx, const int64_t *row_ptr, const std::vector<int> &src, 
     std::vector<int> all_rows(nrows);
     for (int64_t r = 0; r < nrows; r++) all_rows[r] = (int)r;
 
-    CK(cudaMalloc(&ctx->d_row_ptr, (nrows + 1) * sizeof(int64_t)));
-    CK(cudaMalloc(&ctx->d_src, std::max<int64_t>(nnz, 1) * sizeof(int)));
-    CK(cudaMalloc(&ctx->d_w, std::max<int64_t>(nnz, 1) * sizeof(Real)));
-    CK(cudaMalloc(&ctx->d_nbr, (size_t)nb * 6 * sizeof(int)));
-    CK(cudaMalloc(&ctx->d_all_rows, nrows * sizeof(int)));
-    CK(cudaMalloc(&ctx->d_step_rows, std::max<size_t>(step_rows.size(), 1) * sizeof(int)));
-    CK(cudaMalloc(&ctx->d_gpw, nrows * sizeof(Real)));
-    CK(cudaMalloc(&ctx->d_gpg, nrows * sizeof(Real)));
-    CK(cudaMalloc(&ctx->d_gphi, nrows * sizeof(Real)));
+    int rc = GBFK_OK;
+    if (!rc) rc = topo_alloc(ctx, &ctx->d_row_ptr, (nrows + 1) * sizeof(int64_t));
+    if (!rc) rc = topo_alloc(ctx, &ctx->d_src, std::max<int64_t>(nnz, 1) * sizeof(int));
+    if (!rc) rc = topo_alloc(ctx, &ctx->d_w, std::max<int64_t>(nnz, 1) * sizeof(Real));
+    if (!rc) rc = topo_alloc(ctx, &ctx->d_nbr, (size_t)nb * 6 * sizeof(int));
+    if (!rc) rc = topo_alloc(ctx, &ctx->d_all_rows, nrows * sizeof(int));
+    if (!rc) rc = topo_alloc(ctx, &ctx->d_step_rows, std::max<size_t>(step_rows.size(), 1) * sizeof(int));
+    if (!rc) rc = topo_alloc(ctx, &ctx->d_gpw, nrows * sizeof(Real));
+    if (!rc) rc = topo_alloc(ctx, &ctx->d_gpg, nrows * sizeof(Real));
+    if (!rc) rc = topo_alloc(ctx, &ctx->d_gphi, nrows * sizeof(Real));
+    if (rc) return rc;
     CK(cudaMemcpy(ctx->d_row_ptr, row_ptr, (nrows + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
     if (nnz) {
         CK(cudaMemcpy(ctx->d_src, src.data(), nnz * sizeof(int), cudaMemcpyHostToDevice));
@@ -378,7 +421,6 @@ int build_uniform_csr(gbfk_ctx *ctx)
                             src[(int64_t)b * kLabGhosts + g] = sb * kBS3 + (wx & 7) + 8 * ((wy & 7) + 8 * (wz & 7));
                         }
             }
-    if (ctx->d_nbr) { cudaFree(ctx->d_nbr); ctx->d_nbr = nullptr; }
     return ctx->precision == GBFK_F64
                ? set_csr<double>(ctx, row_ptr.data(), src, ones.data(), ones.data(), ones.data(), true)
                : set_csr<float>(ctx, row_ptr.data(), src, ones.data(), ones.data(), ones.data(), true);
@@ -406,8 +448,9 @@ int prepare_static(gbfk_ctx *ctx, double Dw, double Dg)
     if (rc) return rc;
     const double kDw = (double)(Real)Dw, kDg = (double)(Real)Dg;
     if (!ctx->faces_valid || ctx->faces_Dw != kDw || ctx->faces_Dg != kDg) {
-        if (!ctx->d_H) CK(cudaMalloc(&ctx->d_H, (size_t)ctx->nblocks * kFacesPerBlock * sizeof(Real)));
-        if (!ctx->d_btype) CK(cudaMalloc(&ctx->d_btype, (size_t)ctx->nblocks));
+        int rc = topo_alloc(ctx, &ctx->d_H, (size_t)ctx->nblocks * kFacesPerBlock * sizeof(Real));
+        if (!rc) rc = topo_alloc(ctx, &ctx->d_btype, (size_t)ctx->nblocks);
+        if (rc) return rc;
         CK(launch_faces<Real>(view<Real>(ctx), (Real)Dw, (Real)Dg, (Real *)ctx->d_H, ctx->d_meta, ctx->d_btype,
                               ctx->stream));
         ctx->launches++;
@@ -439,7 +482,10 @@ int build_step_lists(gbfk_ctx *ctx)
     for (int b = 0; b < nb; b++)
         if (bt[b] == kBlockEmpty) lists.push_back(b);
     if ((int)lists.size() != nb) return fail(ctx, GBFK_E_CUDA, "rd_step: unknown block type");
-    if (!ctx->d_lists) CK(cudaMalloc(&ctx->d_lists, (size_t)nb * sizeof(int)));
+    {
+        const int rc = topo_alloc(ctx, &ctx->d_lists, (size_t)nb * sizeof(int));
+        if (rc) return rc;
+    }
     CK(cudaMemcpyAsync(ctx->d_lists, lists.data(), (size_t)nb * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->n_heavy = nh;
@@ -555,7 +601,10 @@ int fwt_impl(gbfk_ctx *ctx, double *out)
     const Real *phi = (const Real *)ctx->phi[ctx->cur];
     CK(launch_fill_ghosts<Real>(ctx->d_all_rows, ctx->nrows, ctx->d_row_ptr, ctx->d_src, (const Real *)ctx->d_w,
                                 phi, (Real *)ctx->d_gphi, ctx->stream));
-    if (!ctx->d_fwt) CK(cudaMalloc(&ctx->d_fwt, (size_t)ctx->nblocks * sizeof(double)));
+    {
+        const int rc = topo_alloc(ctx, &ctx->d_fwt, (size_t)ctx->nblocks * sizeof(double));
+        if (rc) return rc;
+    }
     CK(launch_fwt_details<Real>(view<Real>(ctx), phi, ctx->d_fwt, ctx->stream));
     ctx->launches += 2;
     CK(cudaMemcpyAsync(out, ctx->d_fwt, (size_t)ctx->nblocks * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -679,7 +728,7 @@ int gbfk_destroy(gbfk_ctx *ctx)
     if (!ctx) return GBFK_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    free_topology(ctx);
+    release_topology(ctx);
     void *ptrs[] = {ctx->phi[0], ctx->phi[1], ctx->pw, ctx->pg, ctx->d_nan, ctx->d_stage, ctx->d_ints, ctx->d_meta,
                     ctx->d_t1c, ctx->d_flair, ctx->d_pet, ctx->d_roi, ctx->d_model, ctx->d_partial, ctx->d_lik};
     for (void *p : ptrs)
@@ -770,9 +819,12 @@ int gbfk_set_uniform(gbfk_ctx *ctx, int bpd)
     const double h = 1.0 / (8.0 * bpd);
     ctx->h_h.assign(nb, h);
     ctx->identity_slots = true;
-    CK(cudaMalloc(&ctx->d_slot, nb * sizeof(int)));
-    CK(cudaMalloc(&ctx->d_nbr, (size_t)nb * 6 * sizeof(int)));
-    CK(cudaMalloc(&ctx->d_h, nb * ctx->rsize));
+    {
+        int rc = topo_alloc(ctx, &ctx->d_slot, nb * sizeof(int));
+        if (!rc) rc = topo_alloc(ctx, &ctx->d_nbr, (size_t)nb * 6 * sizeof(int));
+        if (!rc) rc = topo_alloc(ctx, &ctx->d_h, nb * ctx->rsize);
+        if (rc) return rc;
+    }
     CK(cudaMemcpy(ctx->d_slot, ctx->h_slot.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d_nbr, nbr.data(), (size_t)nb * 6 * sizeof(int), cudaMemcpyHostToDevice));
     if (ctx->precision == GBFK_F64) {
@@ -837,8 +889,11 @@ int gbfk_set_topology(gbfk_ctx *ctx, const gbfk_blockinfo *blocks, int nblocks, 
         ctx->h_h[i] = blocks[i].h;
         if (blocks[i].slot != i) ctx->identity_slots = false;
     }
-    CK(cudaMalloc(&ctx->d_slot, nblocks * sizeof(int)));
-    CK(cudaMalloc(&ctx->d_h, nblocks * ctx->rsize));
+    {
+        int rc = topo_alloc(ctx, &ctx->d_slot, nblocks * sizeof(int));
+        if (!rc) rc = topo_alloc(ctx, &ctx->d_h, nblocks * ctx->rsize);
+        if (rc) return rc;
+    }
     CK(cudaMemcpy(ctx->d_slot, ctx->h_slot.data(), nblocks * sizeof(int), cudaMemcpyHostToDevice));
     if (ctx->precision == GBFK_F64) {
         CK(cudaMemcpy(ctx->d_h, ctx->h_h.data(), nblocks * sizeof(double), cudaMemcpyHostToDevice));
@@ -1098,7 +1153,7 @@ int gbfk_collapse(gbfk_ctx *ctx, int n, const int *children, const int *parents)
 static int dump_to_device(gbfk_ctx *ctx, int n)
 {
     if (!ctx->have_topology) return fail(ctx, GBFK_E_STATE, "uq_dump: no topology");
-    if (!ctx->d_origin) return fail(ctx, GBFK_E_STATE, "uq_dump: block origins unknown (non power-of-two uniform grid)");
+    if (!ctx->have_origin) return fail(ctx, GBFK_E_STATE, "uq_dump: block origins unknown (non power-of-two uniform grid)");
     if (n <= 0 || (int64_t)n * n * n > ((int64_t)1 << 34)) return fail(ctx, GBFK_E_INVALID, "uq_dump: bad grid size %d", n);
     const size_t bytes = (size_t)n * n * n * sizeof(double);
     if (ctx->model_bytes < bytes) {
@@ -1282,8 +1337,9 @@ struct Adjoint {
         asteps++;
         ctx->launches += 2;
     }
-    static double beta(int c, int r)  // C(c + r, c) = C(c + r, r), capped
+    static double beta(int c, int r)  // C(c + r, c) = C(c + r, r), capped; 0 for r < 0
     {
+        if (r < 0) return 0;
         const int k = std::min(c, r), m = std::max(c, r);
         double b = 1;
         for (int i = 1; i <= k; i++) {
@@ -1291,6 +1347,56 @@ struct Adjoint {
             if (b > 1e18) return 1e18;
         }
         return b;
+    }
+    // Binomial checkpointing (Griewank and Walther, "Algorithm 799: revolve",
+    // ACM TOMS 26(1), 2000): reversing l steps from a stored state with c free
+    // buffers costs the fewest forward steps when the first checkpoint goes
+    // l1 steps ahead, l1 in [max(b(s, r-2), l - b(s-1, r)),
+    // min(b(s, r-1), l - b(s-1, r-1))], with s = c + 1 states held (the
+    // start's own buffer counts) and r the smallest repetition number with
+    // b(s, r) >= l, b(s, r) = C(s + r, s).  Inside the recursion the lower end
+    // is taken; on the chain of checkpoints that the first forward sweep
+    // stores on its way to the horizon, the upper end (those states cost no
+    // extra steps there).
+    static int split(int l, int c, bool upper)
+    {
+        const int s = c + 1;
+        int r = 0;
+        while (beta(s, r) < l) r++;
+        const double lo = std::max(beta(s, r - 2), l - beta(s - 1, r));
+        const double hi = std::min(beta(s, r - 1), l - beta(s - 1, r - 1));
+        const double pick = upper ? std::max(lo, hi) : lo;
+        return (int)std::max(1.0, std::min(pick, (double)(l - 1)));
+    }
+    // The first forward sweep from X (phi_0) to the horizon state F, storing
+    // the states at the chain positions a + split(l, c, true) in slots[c-1],
+    // slots[c-2], ... (the states reverse_chain expects there).
+    void sweep(const Real *X, Real *F, int nsteps, int c)
+    {
+        int pos = 0;
+        const Real *cur = X;
+        while (nsteps - pos > 1 && c > 0 && err == cudaSuccess) {
+            const int l1 = split(nsteps - pos, c, true);
+            advance(cur, slots[c - 1], l1);
+            cur = slots[c - 1];
+            pos += l1;
+            c--;
+        }
+        advance(cur, F, nsteps - pos);
+    }
+    // reverse() along the chain stored by sweep(): slots[c-1] already holds
+    // the state a + split(b - a, c, true).
+    void reverse_chain(int a, int b, int c, Real *X)
+    {
+        const int l = b - a;
+        if (l <= 1 || c == 0 || err != cudaSuccess) {
+            reverse(a, b, c, X);
+            return;
+        }
+        const int l1 = split(l, c, true);
+        Real *S = slots[c - 1];
+        reverse_chain(a + l1, b, c - 1, S);
+        reverse(a, a + l1, c, X);
     }
     // X holds phi_a; LAM holds dL/dphi_b on entry and dL/dphi_a on exit;
     // slots[0..c) are free.
@@ -1310,10 +1416,7 @@ struct Adjoint {
             adjoint_step(X);
             return;
         }
-        int r = 0;
-        while (beta(c, r) < l) r++;
-        int l1 = (int)std::max(1.0, l - beta(c - 1, r));
-        if (l1 >= l) l1 = l - 1;
+        const int l1 = split(l, c, false);
         Real *S = slots[c - 1];
         advance(X, S, l1);
         reverse(a + l1, b, c - 1, S);
@@ -1406,9 +1509,9 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
             e = cudaMemcpyAsync(X0, ctx->phi[ctx->cur], A.fbytes, cudaMemcpyDeviceToDevice, ctx->stream);
         }
     }
-    // forward to the horizon, loss and its gradient
+    // forward to the horizon (storing the first chain of checkpoints), loss and its gradient
     if (e == cudaSuccess) {
-        A.advance(X0, F, p->nsteps);
+        A.sweep(X0, F, p->nsteps, p->nsnapshots);
         e = A.err;
     }
     double lik[4] = {0, 0, 0, 0};
@@ -1448,7 +1551,7 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     }
     // reverse sweep; then the zeros of the blocks where dL/dphi_0 vanishes
     if (e == cudaSuccess) {
-        A.reverse(0, p->nsteps, p->nsnapshots, X0);
+        A.reverse_chain(0, p->nsteps, p->nsnapshots, X0);
         e = A.err;
     }
     if (e == cudaSuccess) {
@@ -1510,7 +1613,7 @@ extern "C" int gbfk_forward_adjoint(gbfk_ctx *ctx, const gbfk_adjoint_params *p,
     if (!ctx) return GBFK_E_INVALID;
     ctx->phi_clamped = false;
     if (!p || !out) return fail(ctx, GBFK_E_INVALID, "forward_adjoint: null argument");
-    if (!ctx->uniform || !ctx->d_origin) return fail(ctx, GBFK_E_STATE, "forward_adjoint: needs a uniform power-of-two grid");
+    if (!ctx->uniform || !ctx->have_origin) return fail(ctx, GBFK_E_STATE, "forward_adjoint: needs a uniform power-of-two grid");
     if (ctx->obs_n != 8 * ctx->bpd || ctx->nroi) return fail(ctx, GBFK_E_STATE, "forward_adjoint: observations must cover the grid (no ROI)");
     if (p->nsteps < 0 || p->nsnapshots < 1 || !(p->slope != 0) || !(p->Dw > 0))
         return fail(ctx, GBFK_E_INVALID, "forward_adjoint: bad parameters");

@@ -22,12 +22,21 @@
 //    the array and give wrong results.  Serialise them.
 //  - the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//    before any stream capture.  The address is kept with the ID of the
+//    device's context and looked up again if the context changed (after a
+//    cudaDeviceReset, say).
+//  - no NaN check: the step kernel's NaN flag lives in the shared array and
+//    is not reported; a step that produces NaN or Inf returns GBFK_OK.
+//  - the caller's current device is restored before returning; an error that
+//    the caller's earlier work left pending is returned as GBFK_E_CUDA and
+//    not cleared.
 #include "gbfk.h"
 #include "gbfk_kernels.cuh"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 namespace gbfk {
@@ -54,6 +63,34 @@ namespace {
 
 std::mutex g_static_mutex;
 unsigned char *g_static_ptr[64] = {};
+unsigned long long g_static_ctx[64] = {};
+
+// Unique ID of the current context (cuCtxGetId through the runtime's driver
+// entry points); 0 if it cannot be had.
+unsigned long long current_context_id()
+{
+    typedef CUresult (*GetCurrent)(CUcontext *);
+    typedef CUresult (*GetId)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (GetCurrent)p;
+        p = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (GetId)p;
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS) return id;
+    return 0;
+}
 
 // Neighbour table, slot table and 1/(h*h) of a uniform periodic bpd^3 grid,
 // written on the device (block b = bx + bpd*(by + bpd*bz) lives in slot b).
@@ -79,14 +116,18 @@ __global__ void static_topology_kernel(int bpd, double ih2, int *nbr, double *ih
     }
 }
 
+// The array's device address on `device` (current): looked up once per device
+// and context.
 int static_scratch(int device, unsigned char **out)
 {
     std::lock_guard<std::mutex> lk(g_static_mutex);
     if (device < 0 || device >= 64) return GBFK_E_INVALID;
-    if (!g_static_ptr[device]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_static_ptr[device] || ctx != g_static_ctx[device]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess || !p) return GBFK_E_CUDA;
         g_static_ptr[device] = (unsigned char *)p;
+        g_static_ctx[device] = ctx;
     }
     *out = g_static_ptr[device];
     return GBFK_OK;
@@ -129,6 +170,13 @@ int static_step(unsigned char *scratch, int bpd, const void *pw, const void *pg,
     return GBFK_OK;
 }
 
+// Restores the caller's current device when the entry point returns.
+struct DeviceGuard {
+    int saved = -1;
+    DeviceGuard() { if (cudaGetDevice(&saved) != cudaSuccess) saved = -1; }
+    ~DeviceGuard() { if (saved >= 0) cudaSetDevice(saved); }
+};
+
 }  // namespace
 }  // namespace gbfk
 
@@ -140,12 +188,26 @@ extern "C" int gbfk_rd_step_static(int precision, int bpd, const void *pw, const
     if (precision != GBFK_F64 && precision != GBFK_F32) return GBFK_E_INVALID;
     if (bpd <= 0) return GBFK_E_INVALID;
     if ((long long)bpd * bpd * bpd > kStaticMaxBlocks) return GBFK_E_TOO_LARGE;
-    if (!pw || !pg || !phi_in || !phi_out || phi_in == phi_out) return GBFK_E_INVALID;
+    if (!pw || !pg || !phi_in || !phi_out) return GBFK_E_INVALID;
+    // phi_out must not overlap phi_in anywhere: the step reads neighbours'
+    // halos from phi_in while other CTAs write phi_out
+    const uintptr_t bytes = (uintptr_t)bpd * bpd * bpd * 512 * (precision == GBFK_F64 ? 8 : 4);
+    const uintptr_t in0 = (uintptr_t)phi_in, out0 = (uintptr_t)phi_out;
+    if (in0 < out0 + bytes && out0 < in0 + bytes) return GBFK_E_INVALID;
+    DeviceGuard guard;
     if (cudaSetDevice(device) != cudaSuccess) return GBFK_E_CUDA;
+    // an error left pending by the caller's own earlier work is reported and
+    // left in place, so that the launch checks below see only this call's
+    if (cudaPeekAtLastError() != cudaSuccess) return GBFK_E_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (s) {
+        // the stream must belong to `device`
+        int sdev = -1;
+        if (cudaStreamGetDevice(s, &sdev) != cudaSuccess || sdev != device) return GBFK_E_INVALID;
+    }
     unsigned char *scratch = nullptr;
     const int rc = static_scratch(device, &scratch);
     if (rc != GBFK_OK) return rc;
-    cudaStream_t s = (cudaStream_t)stream;
     return precision == GBFK_F64 ? static_step<double>(scratch, bpd, pw, pg, phi_in, phi_out, Dw, Dg, rho, dt, s)
                                  : static_step<float>(scratch, bpd, pw, pg, phi_in, phi_out, Dw, Dg, rho, dt, s);
 }

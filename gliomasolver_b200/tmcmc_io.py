@@ -267,29 +267,39 @@ def _atomic_write(path, write):
 
 
 STATE_FILE = "tmcmc_state.npz"
+GENERATION_FILE = "tmcmc_gen_%03d.npz"
 
 
 class Checkpointer:
     """An ``on_generation`` hook for :func:`~gliomasolver_b200.tmcmc.tmcmc`
     that writes, after every generation, what the reference writes during a
-    run (curgen_db_<g>.txt, runinfo.txt; engine_tmcmc.c:1176-1184) and
-    tmcmc_state.npz: every generation's population and statistics in binary
-    and the random generator's state, from which ``load_checkpoint`` resumes
-    the run exactly.  After the last generation it also writes fitness.txt
-    (and, with ``posterior``, posterior.txt and statistics.txt)."""
+    run (curgen_db_<g>.txt, runinfo.txt; engine_tmcmc.c:1176-1184), the
+    generation's population in binary (tmcmc_gen_<g>.npz, written once) and
+    tmcmc_state.npz: the run's statistics and the random generator's state,
+    from which ``load_checkpoint`` resumes the run exactly.  Every file is
+    written under a temporary name and renamed, so a crash leaves either the
+    previous version or the new one.  runinfo.txt holds ``max_stages`` rows
+    (``par.max_stages`` when a parameter file is given), as the reference's
+    reader expects (engine_tmcmc.c:393-394).  After the last generation it
+    also writes fitness.txt (and, with ``posterior``, posterior.txt and
+    statistics.txt)."""
 
-    def __init__(self, directory, par: TMCMCPar = None, posterior: bool = True):
+    def __init__(self, directory, par: TMCMCPar = None, posterior: bool = True, max_stages: int = None):
         self.directory = os.fspath(directory)
         self.par = par
+        self.max_stages = par.max_stages if par is not None else (max_stages or TMCMCPar().max_stages)
         self.posterior = posterior
         os.makedirs(self.directory, exist_ok=True)
 
     def __call__(self, result: TMCMCResult, rng_state: dict):
         g = len(result.stages) - 1
-        par = self.par if self.par is not None else TMCMCPar(max_stages=max(g + 1, 20),
+        par = self.par if self.par is not None else TMCMCPar(max_stages=max(self.max_stages, g + 1),
                                                               pop_size=len(result.stages[0][1]))
-        with open(os.path.join(self.directory, "curgen_db_%03d.txt" % g), "w") as f:
-            f.write(curgen_db_text(*result.stages[g]))
+        db = curgen_db_text(*result.stages[g])
+        _atomic_write(os.path.join(self.directory, "curgen_db_%03d.txt" % g), lambda f: f.write(db.encode()))
+        theta, F = result.stages[g]
+        _atomic_write(os.path.join(self.directory, GENERATION_FILE % g),
+                      lambda f: np.savez(f, theta=theta, F=F))
         text = runinfo_text(result, par.max_stages, par.pop_size)
         _atomic_write(os.path.join(self.directory, "runinfo.txt"), lambda f: f.write(text.encode()))
         arrays = {"p": np.asarray(result.p, dtype=np.float64),
@@ -301,9 +311,6 @@ class Checkpointer:
                   "ss": np.asarray(result.ss, dtype=np.float64),
                   "evaluations": np.int64(result.evaluations),
                   "rng_state": np.frombuffer(json.dumps(rng_state).encode(), dtype=np.uint8)}
-        for k, (theta, F) in enumerate(result.stages):
-            arrays["theta_%03d" % k] = theta
-            arrays["F_%03d" % k] = F
         _atomic_write(os.path.join(self.directory, STATE_FILE), lambda f: np.savez(f, **arrays))
         if result.p_next is not None:
             write_reference_outputs(result, self.directory, par, self.posterior)
@@ -312,9 +319,13 @@ class Checkpointer:
 def load_checkpoint(directory) -> TMCMCCheckpoint:
     """The state a :class:`Checkpointer` left in ``directory``: pass it as
     ``tmcmc(..., start=...)`` with the same likelihood and options."""
-    with np.load(os.path.join(os.fspath(directory), STATE_FILE)) as z:
+    directory = os.fspath(directory)
+    with np.load(os.path.join(directory, STATE_FILE)) as z:
         n = int(z["p"].size)
-        stages = [(z["theta_%03d" % k].copy(), z["F_%03d" % k].copy()) for k in range(n)]
+        stages = []
+        for k in range(n):
+            with np.load(os.path.join(directory, GENERATION_FILE % k)) as gz:
+                stages.append((gz["theta"].copy(), gz["F"].copy()))
         res = TMCMCResult(stages[-1][0], stages[-1][1], [float(v) for v in z["p"]], 0.0,
                           [float(v) for v in z["acceptance"]], int(z["evaluations"]), stages=stages,
                           uniques=[int(v) for v in z["uniques"]], coef_var=[float(v) for v in z["coef_var"]],

@@ -391,15 +391,21 @@ int gbfk_probe_bounded_wait(int device, double *seconds);
  * loading the library holds until the process exits.
  *   pw, pg, phi_in : device arrays of bpd^3 * 512 Real in block-pool order
  *                    (block (bx,by,bz) at slot bx + bpd*(by + bpd*bz));
- *   phi_out        : device array of the same size, not phi_in;
- *   Dw, Dg, rho, dt: as for gbfk_rd_step; stream: cudaStream_t or NULL for
+ *   phi_out        : device array of the same size that overlaps phi_in
+ *                    nowhere (GBFK_E_INVALID otherwise);
+ *   Dw, Dg, rho, dt: as for gbfk_rd_step; stream: a cudaStream_t of `device`
+ *                    (GBFK_E_INVALID for another device's stream) or NULL for
  *                    the legacy default stream; device: CUDA ordinal.
  * Returns GBFK_E_TOO_LARGE when bpd^3 > GBFK_STATIC_MAX_BLOCKS.  Every call
  * on a device shares the scratch array (it keeps the last call's contents and
  * is fully rewritten by each call), so calls that overlap on the GPU race:
- * serialise them.  The first call on a device looks up the array's address
- * with that device current; make it before any stream capture.  The work is
- * asynchronous on the stream. */
+ * serialise them.  The first call on a device (and the first after its
+ * context was reset) looks up the array's address with that device current;
+ * make it before any stream capture.  The work is asynchronous on the stream.
+ * No NaN check: a step that produces NaN or Inf still returns GBFK_OK (check
+ * the output where that matters).  The caller's current device is restored;
+ * an error the caller's earlier work left pending is returned as GBFK_E_CUDA
+ * and left in place. */
 #define GBFK_STATIC_MAX_BLOCKS 512
 int gbfk_rd_step_static(int precision, int bpd, const void *pw, const void *pg, const void *phi_in,
                         void *phi_out, double Dw, double Dg, double rho, double dt, void *stream,

@@ -82,3 +82,27 @@ def test_static_step_rejects_grids_beyond_its_scratch(gbfk_lib):
     assert L.gbfk_rd_step_static(_lib.GBFK_F32, 9, p, p, p, q, 1e-4, 1e-5, 0.1, 0.1, None, 0) == 7
     # the input and the output must differ
     assert L.gbfk_rd_step_static(_lib.GBFK_F32, 2, p, p, p, p, 1e-4, 1e-5, 0.1, 0.1, None, 0) == 1
+
+
+def test_static_step_argument_checks(gbfk_lib):
+    """Overlapping input and output ranges and a stream of another device are
+    refused before any device work; the caller's current device is kept."""
+    import torch
+
+    L = _lib.load()
+    dev = torch.device("cuda", 0)
+    n = 2 * 2 * 2 * 512
+    buf = torch.zeros(3 * n, device=dev)
+    at = lambda k: ctypes.c_void_p(buf[k:].data_ptr())  # noqa: E731
+    # phi_out starts inside phi_in (an offset into the same allocation)
+    assert L.gbfk_rd_step_static(_lib.GBFK_F32, 2, at(0), at(0), at(0), at(n - 1), 1e-4, 1e-5, 0.1, 0.1, None, 0) == 1
+    assert L.gbfk_rd_step_static(_lib.GBFK_F32, 2, at(0), at(0), at(n - 1), at(0), 1e-4, 1e-5, 0.1, 0.1, None, 0) == 1
+    # adjacent ranges do not overlap
+    torch.cuda.set_device(0)
+    assert L.gbfk_rd_step_static(_lib.GBFK_F32, 2, at(0), at(0), at(0), at(n), 1e-4, 1e-5, 0.1, 0.1, None, 0) == 0
+    torch.cuda.synchronize(dev)
+    assert torch.cuda.current_device() == 0
+    if torch.cuda.device_count() > 1:
+        other = torch.cuda.Stream(device=1)
+        assert L.gbfk_rd_step_static(_lib.GBFK_F32, 2, at(0), at(0), at(0), at(n), 1e-4, 1e-5, 0.1, 0.1,
+                                     ctypes.c_void_p(other.cuda_stream), 0) == 1
