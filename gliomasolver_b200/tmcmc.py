@@ -200,6 +200,7 @@ class TMCMCOptions:
     pop_size: int = 512
     max_stages: int = 100         # MaxStages: generations, the prior one included
     tol_cov: float = 1.0          # TolCOV
+    opt_tol: float = 1e-6         # opt.Tol: fzerofind's acceptance of |objlogp| (engine_tmcmc.c:75)
     bbeta: float = 0.2            # proposal covariance scale
     min_chain: int = 0            # MinChainLength
     max_chain: int = 1            # MaxChainLength
@@ -238,25 +239,184 @@ class TMCMCCheckpoint:
     rng_state: dict
 
 
-def _cov_of_weights(F, dp):
-    w = np.exp((F - F.max()) * dp)
-    q = w / w.sum()
-    return q.std(ddof=1) / q.mean()
+FZERO_STEP = 1e-4  # the exponent grid of fzerofind (tmcmc_stats.c:104)
+_FZERO_CHUNK = 2048
 
 
-def next_exponent(F, p, tol_cov):
-    """p_{j+1} in (p, 1] with COV(L^(p_{j+1} - p)) = tol_cov (bisection on
-    the increasing COV), or 1 when even p_{j+1} = 1 stays below it."""
-    if _cov_of_weights(F, 1.0 - p) <= tol_cov:
-        return 1.0
-    lo, hi = p, 1.0
-    for _ in range(100):
+def _seqsum(a, axis=-1):
+    """Sum in index order, as the reference's loops add (numpy's own sum is
+    pairwise and rounds differently)."""
+    return np.cumsum(a, axis=axis).take(-1, axis=axis)
+
+
+def objlogp(x, F, pj, tol_cov):
+    """(COV of the weights exp((F - max F) (x - pj)) - tol_cov)^2 for each
+    exponent in ``x`` (Objlogp, tmcmc_stats.c:18-50: weights normalised by
+    their sum, mean and sample standard deviation, sums in index order)."""
+    x = np.atleast_1d(np.asarray(x, dtype=np.float64))
+    F = np.asarray(F, dtype=np.float64)
+    n = F.size
+    with np.errstate(over="ignore", invalid="ignore", divide="ignore"):
+        w = np.exp((F - F.max())[None, :] * (x - pj)[:, None])
+        q = w / _seqsum(w)[:, None]
+        mean = _seqsum(q) / n
+        std = np.sqrt(_seqsum((q - mean[:, None]) ** 2) / (n - 1))
+        return (std / mean - tol_cov) ** 2
+
+
+def fzerofind(F, pj, tol_cov, opt_tol):
+    """The reference's exponent search (fzerofind, tmcmc_stats.c:96-215):
+    objlogp on the grid x = x_lo + k step of [0, 4) with step 1e-4, in order,
+    keeping the first smallest value and stopping at the first value within
+    opt_tol; without such a value the grid is refined around the smallest one
+    (+-10 steps, step / 10) until the step falls below 1e-16.  Returns
+    (converged, x, f); the reference returns "converged" with x = f = 0 when
+    the step runs out."""
+    x_lo, x_hi, step = 0.0, 4.0, FZERO_STEP
+    while True:
+        niters = int((x_hi - x_lo) / step)
+        m, fm, found = 0.0, np.finfo(np.float64).max, False
+        for start in range(0, niters, _FZERO_CHUNK):
+            it = np.arange(start, min(niters, start + _FZERO_CHUNK), dtype=np.float64)
+            xs = x_lo + it * step
+            fx = objlogp(xs, F, pj, tol_cov)
+            with np.errstate(invalid="ignore"):
+                hit = np.flatnonzero(np.abs(fx) <= opt_tol)
+            seg = fx[: hit[0] + 1] if hit.size else fx
+            valid = np.flatnonzero(~np.isnan(seg))
+            if valid.size:
+                k = valid[np.argmin(seg[valid])]
+                if seg[k] < fm:
+                    fm, m = float(seg[k]), float(xs[k])
+            if hit.size:
+                found = True
+                break
+        if found:
+            return True, m, fm
+        x_lo = max(m - 10 * step, 0.0)
+        x_hi = min(m + 10 * step, 4.0)
+        step = 0.1 * step
+        if step < 1e-16:
+            return True, 0.0, 0.0
+
+
+def force_pos_def(S):
+    """Diagonal loading until S is positive definite (force_pos_def2,
+    posdef.c:273-341): while an eigenvalue is not positive, add
+    max(0.01 max|diag|, 1e-15) - min(diag, 0) to the diagonal if some
+    diagonal entry is at most 1e-15, else scale the diagonal by 1.01."""
+    S = np.array(S, dtype=np.float64, copy=True)
+    while not np.all(np.linalg.eigvalsh(S) > 0):
+        d = np.diag(S).copy()
+        m = np.max(np.abs(d)) * 0.01
+        if np.any(d <= 1e-15):
+            neg = d.min()
+            addit = m - neg if neg < 0 else max(m, 1e-15)
+            S[np.diag_indices_from(S)] = d + addit
+        else:
+            S[np.diag_indices_from(S)] = d * 1.01
+    return S
+
+
+def make_posdef(S):
+    """S unchanged when positive definite, else force_pos_def (make_posdef
+    with method 2, posdef.c:577-616, as calculate_statistics calls it)."""
+    S = np.asarray(S, dtype=np.float64)
+    return S.copy() if np.all(np.linalg.eigvalsh(S) > 0) else force_pos_def(S)
+
+
+@dataclass
+class StageStatistics:
+    p_next: float        # the next tempering exponent
+    coef_var_next: float  # the search's objective there (CoefVar[gen + 1] until the next stage)
+    coef_var: float      # COV of the weights toward p_next (CoefVar[gen])
+    log_selection: float  # log evidence increment (logselection[gen])
+    q: np.ndarray        # normalised weights
+    mean: np.ndarray     # weighted mean of the population (meantheta[gen])
+    ss: np.ndarray       # weighted sample covariance, made positive definite (SS)
+
+
+def cov_root(F, pj, tol_cov, opt_tol):
+    """The exponent search the reference tries first (fminsearch,
+    tmcmc_stats.c:315-408: GSL's simplex minimiser of objlogp started at pj),
+    here as bisection for COV = tol_cov on (pj, pj + 4] (the COV of the
+    weights grows with the exponent above pj).  Returns (converged, x, f)
+    with the reference's convergence test |f| <= opt_tol; without a root in
+    the bracket it reports no convergence, as the simplex search does when
+    the target COV is out of reach."""
+    F = np.asarray(F, dtype=np.float64)
+    lo, hi = pj, pj + 4.0
+    if objlogp(hi, F, pj, tol_cov)[0] <= opt_tol:
+        return True, hi, float(objlogp(hi, F, pj, tol_cov)[0])
+
+    def cov(x):
+        return np.sqrt(objlogp(x, F, pj, 0.0)[0])
+
+    if not cov(hi) > tol_cov:
+        return False, 0.0, 0.0
+    for _ in range(200):
         mid = 0.5 * (lo + hi)
-        if _cov_of_weights(F, mid - p) > tol_cov:
+        if mid in (lo, hi):
+            break
+        if cov(mid) > tol_cov:
             hi = mid
         else:
             lo = mid
-    return max(lo, p + 1e-12)
+    x = hi if abs(cov(hi) - tol_cov) <= abs(cov(lo) - tol_cov) else lo
+    f = float(objlogp(x, F, pj, tol_cov)[0])
+    return (abs(f) <= opt_tol), x, f
+
+
+def next_exponent_search(F, pj, tol_cov, opt_tol):
+    """(p_next, objective there) as calculate_statistics sets them
+    (tmcmc_stats.c:558-617): the root search, then fzerofind if it did not
+    converge; the result if it lies above pj, else pj + 1e-5; at most 1."""
+    conv, xmin, fmin = cov_root(F, pj, tol_cov, opt_tol)
+    if not conv:
+        conv, xmin, fmin = fzerofind(F, pj, tol_cov, opt_tol)
+    if conv and xmin > pj:
+        pn, fn = xmin, fmin
+    else:
+        pn, fn = pj + 0.1 * FZERO_STEP, float("nan")
+    return min(pn, 1.0), fn
+
+
+def stage_statistics(F, theta, pj, tol_cov, opt_tol, p_next=None):
+    """calculate_statistics (tmcmc_stats.c:545-765) for one generation: the
+    next exponent (next_exponent_search, or ``p_next`` when given); weights
+    exp(F (p_next - pj) - max) normalised by their sum in index order; log
+    evidence increment log(sum) + max - log(n); the weighted mean and
+    covariance summed over the population in index order (the covariance
+    entry (a, b) takes its product in the order (max(a, b), min(a, b)), the
+    last one the reference writes), made positive definite."""
+    F = np.asarray(F, dtype=np.float64)
+    theta = np.asarray(theta, dtype=np.float64)
+    n, d = theta.shape
+    if p_next is None:
+        pn, cvn = next_exponent_search(F, pj, tol_cov, opt_tol)
+    else:
+        pn, cvn = float(p_next), float("nan")
+    flcp = F * (pn - pj)
+    fjmax = flcp.max()
+    w = np.exp(flcp - fjmax)
+    sw = float(_seqsum(w))
+    q = w / sw
+    log_sel = float(np.log(sw) + fjmax - np.log(n))
+    mq = float(_seqsum(q)) / n
+    cv = float(np.sqrt(_seqsum((q - mq) ** 2) / (n - 1)) / mq)
+    mean = _seqsum(theta * q[:, None], axis=0)
+    dev = theta - mean
+    ss = np.empty((d, d))
+    for a in range(d):
+        for b in range(d):
+            hi, lo = max(a, b), min(a, b)
+            ss[a, b] = _seqsum((q * dev[:, hi]) * dev[:, lo])
+    return StageStatistics(float(pn), float(cvn), cv, log_sel, q, mean, make_posdef(ss))
+
+
+def next_exponent(F, p, tol_cov, opt_tol=1e-6):
+    """The exponent after p (next_exponent_search)."""
+    return next_exponent_search(np.asarray(F, dtype=np.float64), p, tol_cov, opt_tol)[0]
 
 
 def _distinct_points(theta, tol=1e-6):
@@ -269,16 +429,6 @@ def _distinct_points(theta, tol=1e-6):
             table[un] = x
             un += 1
     return un
-
-
-def _posdef(S):
-    """The symmetric part of S with its eigenvalues raised to a small
-    positive floor (the reference forces positive definiteness,
-    posdef.c)."""
-    S = 0.5 * (S + S.T)
-    w, V = np.linalg.eigh(S)
-    floor = max(w.max(), 1e-300) * 1e-12
-    return (V * np.maximum(w, floor)) @ V.T
 
 
 def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions(), on_generation=None, start=None):
@@ -328,13 +478,13 @@ def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions(), on_generati
         nevals = old.evaluations
         rng.bit_generator.state = start.rng_state
 
-    def record(theta, F, q, log_sel, mean, ss):
+    def record(theta, F, st):
         rec.stages.append((theta.copy(), F.copy()))
         rec.uniques.append(_distinct_points(theta))
-        rec.coef_var.append(float(q.std(ddof=1) / q.mean()))
-        rec.log_selection.append(float(log_sel))
-        rec.mean_theta.append(mean)
-        rec.ss = _posdef(ss)
+        rec.coef_var.append(st.coef_var)
+        rec.log_selection.append(st.log_selection)
+        rec.mean_theta.append(st.mean)
+        rec.ss = st.ss
         rec.theta, rec.loglik, rec.log_evidence, rec.evaluations = theta, F, float(log_ev), nevals
         if on_generation is not None:
             on_generation(rec, rng.bit_generator.state)
@@ -342,21 +492,13 @@ def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions(), on_generati
     done = p[-1] >= 1.0
     for _ in range(0 if done else opts.max_stages - len(p)):
         pj = p[-1]
-        pn = next_exponent(F, pj, opts.tol_cov)
-        flcp = F * (pn - pj)
-        w = np.exp(flcp - flcp.max())
-        log_sel = np.log(w.sum()) + flcp.max() - np.log(len(F))
-        log_ev += log_sel
-        q = w / w.sum()
-        mean = q @ theta
-        dev = theta - mean
-        ss = (dev.T * q) @ dev
-        record(theta, F, q, log_sel, mean, ss)
+        st = stage_statistics(F, theta, pj, opts.tol_cov, opts.opt_tol)
+        pn, q = st.p_next, st.q
+        log_ev += st.log_selection
+        record(theta, F, st)
         sel = rng.multinomial(opts.pop_size, q)
-        # the proposal covariance bbeta * SS, bbeta applied to the weighted
-        # deviations before the product (this operand order fixes the run's
-        # rounding, and with it every later generation)
-        cov = _posdef((opts.bbeta * (dev.T * q)) @ dev)
+        # the proposal covariance bbeta * SS (compute_candidate, engine_tmcmc.c:661-681)
+        cov = opts.bbeta * st.ss
         # leaders with chain lengths (split at max_chain, raised to min_chain)
         chains = []
         for i in np.flatnonzero(sel):
@@ -400,16 +542,10 @@ def tmcmc(loglik, lower, upper, opts: TMCMCOptions = TMCMCOptions(), on_generati
     # The last generation's own statistics, toward the exponent that would
     # follow it (1 after the final stage, so uniform weights), as the
     # reference computes them after its last stage.
-    pj = p[-1]
-    rec.p_next = 1.0 if pj >= 1.0 else next_exponent(F, pj, opts.tol_cov)
-    flcp = F * (rec.p_next - pj)
-    w = np.exp(flcp - flcp.max())
-    q = w / w.sum()
-    mean = q @ theta
-    dev = theta - mean
-    log_sel = np.log(w.sum()) + flcp.max() - np.log(len(F))
-    log_ev += log_sel
-    record(theta, F, q, log_sel, mean, (dev.T * q) @ dev)
+    st = stage_statistics(F, theta, p[-1], opts.tol_cov, opts.opt_tol)
+    rec.p_next = st.p_next
+    log_ev += st.log_selection
+    record(theta, F, st)
     rec.theta, rec.loglik, rec.log_evidence, rec.evaluations = theta, F, float(log_ev), nevals
     return rec
 

@@ -8,14 +8,22 @@ from gliomasolver_b200.tmcmc import TMCMCOptions, next_exponent, tmcmc
 
 
 def test_next_exponent_hits_the_target_cov():
+    """The reference's grid search stops at the first exponent whose
+    (COV - 1)^2 is within opt.Tol: |COV - 1| <= 1e-3 at the engine's default
+    1e-6, and far closer at the 1e-12 of tmcmc_glioma.par."""
     rng = np.random.default_rng(1)
     F = rng.normal(0, 50, 1000)
-    p1 = next_exponent(F, 0.0, 1.0)
-    w = np.exp((F - F.max()) * p1)
-    q = w / w.sum()
-    assert 0 < p1 < 1
-    assert q.std(ddof=1) / q.mean() == pytest.approx(1.0, rel=1e-6)
-    assert next_exponent(np.zeros(10), 0.3, 1.0) == 1.0     # flat likelihood: straight to 1
+    for tol, rel in ((1e-6, 1e-3), (1e-12, 1e-6)):
+        p1 = next_exponent(F, 0.0, 1.0, tol)
+        w = np.exp((F - F.max()) * p1)
+        q = w / w.sum()
+        assert 0 < p1 < 1
+        assert q.std(ddof=1) / q.mean() == pytest.approx(1.0, rel=rel)
+    # a flat likelihood never reaches the target COV: the reference then
+    # steps the exponent by 1e-5 (calculate_statistics, tmcmc_stats.c:611-617)
+    assert next_exponent(np.zeros(10), 0.3, 1.0) == pytest.approx(0.3 + 1e-5, abs=1e-15)
+    # a root above 1 ends the tempering
+    assert next_exponent(rng.normal(0, 0.5, 1000), 0.3, 1.0) == 1.0
 
 
 def test_gaussian_posterior_and_evidence():
