@@ -20,6 +20,7 @@ threaded TBB stand-in) on the host cores instead.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import re
@@ -57,6 +58,84 @@ def workload_config(n, precision):
         "Dw_cm2_day": DW, "rho_day": RHO, "L_cm": L_CM, "anatomy_seed": SEED,
         "l2": "inputs larger than L2: phi in/out + p_w + p_g = %d MB per step" % (16 * n ** 3 // 2 ** 20),
     }
+
+
+def heavy_blocks(pw, pg):
+    """Blocks that read p_w and p_g in the pipelined step: a cell with tissue
+    (p_w + p_g > 0) in the block or in its face halo (periodic)."""
+    t = (pw + pg) > 0
+    halo = t.copy()
+    for ax in range(3):
+        halo |= np.roll(t, 1, axis=ax) | np.roll(t, -1, axis=ax)
+    n = t.shape[0]
+    b = n // 8
+    return int(halo.reshape(b, 8, b, 8, b, 8).any(axis=(1, 3, 5)).sum())
+
+
+def fp64_lines(stream, local, steps):
+    """FP64 storage (the reference built with Real = double): config 1 in full
+    (64^3, 739 steps to T = 150 d) against the reference's own output (the
+    golden fixture: SHA-256 and relative L2 of a subsample), and the 256^3
+    workload of the headline line in FP64.  CUDA events on the stream."""
+    import hashlib
+
+    import torch
+
+    from gliomasolver_b200 import BlockPool
+
+    peak, _ = measured_peak()
+    out = {}
+    with np.load(ROOT / "tests" / "golden" / "config1_n64_f64.npz") as z:
+        fx = {k: z[k] for k in z.files}
+    n = int(fx["n"])
+    pw, pg, c0, _ = make_case(n, int(fx["seed"]))
+    with BlockPool((n // 8) ** 3, "f64", device=local, stream=stream.cuda_stream) as pool:
+        pool.set_uniform(n // 8)
+        for name, a in (("p_w", pw), ("p_g", pg), ("phi", c0)):
+            pool.upload_dense(name, a)
+        pool.rd_step(float(fx["Dw"]), float(fx["Dg"]), float(fx["rho"]), float(fx["dt"]), 1)  # face coefficients
+        pool.upload_dense("phi", c0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pool.rd_step(float(fx["Dw"]), float(fx["Dg"]), float(fx["rho"]), float(fx["dt"]), int(fx["nsteps"]))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        phi = pool.download_dense("phi")
+    sub = phi[::4, ::4, ::4]
+    k = int(fx["nsteps"])
+    out["config1_n64"] = {
+        "workload": f"config 1: {n}^3 uniform, FP64, {k} steps to T = 150 d (fields L2-resident: 8 MB)",
+        "steps": k, "seconds": sec, "cell_updates_per_s": n ** 3 * k / sec,
+        "algorithmic_gbs": 32 * n ** 3 * k / sec / 1e9, "hbm_frac_algorithmic": 32 * n ** 3 * k / sec / 1e9 / peak,
+        "rel_l2_vs_reference": float(np.linalg.norm(sub - fx["out_sub"]) / np.linalg.norm(fx["out_sub"])),
+        "sha256_equal_to_reference": hashlib.sha256(np.ascontiguousarray(phi).tobytes()).hexdigest()
+        == str(fx["output_sha"])}
+    n = N_GRID
+    pw, pg, c0, _ = make_case(n, SEED)
+    s = make_schedule(DW, RHO, TEND, L_CM, n // 8, "f64")
+    with BlockPool((n // 8) ** 3, "f64", device=local, stream=stream.cuda_stream) as pool:
+        pool.set_uniform(n // 8)
+        for name, a in (("p_w", pw), ("p_g", pg), ("phi", c0)):
+            pool.upload_dense(name, a)
+        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, 5)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pool.rd_step(s.Dw, s.Dg, s.rho, s.dt, steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        heavy = heavy_blocks(pw, pg)
+    per = sec / steps
+    out["uniform_n256"] = {
+        "workload": f"the headline workload in FP64: {n}^3 uniform frozen topology, {steps} steps",
+        "ms_per_step": 1e3 * per, "cell_updates_per_s": n ** 3 / per,
+        "algorithmic_gbs": 32 * n ** 3 / per / 1e9, "algorithmic_frac": 32 * n ** 3 / per / 1e9 / peak,
+        "minimum_bytes_gbs": 8 * (2 * n ** 3 + 2 * 512 * heavy) / per / 1e9,
+        "minimum_bytes_frac": 8 * (2 * n ** 3 + 2 * 512 * heavy) / per / 1e9 / peak}
+    return out
 
 
 def measured_peak():
@@ -126,14 +205,25 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_run(steps, warmup, n_sample=CPU_SAMPLE_N, precision="f32", target_s=None):
-    """The reference's own operators on the host cores (oracle/_ref), else the
-    oracle restatement on one core.  Returns (record, kind, cores, n, steps)."""
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_reference_run(steps, warmup, n_sample=CPU_SAMPLE_N, precision="f32", target_s=None, threads=None):
+    """The reference's own operators on the host cores (oracle/_ref; all of
+    them, or ``threads``), else the oracle restatement on one core.  Returns
+    (record, kind, cores, n, steps)."""
     from oracle import oracle as O
 
     pw, pg, c0, _ = make_case(n_sample, SEED)
     s = make_schedule(DW, RHO, TEND, L_CM, n_sample // 8, precision)
-    cores = os.cpu_count() or 1
+    cores = threads or os.cpu_count() or 1
     if O.ref_available(precision):
         if target_s is not None:
             probe = O.ref_time(pw, pg, c0, s.Dw, s.Dg, s.rho, s.dt, 3, precision, threads=cores, warmup=1)
@@ -339,7 +429,7 @@ def adjoint_sample(stream, local, bpd=16, nsnap=64):
     }
 
 
-def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9):
+def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9, max_steps=None):
     """Config 5: forward + discrete adjoint for 16 samples at 256^3, FP32 state,
     each sample with its own seeded anatomy (brain scale U[0.8, 1.2]) and
     parameters sampled as in config 3 (Dw log-U[0.02,0.3], rho
@@ -395,6 +485,8 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9):
     def one(pool, cap_snap, prec, p_w, p_g, st, masks=None):
         R = np.float32 if prec == "f32" else np.float64
         s = make_schedule(st.Dw_cm2_day, st.rho_day, st.tend_day, L_CM, bpd, prec)
+        if max_steps is not None and s.nsteps > max_steps:
+            s = dataclasses.replace(s, nsteps=max_steps)
         pool.upload_dense("p_w", p_w.astype(R))
         pool.upload_dense("p_g", p_g.astype(R))
         if masks is None:
@@ -445,7 +537,9 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9):
     return {
         "workload": f"{nsamples} samples, forward + discrete adjoint at {n}^3, FP32 state, own anatomy each "
                     f"(scale U[0.8,1.2]), config-3 parameter sampling, checkpoints admitted by a "
-                    f"{hbm_cap / 1e9:.0f} GB HBM cap (up to {cap32} of 67 MB), one sample per call",
+                    f"{hbm_cap / 1e9:.0f} GB HBM cap (up to {cap32} of 67 MB), one sample per call"
+                    + (f"; horizons capped at {max_steps} steps (T' = min(T, {max_steps} dt))" if max_steps else ""),
+        "max_steps_per_sample": max_steps,
         "samples": nsamples, "steps_total": steps_total, "forward_steps_run": fwd_total, "seconds": t_total,
         "gradient_samples_per_s": nsamples / t_total,
         "roofline": {"achieved": alg / t_total / 1e9, "peak": peak, "unit": "GB/s", "frac": alg / t_total / 1e9 / peak,
@@ -568,13 +662,26 @@ def gpu_arm(args):
     achieved = alg_bytes / kernel_s / 1e9
     peak, peak_kind = measured_peak()
     traffic = profiled_traffic(pool.step_kernel) if (n, prec) == (N_GRID, "f32") else None
+    # the fewest bytes the exact shortcuts allow: phi in and out for every
+    # cell, p_w and p_g only for blocks with tissue in a cell or a face halo
+    heavy = heavy_blocks(pw, pg)
+    min_bytes = word * (2 * cells + 2 * 512 * heavy)
     roofline = {"kernel": KERNEL_NAMES[pool.step_kernel].format(real="float" if prec == "f32" else "double"),
-                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "algorithmic_bytes_per_launch": alg_bytes,
-                # DRAM bytes actually moved (ncu, one launch) over the same launch time:
-                # below the algorithmic bytes because empty blocks read no p_w/p_g
-                "traffic_frac": (traffic / kernel_s / 1e9 / peak) if traffic else None}
+                "bound": "hbm", "unit": "GB/s", "peak": peak,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                "algorithmic_achieved": achieved, "algorithmic_frac": achieved / peak,
+                "minimum_bytes_per_launch": min_bytes, "heavy_blocks": heavy,
+                "traffic_over_minimum": (traffic / min_bytes) if traffic else None}
+    if traffic:
+        # DRAM bytes of a warm launch (ncu) over the CUDA-event launch time: the
+        # HBM fraction.  The algorithmic figure (4 words per cell-update) exceeds
+        # what DRAM moves because empty blocks read no p_w, p_g or coefficients.
+        roofline.update({"achieved": traffic / kernel_s / 1e9, "frac": traffic / kernel_s / 1e9 / peak,
+                         "frac_basis": "DRAM bytes per warm launch (ncu) / CUDA-event launch time"})
+    else:
+        roofline.update({"achieved": achieved, "frac": achieved / peak,
+                         "frac_basis": "algorithmic bytes (4 words per cell-update) / CUDA-event launch time"})
 
     # ---- end to end through the public API with host buffers -------------
     e2e_steps = max(1, min(args.steps, 50))
@@ -623,14 +730,15 @@ def gpu_arm(args):
     adj = None
     adj5 = None
     adaptive = None
+    fp64 = fp64_lines(stream, local, args.steps) if prec == "f32" and n == N_GRID and not args.no_fp64 else None
     if args.adaptive_steps > 0 and rank == 0:
         adaptive = adaptive_forward(args.adaptive_steps, prec)
     if not args.no_batch:
         batch = batched_stage(args, stream, local)
     if not args.no_batch or args.adjoint_sample:
         adj = adjoint_sample(stream, local)
-    if args.adjoint_batch:
-        adj5 = adjoint_batch(stream, local)
+    if args.adjoint_batch_steps != 0 and rank == 0:
+        adj5 = adjoint_batch(stream, local, max_steps=args.adjoint_batch_steps if args.adjoint_batch_steps > 0 else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -638,7 +746,18 @@ def gpu_arm(args):
                                                        target_s=15.0)
         cpu = {"value": rec["cell_updates_per_s"], "unit": UNIT, "cores": cores, "kind": kind,
                "sample": f"{n_s}^3 grid of the same synthetic anatomy, {st} steps of the stepping loop "
-                         f"({rec['seconds']:.1f} s) on {cores} host threads"}
+                         f"({rec['seconds']:.1f} s) on {cores} host threads",
+               "cpu_model": cpu_model(), "host_threads": os.cpu_count()}
+        # the same reference on one core, and its FP64 build on all cores
+        r1, k1, c1, n1, st1 = cpu_reference_run(0, 1, CPU_SAMPLE_N, prec, target_s=6.0, threads=1)
+        cpu["one_core"] = {"value": r1["cell_updates_per_s"], "unit": UNIT, "cores": c1, "kind": k1,
+                           "sample": f"{n1}^3 grid, {st1} steps ({r1['seconds']:.1f} s) on 1 host thread"}
+        other = "f64" if prec == "f32" else "f32"
+        r2, k2, c2, n2, st2 = cpu_reference_run(0, 1, N_GRID if n == N_GRID else CPU_SAMPLE_N, other,
+                                                target_s=8.0)
+        cpu[other] = {"value": r2["cell_updates_per_s"], "unit": UNIT, "cores": c2, "kind": k2,
+                      "sample": f"{n2}^3 grid, {st2} steps ({r2['seconds']:.1f} s) on {c2} host threads, "
+                                f"the reference built with Real = {'double' if other == 'f64' else 'float'}"}
 
     if rank == 0:
         line = {
@@ -648,7 +767,9 @@ def gpu_arm(args):
             "parallelism": "replicas" if world > 1 else "single",
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
             "batched_stage": batch, "forward_adjoint": adj, "forward_adjoint_16x256": adj5,
-            "adaptive_forward": adaptive,
+            "adaptive_forward": adaptive, "fp64": fp64,
+            "not_in_value": "face_kernel (harmonic means, once per topology and (Dw, Dg): about 190 us at 256^3) "
+                            "runs in the warm-up, outside the timed steps",
         }
         print(json.dumps(line), flush=True)
     pool.close()
@@ -670,8 +791,10 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched TMCMC-stage measurement")
     ap.add_argument("--adjoint-sample", action="store_true",
                     help="run the config-4 gradient sample even with --no-batch")
-    ap.add_argument("--adjoint-batch", action="store_true",
-                    help="also run config 5 (16 gradient samples at 256^3, a few minutes)")
+    ap.add_argument("--adjoint-batch-steps", type=int, default=3000,
+                    help="config 5 (16 gradient samples at 256^3): cap on each sample's steps (-1: the full "
+                         "horizons, a few minutes; 0: skip)")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 lines (config 1, 256^3)")
     ap.add_argument("--adaptive-steps", type=int, default=400,
                     help="steps of the config-2 adaptive run on the resident drop-in (0: skip)")
     ap.add_argument("--step-kernel", default="auto", choices=["auto", "block", "pipelined"],

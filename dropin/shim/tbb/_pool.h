@@ -3,11 +3,12 @@
  * MRAG library names (task_scheduler_init, tick_count, blocked_range,
  * parallel_for, pipeline/filter, concurrent_bounded_queue, allocators).
  * TBB is not installed in this image; this shim lets the reference's own
- * sources compile unmodified for the oracle and the CPU baseline.
+ * sources compile unmodified: for the oracle and the CPU baseline, and for
+ * the drop-in driver whose block tree is the reference's own grid.
  *
  * Threads are POSIX threads (the reference compiles as gnu++98, so no
  * std::thread).  One global worker count is set by task_scheduler_init(n),
- * else by the environment variable GBFK_ORACLE_THREADS, else by the number
+ * else by the environment variable GBFK_TBB_THREADS, else by the number
  * of online cores.
  */
 #pragma once
@@ -25,7 +26,7 @@ inline int thread_count()
 {
     int &n = thread_count_ref();
     if (n <= 0) {
-        const char *e = getenv("GBFK_ORACLE_THREADS");
+        const char *e = getenv("GBFK_TBB_THREADS");
         if (e && atoi(e) > 0) n = atoi(e);
         else {
             long c = sysconf(_SC_NPROCESSORS_ONLN);

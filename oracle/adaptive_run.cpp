@@ -1,11 +1,12 @@
 /*
- * Adaptive forward run (config 2's schedule) on the reference's own MRAG grid.
+ * Adaptive forward run (config 2's schedule) on the reference's own MRAG grid,
+ * every step and every adaptation by the reference's own code: the oracle of
+ * the resident drop-in driver (dropin/glioma_adaptive.cpp).
  *
- * Test infrastructure: compiled with the reference's unmodified sources and
- * the adapter include/gbfk_mrag.hpp, linked against libgbfk.so (see
- * oracle/Makefile, target dropin).  The gpu mode needs a GPU at run time.
+ * Test infrastructure: compiled with the reference's unmodified sources (see
+ * oracle/Makefile, target dropin); no GPU.
  *
- *   adaptive_run <in.bin> <maxlevel> <refine_tol> <compress_tol> <nsteps> <every> <ref|gpu> <out.bin>
+ *   adaptive_run <in.bin> <maxlevel> <refine_tol> <compress_tol> <nsteps> <every> ref <out.bin>
  *
  * The grid starts at level 2 (4^3 blocks, periodic, stencil [-1,2)) and is
  * refined with Science::AutomaticRefinement up to <maxlevel>, resampling
@@ -13,24 +14,18 @@
  * hook), then compressed once with Science::AutomaticCompression, as the
  * reference's driver does before its time loop
  * (Glioma/Glioma_ReactionDiffusion.cpp:311-313).  Then <nsteps> RD steps,
- * with Science::AutomaticRefinement after every <every> steps (the driver
- * re-adapts at its dump times, :319-331; interpolation by the reference's
- * own splitter, no resampling).
- *   ref: each step is the reference's pipeline_process + process
- *        (:176-187, threaded TBB stand-in);
- *   gpu: the leaves stay on the device while the grid does not change: an
- *        upload of the topology and fields (gbfk_mrag::Device) after each
- *        refinement, gbfk_rd_step(every), then the wavelet details on the
- *        device (gbfk_fwt_details); phi goes back to the host grid only when
- *        some block qualifies for refinement (and at the end).
+ * each the reference's pipeline_process + process (:176-187, threaded TBB
+ * stand-in); after every <every> steps the grid re-adapts: one loop of
+ * Science::AutomaticRefinement (as the driver's in-loop call, :325) and
+ * Science::AutomaticCompression to convergence (the driver's commented-out
+ * call, :326), interpolation by the reference's own splitter and collapser.
  * Coefficients: Dw = 0.2 cm^2/day on L = 25.6 cm, Dg = Dw/10, rho = 0.05/day,
  * dt = the reference's CFL formula (:304-307) with h of the finest level.
  *
  * Prints one JSON line (blocks and a hash of the sorted (level, index) list
- * after every adaptation; seconds spent stepping, uploads included; seconds
- * of the uploads and of the host refinements) and writes phi sampled on
- * the finest uniform grid (each finest cell takes the value of the leaf cell
- * that covers it) as int32 n + n^3 float64, x fastest.
+ * after every adaptation; seconds spent stepping and adapting) and writes phi
+ * sampled on the finest uniform grid (each finest cell takes the value of the
+ * leaf cell that covers it) as int32 n + n^3 float64, x fastest.
  */
 #include <sys/time.h>
 
@@ -43,7 +38,6 @@
 #include <vector>
 
 #include "Glioma_Types.h"
-#include "gbfk_mrag.hpp"
 
 static int maxStencil[2][3] = {{-1, -1, -1}, {+2, +2, +2}};
 
@@ -140,15 +134,14 @@ static void ref_step(Grid<W, B> &grid, BlockProcessing &bp, Real Dw, Real Dg, Re
 int main(int argc, char **argv)
 {
     if (argc != 9)
-        die("usage: adaptive_run <in.bin> <maxlevel> <refine_tol> <compress_tol> <nsteps> <every> <ref|gpu> "
-            "<out.bin>");
+        die("usage: adaptive_run <in.bin> <maxlevel> <refine_tol> <compress_tol> <nsteps> <every> ref <out.bin>");
     read_dense(argv[1]);
     const int maxLevel = atoi(argv[2]);
     const double rtol = atof(argv[3]), ctol = atof(argv[4]);
     const int nsteps = atoi(argv[5]), every = atoi(argv[6]);
     const std::string mode = argv[7];
     if (g_n != 8 << maxLevel) die("the dense input must have 8 * 2^maxlevel cells per direction");
-    if (every <= 0 || nsteps < 0 || (mode != "ref" && mode != "gpu")) die("bad arguments");
+    if (every <= 0 || nsteps < 0 || mode != "ref") die("bad arguments");
 
     Refiner_SpaceExtension refiner(1, maxLevel);
     Compressor compressor(1);
@@ -173,53 +166,25 @@ int main(int argc, char **argv)
     hashes.push_back(leaves_hash(grid, nb0));
     nblocks.push_back(nb0);
 
-    /* room for every leaf the finest level allows; created before the
-     * timed loop (context creation is not stepping) */
-    gbfk_mrag::Device *dev = mode == "gpu" ? new gbfk_mrag::Device((1 << (3 * maxLevel)) + 64) : NULL;
     BlockProcessing ref;
-    double t_step = 0, t_upload = 0, t_adapt = 0;
-    int n_uploads = 0, n_refines = 0;
+    double t_step = 0, t_adapt = 0;
     long long cell_updates = 0;
     for (int done = 0; done < nsteps;) {
         const int k = std::min(every, nsteps - done);
-        std::vector<BlockInfo> vInfo = grid.getBlocksInfo();
+        const int leaves = (int)grid.getBlocksInfo().size();
         const double t0 = now();
-        bool refine = true;
-        if (mode == "ref") {
-            for (int s = 0; s < k; s++) ref_step(grid, ref, Dw, Dg, rho, dt);
-        } else {
-            if (!dev->same_leaves(vInfo)) {
-                const double tu = now();
-                dev->upload(vInfo, grid.getBlockCollection(), grid.getBoundaryInfo());
-                t_upload += now() - tu;
-                n_uploads++;
-            }
-            gbfk_mrag::check(dev->ctx, gbfk_rd_step(dev->ctx, Dw, Dg, rho, dt, k, 1), "gbfk_rd_step");
-            /* AutomaticRefinement refines the blocks below maxlevel whose
-             * detail is >= the tolerance (MRAGScienceCore.h:59-84); with
-             * the details computed on the device (bit-identical), the
-             * host grid needs phi back only when some block qualifies */
-            std::vector<double> det(vInfo.size());
-            gbfk_mrag::check(dev->ctx, gbfk_fwt_details(dev->ctx, &det[0]), "gbfk_fwt_details");
-            refine = false;
-            for (size_t i = 0; i < vInfo.size(); i++)
-                if (vInfo[i].level < maxLevel && det[i] >= rtol) refine = true;
-            if (refine || done + k >= nsteps) dev->download_phi(vInfo, grid.getBlockCollection());
-        }
+        for (int s = 0; s < k; s++) ref_step(grid, ref, Dw, Dg, rho, dt);
         t_step += now() - t0;
-        cell_updates += (long long)k * (long long)vInfo.size() * 512;
+        cell_updates += (long long)k * (long long)leaves * 512;
         done += k;
-        if (refine) {
-            const double ta = now();
-            Science::AutomaticRefinement<0, 0>(grid, blockfwt, rtol, maxLevel, 1, NULL);
-            t_adapt += now() - ta;
-            n_refines++;
-        }
+        const double ta = now();
+        Science::AutomaticRefinement<0, 0>(grid, blockfwt, rtol, maxLevel, 1, NULL);
+        Science::AutomaticCompression<0, 0>(grid, blockfwt, ctol, -1, NULL);
+        t_adapt += now() - ta;
         int nb = 0;
         hashes.push_back(leaves_hash(grid, nb));
         nblocks.push_back(nb);
     }
-    delete dev;
 
     /* phi on the finest uniform grid */
     const int n = g_n;
@@ -248,10 +213,8 @@ int main(int argc, char **argv)
     fclose(f);
 
     printf("{\"mode\": \"%s\", \"real_bytes\": %d, \"maxlevel\": %d, \"steps\": %d, \"every\": %d, \"dt\": %.17g, "
-           "\"step_seconds\": %.6f, \"upload_seconds\": %.6f, \"uploads\": %d, \"adapt_seconds\": %.6f, "
-           "\"refinements\": %d, \"cell_updates\": %lld, \"blocks\": [",
-           mode.c_str(), (int)sizeof(Real), maxLevel, nsteps, every, (double)dt, t_step, t_upload, n_uploads,
-           t_adapt, n_refines, cell_updates);
+           "\"step_seconds\": %.6f, \"adapt_seconds\": %.6f, \"cell_updates\": %lld, \"blocks\": [",
+           mode.c_str(), (int)sizeof(Real), maxLevel, nsteps, every, (double)dt, t_step, t_adapt, cell_updates);
     for (size_t i = 0; i < nblocks.size(); i++) printf("%s%d", i ? ", " : "", nblocks[i]);
     printf("], \"hashes\": [");
     for (size_t i = 0; i < hashes.size(); i++) printf("%s\"%016llx\"", i ? ", " : "", hashes[i]);

@@ -242,7 +242,7 @@ def ref_uniform(pw, pg, phi, Dw, Dg, rho, dt, nsteps, precision="f64", threads=N
     n = pw.shape[0]
     env = dict(os.environ)
     if threads:
-        env["GBFK_ORACLE_THREADS"] = str(threads)
+        env["GBFK_TBB_THREADS"] = str(threads)
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         _write_dense(fin, pw, pg, phi)
@@ -267,7 +267,7 @@ def ref_time(pw, pg, phi, Dw, Dg, rho, dt, nsteps, precision="f32", threads=None
     returns its JSON record."""
     env = dict(os.environ)
     if threads:
-        env["GBFK_ORACLE_THREADS"] = str(threads)
+        env["GBFK_TBB_THREADS"] = str(threads)
     with tempfile.TemporaryDirectory() as td:
         fin = os.path.join(td, "in.bin")
         _write_dense(fin, pw, pg, phi)
@@ -369,7 +369,7 @@ def ref_topology(base_bpd, maxlevel, refine_tol, every, precision="f64"):
         out = os.path.join(td, "topo.bin")
         r = subprocess.run([str(REF_DIR / f"topo_harness_{precision}"), str(int(base_bpd)), str(int(maxlevel)),
                             _fmt(refine_tol), str(int(every)), out], check=True, capture_output=True, text=True,
-                           env=dict(os.environ, GBFK_ORACLE_THREADS="1"))
+                           env=dict(os.environ, GBFK_TBB_THREADS="1"))
         res = read_topology_dump(out)
     res["summary"] = json.loads(r.stdout.strip().splitlines()[-1])
     return res
@@ -400,7 +400,7 @@ def ref_uq_dump(prefix, tumor_ic, refine_tol, compress_tol, precision="f64", sig
     with tempfile.TemporaryDirectory() as td:
         r = subprocess.run([str(REF_DIR / f"uq_harness_{precision}"), os.fspath(prefix),
                             *(_fmt(v) for v in tumor_ic), _fmt(refine_tol), _fmt(compress_tol), td, _fmt(sigma)],
-                           check=True, capture_output=True, text=True, env=dict(os.environ, GBFK_ORACLE_THREADS="1"))
+                           check=True, capture_output=True, text=True, env=dict(os.environ, GBFK_TBB_THREADS="1"))
         res = read_topology_dump(os.path.join(td, "leaves.bin"))
         res["dump"] = read_matrix3d(os.path.join(td, "HGG_data.dat"))
     res["summary"] = json.loads(r.stdout.strip().splitlines()[-1])

@@ -35,7 +35,7 @@ def test_dropin_on_reference_adaptive_grid(gbfk_lib, prec):
             for a in (pw, pg, c0):
                 f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
         r = subprocess.run([str(exe), fin, str(maxlevel), "1e-3", "20"], capture_output=True, text=True,
-                           timeout=600, env=dict(os.environ, GBFK_ORACLE_THREADS=str(os.cpu_count() or 1)))
+                           timeout=600, env=dict(os.environ, GBFK_TBB_THREADS=str(os.cpu_count() or 1)))
     assert r.returncode == 0, r.stderr[-2000:]
     rec = json.loads(r.stdout.strip().splitlines()[-1])
     assert len(rec["levels"]) >= 2, rec

@@ -19,7 +19,7 @@ def test_flatten_matches_the_serial_layout(maxlevel, rtol, ctol, threads):
     if not EXE.exists():
         pytest.skip("oracle/_ref/flatten_check is built only where the reference sources are")
     r = subprocess.run([str(EXE), str(maxlevel), rtol, ctol, str(threads)], capture_output=True, text=True,
-                       timeout=300, env=dict(os.environ, GBFK_ORACLE_THREADS="2"))
+                       timeout=300, env=dict(os.environ, GBFK_TBB_THREADS="2"))
     rec = json.loads(r.stdout.strip().splitlines()[-1])
     print(json.dumps(rec))
     assert r.returncode == 0 and rec["ok"], rec
