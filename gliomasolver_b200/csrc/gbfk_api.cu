@@ -1266,8 +1266,7 @@ struct Adjoint {
     gbfk_ctx *ctx;
     PoolView<Real> v;
     size_t fbytes;
-    Real *T0, *T1, *T2, *LAM, *MU;
-    unsigned char *FL;
+    Real *T0, *T1, *T2, *LAM;
     std::vector<Real *> slots;
     double *grad_acc;
     Real rho;
@@ -1329,13 +1328,27 @@ struct Adjoint {
             cur = out;
         }
     }
+    // the adjoint state between launches (double-buffered); `latest` is the
+    // set the last launch wrote
+    AdjBuffers sets[2];
+    int latest = 0;
+    // one adjoint step through the forward step from phi_k (one launch)
     void adjoint_step(const Real *phi_k)
     {
         if (err != cudaSuccess) return;
-        err = launch_adjoint_step<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, phi_k, LAM, MU, FL, rho,
-                                        dt, Dw, grad_acc, ctx->stream);
+        err = launch_adjoint_fused<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, phi_k, LAM, sets[latest],
+                                         sets[latest ^ 1], asteps == 0 ? 1 : 0, rho, dt, Dw, grad_acc, ctx->stream);
+        latest ^= 1;
+        ctx->launches++;
         asteps++;
-        ctx->launches += 2;
+    }
+    // lambda_0 into LAM after the sweep (LAM already holds it when no step ran)
+    void finish()
+    {
+        if (err != cudaSuccess || asteps == 0) return;
+        err = launch_adjoint_fused<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, nullptr, LAM,
+                                         sets[latest], sets[latest ^ 1], 2, rho, dt, Dw, grad_acc, ctx->stream);
+        ctx->launches++;
     }
     static double beta(int c, int r)  // C(c + r, c) = C(c + r, r), capped; 0 for r < 0
     {
@@ -1437,13 +1450,16 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     A.rho = (Real)p->rho;
     A.dt = p->dt;
     A.Dw = (double)(Real)p->Dw;
-    // buffers: X0, F, T0, T1, T2, LAM, MU, cell flags + block tails, gradient
-    // partials, x0-gradient partials, then the checkpoints; kept in the
-    // context between calls
+    // buffers: X0, F, T0, T1, T2, LAM, mu and cell flags + block status of
+    // adjoint set 0, gradient partials, x0-gradient partials, the
+    // checkpoints, then mu and flags of set 1 and the self terms of both
+    // sets; kept in the context between calls
     const int xparts = 148 * 4;
-    const size_t sizes[10] = {A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes,
+    const size_t selfbytes = (size_t)nb * kBS3 * sizeof(double);
+    const size_t sizes[15] = {A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes,
                               (size_t)nb * kAdjFlagBytesPerBlock, (size_t)nb * kGradSlots * sizeof(double),
-                              (size_t)xparts * 6 * sizeof(double)};
+                              (size_t)xparts * 6 * sizeof(double), 0, A.fbytes,
+                              (size_t)nb * kAdjFlagBytesPerBlock, selfbytes, selfbytes};
     auto release = [&]() {
         cudaStreamSynchronize(ctx->stream);
         for (void *q : ctx->adj_mem)
@@ -1456,9 +1472,9 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     if (ctx->adj_fbytes != A.fbytes || ctx->adj_nblocks != nb || ctx->adj_nsnap < p->nsnapshots) {
         release();
         // the work fields one by one, the checkpoints in one allocation
-        ctx->adj_mem.assign(11, nullptr);
-        for (size_t i = 0; i < 11 && e == cudaSuccess; i++)
-            e = cudaMalloc(&ctx->adj_mem[i], i < 10 ? sizes[i] : A.fbytes * (size_t)p->nsnapshots);
+        ctx->adj_mem.assign(15, nullptr);
+        for (size_t i = 0; i < 15 && e == cudaSuccess; i++)
+            e = cudaMalloc(&ctx->adj_mem[i], i != 10 ? sizes[i] : A.fbytes * (size_t)p->nsnapshots);
         if (e != cudaSuccess) {
             cudaGetLastError();
             release();
@@ -1474,9 +1490,11 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     A.T1 = (Real *)ctx->adj_mem[3];
     A.T2 = (Real *)ctx->adj_mem[4];
     A.LAM = (Real *)ctx->adj_mem[5];
-    A.MU = (Real *)ctx->adj_mem[6];
-    A.FL = (unsigned char *)ctx->adj_mem[7];
     A.grad_acc = (double *)ctx->adj_mem[8];
+    for (int k = 0; k < 2; k++) {
+        unsigned char *fl = (unsigned char *)ctx->adj_mem[k ? 12 : 7];
+        A.sets[k] = {ctx->adj_mem[k ? 11 : 6], (double *)ctx->adj_mem[13 + k], fl, fl + (size_t)nb * kBS3};
+    }
     double *xpart = (double *)ctx->adj_mem[9];
     A.slots.assign(p->nsnapshots, nullptr);
     for (int i = 0; i < p->nsnapshots; i++) A.slots[i] = (Real *)((char *)ctx->adj_mem[10] + A.fbytes * (size_t)i);
@@ -1546,17 +1564,15 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     if (e == cudaSuccess) {
         e = launch_loss_grad<Real>(bpd, F, ctx->d_t1c, ctx->d_flair, p->t1_uc, p->t2_uc, p->slope, A.LAM, ctx->stream);
         ctx->launches++;
-        // dL/dphi at the horizon is written in every block
-        if (e == cudaSuccess) e = cudaMemsetAsync(A.FL + (size_t)nb * (kBS3 + 1), 0, (size_t)nb, ctx->stream);
     }
-    // reverse sweep; then the zeros of the blocks where dL/dphi_0 vanishes
+    // reverse sweep, then lambda_0 into LAM
     if (e == cudaSuccess) {
         A.reverse_chain(0, p->nsteps, p->nsnapshots, X0);
         e = A.err;
     }
     if (e == cudaSuccess) {
-        e = launch_adjoint_unsparse<Real>(A.v, A.FL, A.LAM, ctx->stream);
-        ctx->launches++;
+        A.finish();
+        e = A.err;
     }
     // parameter gradients
     std::vector<double> acc((size_t)nb * kGradSlots);

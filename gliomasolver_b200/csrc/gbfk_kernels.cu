@@ -516,28 +516,39 @@ cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigne
 // switch.  The switches (dom, the doubling, the clamp) are piecewise constant
 // in phi and are held fixed (their derivative is taken as 0), and rounding is
 // treated as exact.  Given lambda' = dL/dphi', one adjoint step forms
-//   mu_i     = lambda'_i * [0 < pre_i <= 1]                      (adj_mu)
+//   mu_i     = lambda'_i * [0 < pre_i <= 1]
 //   lambda_j = mu_j + dt * ( dom_j mu_j (-ih2 sum_k H~_jk + rho (1 - 2 phi_j))
-//                           + ih2 sum_{i nbr j} dom_i mu_i H~_ij )  (adj_lambda)
+//                           + ih2 sum_{i nbr j} dom_i mu_i H~_ij )
 // and accumulates dL/drho += sum_i mu_i dt dom_i phi_i (1 - phi_i) and
 // dL/dDw += sum_i mu_i dt dom_i (diffusive part of r_i) / Dw (the face
 // coefficients are homogeneous of degree 1 in (Dw, Dg = 0.1 Dw)).
-// adj_mu recomputes the forward step of its block exactly like step_block and
-// records per cell: bit 0 = dom, bit 1+k = coefficient k doubled; and per
-// block whether any of its cells is inside the domain.  A block with no such
-// cell has mu = lambda' [0 < phi <= 1], no gradient terms and, unless a face
-// neighbour has a domain cell, lambda = mu: both kernels take that short
-// path without the halo, the coefficients or the reductions.
-// lambda and mu are block-sparse: mu (and so lambda) vanishes wherever
-// pre = 0, i.e. outside the tumour's support, so after the first adjoint
-// step most blocks are zero.  A block whose lambda' is zero in every cell
-// (lam_zero) has mu = 0 without a look at the forward state; a block whose
-// mu is zero records kAdjMuZero and writes neither mu nor flags; lambda of a
-// block is zero when its mu is and no face neighbour contributes, which
-// adj_lambda records in lam_zero instead of writing the cells.  Every value
-// equals the dense computation's (a zero block's cells are +0 where the
-// dense kernels could produce -0: a sign of zero that no later product or
-// sum turns into a different number).
+//
+// One launch per adjoint step (adj_fused_kernel): lambda_{k+1} of a block
+// needs mu_{k+1} of the block and of its face neighbours, and mu_k of the
+// block needs only lambda_{k+1} of the block itself and the forward state
+// phi_k.  So the launch for step k first forms lambda_{k+1} in registers
+// (phase A, from the mu, cell flags, block status and per-cell "self" term
+// of step k + 1 that the previous launch stored), then recomputes the
+// forward step of its block exactly like step_block (phase B) and forms
+// mu_k, the cell flags (bit 0 = dom, bit 1 + k = coefficient k doubled), the
+// block status, the self term of step k and the gradient partials, and
+// stores those for the next launch (double-buffered: neighbours still read
+// the previous set during this launch).  lambda itself is written only by a
+// final launch (lambda_0); the first launch reads lambda_N, the loss
+// gradient, instead of phase A.  The self term of a domain cell j is
+//   self_j = mu_j * (-ih2 * sum_k H~_jk + rho * (1 - 2 phi_j))
+// (0 elsewhere), kept in double, and phase A forms
+//   lambda_j = mu_j + dt * ((0 + self_j) + sum_{i nbr j} ih2 H~_ij mu_i).
+// A block with no domain cell has mu = lambda' [0 < phi <= 1], no gradient
+// or self terms and, unless a face neighbour has a domain cell, lambda = mu.
+// The state is block-sparse: mu (and so lambda) vanishes wherever pre = 0,
+// i.e. outside the tumour's support.  A block whose lambda_{k+1} is zero (its
+// own status says mu_{k+1} = 0 and no face neighbour contributes) gets
+// mu_k = 0 without a look at the forward state; a block whose mu is zero
+// records kAdjMuZero and writes neither mu, flags nor self terms.  Every
+// value equals the dense computation's (a zero block's cells are +0 where
+// the dense formulas could produce -0: a sign of zero that no later product
+// or sum turns into a different number).
 
 __device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
 {
@@ -547,82 +558,192 @@ __device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
     s = t;
 }
 
-// Per-block status of an adjoint step, written by adj_mu: exactly one of
-// 0 (mu not zero, no domain cell), kAdjDom (mu not zero, a domain cell) and
-// kAdjMuZero (mu is zero in every cell; its mu values and cell flags are not
+// Per-block status of an adjoint step: exactly one of 0 (mu not zero, no
+// domain cell), kAdjDom (mu not zero, a domain cell) and kAdjMuZero (mu is
+// zero in every cell; its mu values, cell flags and self terms are not
 // written, and the block contributes nothing to any lambda).
 constexpr unsigned char kAdjDom = 1;
 constexpr unsigned char kAdjMuZero = 2;
 
-template <typename Real>
-__device__ __forceinline__ bool nonzero4(const Vec4<Real> &a)
-{
-    return a.v[0] != (Real)0 || a.v[1] != (Real)0 || a.v[2] != (Real)0 || a.v[3] != (Real)0;
-}
+struct AdjSet {
+    void *mu;               // Real per cell (pool order)
+    double *self;           // per cell
+    unsigned char *flags;   // per cell: bit 0 dom, bit 1 + k coefficient k doubled
+    unsigned char *status;  // per block: 0, kAdjDom or kAdjMuZero
+};
 
-template <typename Real>
-__global__ void __launch_bounds__(128)
-adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
-              const double *__restrict__ ih2blk, const Real *__restrict__ phi, const Real *__restrict__ lam_next,
-              const unsigned char *__restrict__ lam_zero, Real *__restrict__ mu, unsigned char *__restrict__ flags,
-              unsigned char *__restrict__ status, Real rho, double dt, double inv_Dw, double *__restrict__ grad_acc)
+// Cell mapping of the fused adjoint step: thread t owns the column x = t % 8,
+// y = (t / 8) % 8 at z = 4 (t / 64) + i, i = 0..3, so that a warp reads 32
+// consecutive cells of a plane from global memory; its lab rows are 24 Reals
+// apart (planes 240), which spreads the four rows a warp touches over all 32
+// shared-memory banks for every neighbour offset (with 16-Real rows, as the
+// one-CTA-per-block kernels use, rows y and y + 2 share banks).
+constexpr int kAPitch = 24;
+constexpr int kAPlane = kAPitch * kLab;
+constexpr int kALab = kAPlane * kLab;
+
+__device__ __forceinline__ int lab_a(int x, int y, int z) { return (x + 1) + kAPitch * (y + 1) + kAPlane * (z + 1); }
+
+// resident CTAs per SM the fused adjoint step's register allocation targets
+#ifndef GBFK_ADJ_MIN_BLOCKS
+#define GBFK_ADJ_MIN_BLOCKS 8
+#endif
+
+template <typename Real, int kMode>  // kMode: 0 middle, 1 first (lambda_N given), 2 last (write lambda_0)
+__global__ void __launch_bounds__(128, sizeof(Real) == 4 ? GBFK_ADJ_MIN_BLOCKS : 8)
+adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
+                 const double *__restrict__ ih2blk, const Real *__restrict__ phi, Real *__restrict__ lam,
+                 AdjSet prev, AdjSet out, Real rho, double dt, double inv_Dw, double *__restrict__ grad_acc)
 {
-    __shared__ __align__(16) Real ph[kStepLab];
+    __shared__ __align__(16) Real sm[kALab];  // phase A: mu of step k+1; phase B: phi_k
+    __shared__ unsigned char sfl[kALab];
+    __shared__ unsigned char sst[8];
     __shared__ double red[4][4];
     pdl_wait_then_release();
     const int blk = blockIdx.x, t = threadIdx.x;
-    if (lam_zero[blk]) {
-        // lambda' = 0 in the block: mu = 0 whatever the step does, no gradient terms
-        if (t == 0) status[blk] = kAdjMuZero;
-        return;
-    }
     const int64_t base = slot_of(v, blk) * kBS3;
-    const int x4 = (t & 1) * 4, y = (t >> 1) & 7, z = t >> 4;
-    const int c0 = x4 + kBS * (y + kBS * z);
-    const int l0 = lab_p(x4, y, z);
-    Vec4<Real> p;
-    p.load(phi + base + c0);
+    const int x = t & 7, y = (t >> 3) & 7, z0 = (t >> 6) * 4;
+    const int c0 = x + kBS * (y + kBS * z0);  // cell i is c0 + 64 i
+    const int l0 = lab_a(x, y, z0);            // lab cell i is l0 + kAPlane i
+    const double ih2 = ih2blk[blk];
+    const Real *Hb = H + (int64_t)blk * kFacesPerBlock;
+    const int ln[6] = {-1, 1, -kAPitch, kAPitch, -kAPlane, kAPlane};
+
+    // ---- phase A: lambda_{k+1} of this block -------------------------------
+    Real lamv[4];
+    if (kMode == 1) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) lamv[i] = lam[base + c0 + 64 * i];
+    } else {
+        if (t < 7) sst[t] = prev.status[t == 6 ? blk : face_neighbour(v, blk, t)];
+        __syncthreads();
+        const unsigned self = sst[6];
+        bool contrib = false;
+#pragma unroll
+        for (int f = 0; f < 6; f++) contrib |= sst[f] == kAdjDom;
+        if ((self & kAdjMuZero) && !contrib) {
+            // lambda_{k+1} = 0 in the block: mu_k = 0 whatever the step does
+            if (kMode == 2) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) lam[base + c0 + 64 * i] = (Real)0;
+            } else if (t == 0) {
+                out.status[blk] = kAdjMuZero;
+            }
+            return;
+        }
+        const Real *mu_p = (const Real *)prev.mu;
+        const bool own = !(self & kAdjMuZero);
+        Real m[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) m[i] = own ? mu_p[base + c0 + 64 * i] : (Real)0;
+        if (!(self & kAdjDom) && !contrib) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) lamv[i] = m[i];  // no domain cell and no contribution: lambda = mu
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                sm[l0 + kAPlane * i] = m[i];
+                sfl[l0 + kAPlane * i] = own ? prev.flags[base + c0 + 64 * i] : (unsigned char)0;
+            }
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                const int q = t + 128 * i;
+                const int f = q >> 6, pc = q & 63;
+                int lx, ly, lz, sc;
+                face_cell(f, pc, lx, ly, lz, sc);
+                const int l = lab_a(lx, ly, lz);
+                if (sst[f] == kAdjDom) {
+                    const int nb = face_neighbour(v, blk, f);
+                    sm[l] = mu_p[(int64_t)nb * kBS3 + sc];
+                    sfl[l] = prev.flags[(int64_t)nb * kBS3 + sc];
+                } else {
+                    sm[l] = (Real)0;
+                    sfl[l] = 0;
+                }
+            }
+            double sf[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) sf[i] = (self & kAdjDom) ? prev.self[base + c0 + 64 * i] : 0.;
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int z = z0 + i, l = l0 + kAPlane * i;
+                const int rx = (z * 8 + y) * 9 + x, ry = 576 + (z * 9 + y) * 8 + x, rz = 1152 + (z * 8 + y) * 8 + x;
+                const double hf[6] = {(double)Hb[rx], (double)Hb[rx + 1], (double)Hb[ry], (double)Hb[ry + 8],
+                                      (double)Hb[rz], (double)Hb[rz + 64]};
+                double acc = 0;
+                acc += sf[i];
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    const unsigned fi = sfl[l + ln[k]];
+                    if (!(fi & 1u)) continue;
+                    const double hik = ((fi >> (1 + (k ^ 1))) & 1u) ? 2. * hf[k] : hf[k];
+                    acc += ih2 * hik * (double)sm[l + ln[k]];
+                }
+                lamv[i] = (Real)((double)m[i] + dt * acc);
+            }
+            __syncthreads();  // sm and sfl are reused below
+        }
+        if (kMode == 2) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) lam[base + c0 + 64 * i] = lamv[i];
+            return;
+        }
+    }
+
+    // ---- phase B: mu_k, cell flags, status and self term of step k --------
+    Real p[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) p[i] = phi[base + c0 + 64 * i];
     const unsigned char bt = v.btype[blk];
     unsigned mw[4];
     if (bt == kBlockMixed) {
-        for (int i = 0; i < 4; i++) mw[i] = meta[base + c0 + i];
+#pragma unroll
+        for (int i = 0; i < 4; i++) mw[i] = meta[base + c0 + 64 * i];
     } else {
-        const unsigned m = bt == kBlockEmpty ? kMetaAllEmpty : kMetaAllTissue;
-        mw[0] = mw[1] = mw[2] = mw[3] = m;
+        const unsigned mm = bt == kBlockEmpty ? kMetaAllEmpty : kMetaAllTissue;
+        mw[0] = mw[1] = mw[2] = mw[3] = mm;
     }
     bool doms[4], any = false;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const Real ph0 = p.v[i];
+        const Real ph0 = p[i];
         const unsigned cls = mw[i] & 3u;
         if (cls == kTissue && ph0 >= (Real)0) doms[i] = true;
         else if (cls == kEmpty) doms[i] = ph0 > (Real)0;
         else {
             Real pw, pg;
-            lab_pwpg(v, blk, base, x4 + i, y, z, pw, pg);
+            lab_pwpg(v, blk, base, x, y, z0 + i, pw, pg);
             doms[i] = in_domain(pw, pg, ph0);
         }
         any |= doms[i];
     }
+    Real *mu_o = (Real *)out.mu;
     if (!__syncthreads_or(any)) {
-        // no cell inside the domain: dphidt = 0, pre = phi, no gradient terms
-        Vec4<Real> lam, out;
-        lam.load(lam_next + base + c0);
+        // no cell inside the domain: dphidt = 0, pre = phi, no gradient or self terms
+        Real o[4];
+        bool nz = false;
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-            const Real pre = to_real<Real>(__dadd_rn((double)p.v[i], __dmul_rn(dt, 0.)));
-            out.v[i] = (pre > (Real)0 && pre <= (Real)1) ? lam.v[i] : (Real)0;
+            const Real pre = to_real<Real>(__dadd_rn((double)p[i], __dmul_rn(dt, 0.)));
+            o[i] = (pre > (Real)0 && pre <= (Real)1) ? lamv[i] : (Real)0;
+            nz |= o[i] != (Real)0;
         }
-        if (!__syncthreads_or(nonzero4(out))) {
-            if (t == 0) status[blk] = kAdjMuZero;
+        if (!__syncthreads_or(nz)) {
+            if (t == 0) out.status[blk] = kAdjMuZero;
             return;
         }
-        out.store(mu + base + c0);
-        *reinterpret_cast<uchar4 *>(flags + base + c0) = make_uchar4(0, 0, 0, 0);
-        if (t == 0) status[blk] = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            mu_o[base + c0 + 64 * i] = o[i];
+            out.flags[base + c0 + 64 * i] = 0;
+        }
+        if (t == 0) out.status[blk] = 0;
         return;
     }
-    p.store(ph + l0);
+    Real *ph = sm;
+#pragma unroll
+    for (int i = 0; i < 4; i++) ph[l0 + kAPlane * i] = p[i];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         const int q = t + 128 * i;
@@ -630,28 +751,28 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
         int lx, ly, lz, sc;
         face_cell(f, pc, lx, ly, lz, sc);
         const int nb = face_neighbour(v, blk, f);
-        ph[lab_p(lx, ly, lz)] = phi[(int64_t)nb * kBS3 + sc];
+        ph[lab_a(lx, ly, lz)] = phi[(int64_t)nb * kBS3 + sc];
     }
     __syncthreads();
-    const Real *Hb = H + (int64_t)blk * kFacesPerBlock;
-    const double ih2 = ih2blk[blk];
     const Real eps = (Real)0.1;
     double grho = 0, grho_c = 0, gdw = 0, gdw_c = 0;
-    Vec4<Real> lam;
-    lam.load(lam_next + base + c0);
-    Vec4<Real> out;
+    bool nz = false;
+    Real o[4];
     unsigned char fl[4];
+    double sfo[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const int x = x4 + i;
-        const Real ph0 = p.v[i];
+        const int z = z0 + i;
+        const Real ph0 = p[i];
         const bool dom = doms[i];
         unsigned char f = dom ? 1 : 0;
         Real dphidt = (Real)0.;
-        double flux_diff = 0;
+        double flux_diff = 0, sdf = 0;
         if (dom) {
-            const int l = l0 + i;
-            Real phn[6] = {ph[l - 1], ph[l + 1], ph[l - kPitch], ph[l + kPitch], ph[l - kPlane], ph[l + kPlane]};
+            const int l = l0 + kAPlane * i;
+            Real phn[6];
+#pragma unroll
+            for (int k = 0; k < 6; k++) phn[k] = ph[l + ln[k]];
             bool low[6];
 #pragma unroll
             for (int k = 0; k < 6; k++) {
@@ -666,9 +787,9 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
                 if (slow) {
                     const int nx = x + (k == 0 ? -1 : k == 1 ? 1 : 0);
                     const int ny = y + (k == 2 ? -1 : k == 3 ? 1 : 0);
-                    const int nz = z + (k == 4 ? -1 : k == 5 ? 1 : 0);
+                    const int nz2 = z + (k == 4 ? -1 : k == 5 ? 1 : 0);
                     Real pw, pg;
-                    lab_pwpg(v, blk, base, nx, ny, nz, pw, pg);
+                    lab_pwpg(v, blk, base, nx, ny, nz2, pw, pg);
                     low[k] = domain_chf(phn[k], pw, pg) < eps;
                 }
             }
@@ -685,32 +806,37 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
 #pragma unroll
             for (int k = 1; k < 6; k++) sin_ = radd(sin_, rmul(df[k], phn[k]));
             const double fluxIn = __dmul_rn(ih2, (double)sin_);
-            const Real sdf = radd(radd(radd(radd(radd(df[0], df[1]), df[2]), df[3]), df[4]), df[5]);
-            const double fluxOut = -__dmul_rn((double)rmul(sdf, ph0), ih2);
+            const Real sdfr = radd(radd(radd(radd(radd(df[0], df[1]), df[2]), df[3]), df[4]), df[5]);
+            const double fluxOut = -__dmul_rn((double)rmul(sdfr, ph0), ih2);
             const double reaction = __dmul_rn((double)rmul(rho, ph0), __dadd_rn(1., -(double)ph0));
             dphidt = to_real<Real>(__dadd_rn(__dadd_rn(fluxOut, fluxIn), reaction));
             flux_diff = fluxOut + fluxIn;
+#pragma unroll
+            for (int k = 0; k < 6; k++) sdf += (double)df[k];
         }
         const Real pre = to_real<Real>(__dadd_rn((double)ph0, __dmul_rn(dt, (double)dphidt)));
         const bool pass = pre > (Real)0 && pre <= (Real)1;
-        const Real m = pass ? lam.v[i] : (Real)0;
-        out.v[i] = m;
+        const Real mv = pass ? lamv[i] : (Real)0;
+        o[i] = mv;
+        nz |= mv != (Real)0;
         fl[i] = f;
+        sfo[i] = dom ? (double)mv * (-ih2 * sdf + (double)rho * (1. - 2. * (double)ph0)) : 0.;
         if (dom && pass) {
-            neumaier_add(grho, grho_c, (double)m * dt * (double)ph0 * (1. - (double)ph0));
-            neumaier_add(gdw, gdw_c, (double)m * dt * flux_diff * inv_Dw);
+            neumaier_add(grho, grho_c, (double)mv * dt * (double)ph0 * (1. - (double)ph0));
+            neumaier_add(gdw, gdw_c, (double)mv * dt * flux_diff * inv_Dw);
         }
     }
-    // a block whose mu is zero everywhere writes neither mu nor its flags
-    const bool written = __syncthreads_or(nonzero4(out));
+    // a block whose mu is zero everywhere writes neither mu, flags nor self terms
+    const bool written = __syncthreads_or(nz);
     if (written) {
-        out.store(mu + base + c0);
-        *reinterpret_cast<uchar4 *>(flags + base + c0) = make_uchar4(fl[0], fl[1], fl[2], fl[3]);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            mu_o[base + c0 + 64 * i] = o[i];
+            out.flags[base + c0 + 64 * i] = fl[i];
+            out.self[base + c0 + 64 * i] = sfo[i];
+        }
     }
-    if (t == 0) status[blk] = written ? kAdjDom : kAdjMuZero;
-    // CTA partials (warp shuffles, then the 4 warps in order), accumulated
-    // into this CTA's own slot (deterministic: one writer per slot and
-    // launches are ordered on the stream)
+    if (t == 0) out.status[blk] = written ? kAdjDom : kAdjMuZero;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         const double a0 = __shfl_down_sync(0xffffffffu, grho, off), a1 = __shfl_down_sync(0xffffffffu, grho_c, off);
@@ -742,138 +868,22 @@ adj_mu_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short
     }
 }
 
-// lambda of a block from the mu and cell flags of the block and of its face
-// neighbours.  Only kAdjDom neighbours contribute (the others have no domain
-// cell or mu = 0); a kAdjMuZero block with no contributing neighbour has
-// lambda = 0 and records that in lam_zero instead of writing its cells.
 template <typename Real>
-__global__ void __launch_bounds__(128)
-adj_lambda_kernel(PoolView<Real> v, const Real *__restrict__ H, const double *__restrict__ ih2blk,
-                  const Real *__restrict__ phi, const Real *__restrict__ mu, const unsigned char *__restrict__ flags,
-                  const unsigned char *__restrict__ status, Real *__restrict__ lam, unsigned char *__restrict__ lam_zero,
-                  Real rho, double dt)
-{
-    __shared__ __align__(16) Real smu[kStepLab];
-    __shared__ unsigned char sfl[kStepLab];
-    __shared__ unsigned char sst[8];
-    pdl_wait_then_release();
-    const int blk = blockIdx.x, t = threadIdx.x;
-    // threads 0..5: the face neighbours, thread 6: the block itself
-    if (t < 7) sst[t] = status[t == 6 ? blk : face_neighbour(v, blk, t)];
-    __syncthreads();
-    const unsigned self = sst[6];
-    bool contrib = false;
-#pragma unroll
-    for (int f = 0; f < 6; f++) contrib |= sst[f] == kAdjDom;
-    if ((self & kAdjMuZero) && !contrib) {
-        if (t == 0) lam_zero[blk] = 1;
-        return;
-    }
-    if (t == 0) lam_zero[blk] = 0;
-    const int64_t base = slot_of(v, blk) * kBS3;
-    const int x4 = (t & 1) * 4, y = (t >> 1) & 7, z = t >> 4;
-    const int c0 = x4 + kBS * (y + kBS * z);
-    const int l0 = lab_p(x4, y, z);
-    const bool own = !(self & kAdjMuZero);
-    Vec4<Real> m;
-    if (own) m.load(mu + base + c0);
-    else m.v[0] = m.v[1] = m.v[2] = m.v[3] = (Real)0;
-    if (!(self & kAdjDom) && !contrib) {
-        // no domain cell in the block and no contribution from its neighbours: lambda = mu
-        m.store(lam + base + c0);
-        return;
-    }
-    m.store(smu + l0);
-    uchar4 f4 = make_uchar4(0, 0, 0, 0);
-    if (own) f4 = *reinterpret_cast<const uchar4 *>(flags + base + c0);
-    sfl[l0] = f4.x; sfl[l0 + 1] = f4.y; sfl[l0 + 2] = f4.z; sfl[l0 + 3] = f4.w;
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-        const int q = t + 128 * i;
-        const int f = q >> 6, pc = q & 63;
-        int lx, ly, lz, sc;
-        face_cell(f, pc, lx, ly, lz, sc);
-        const int l = lab_p(lx, ly, lz);
-        if (sst[f] == kAdjDom) {
-            const int nb = face_neighbour(v, blk, f);
-            smu[l] = mu[(int64_t)nb * kBS3 + sc];
-            sfl[l] = flags[(int64_t)nb * kBS3 + sc];
-        } else {
-            smu[l] = (Real)0;
-            sfl[l] = 0;
-        }
-    }
-    Vec4<Real> p;
-    if (self & kAdjDom) p.load(phi + base + c0);
-    else p.v[0] = p.v[1] = p.v[2] = p.v[3] = (Real)0;  // no cell has the domain flag
-    __syncthreads();
-    const Real *Hb = H + (int64_t)blk * kFacesPerBlock;
-    const double ih2 = ih2blk[blk];
-    Vec4<Real> out;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int x = x4 + i;
-        const int l = l0 + i;
-        const int rx = (z * 8 + y) * 9 + x, ry = 576 + (z * 9 + y) * 8 + x, rz = 1152 + (z * 8 + y) * 8 + x;
-        const double hf[6] = {(double)Hb[rx], (double)Hb[rx + 1], (double)Hb[ry], (double)Hb[ry + 8],
-                              (double)Hb[rz], (double)Hb[rz + 64]};
-        const int ln[6] = {l - 1, l + 1, l - kPitch, l + kPitch, l - kPlane, l + kPlane};
-        const unsigned fj = sfl[l];
-        const double muj = (double)smu[l];
-        double acc = 0;
-        if (fj & 1u) {
-            double sdf = 0;
-#pragma unroll
-            for (int k = 0; k < 6; k++) sdf += ((fj >> (1 + k)) & 1u) ? 2. * hf[k] : hf[k];
-            const double ph0 = (double)p.v[i];
-            acc += muj * (-ih2 * sdf + (double)rho * (1. - 2. * ph0));
-        }
-#pragma unroll
-        for (int k = 0; k < 6; k++) {
-            const unsigned fi = sfl[ln[k]];
-            if (!(fi & 1u)) continue;
-            // neighbour i sees this cell in direction k^1
-            const double hik = ((fi >> (1 + (k ^ 1))) & 1u) ? 2. * hf[k] : hf[k];
-            acc += ih2 * hik * (double)smu[ln[k]];
-        }
-        out.v[i] = (Real)(muj + dt * acc);
-    }
-    out.store(lam + base + c0);
-}
-
-// zeros into the cells of the lam_zero blocks
-template <typename Real>
-__global__ void __launch_bounds__(128)
-adj_unsparse_kernel(PoolView<Real> v, const unsigned char *__restrict__ lam_zero, Real *__restrict__ lam)
-{
-    const int blk = blockIdx.x;
-    if (!lam_zero[blk]) return;
-    Vec4<Real> z;
-    z.v[0] = z.v[1] = z.v[2] = z.v[3] = (Real)0;
-    z.store(lam + slot_of(v, blk) * kBS3 + threadIdx.x * 4);
-}
-
-template <typename Real>
-cudaError_t launch_adjoint_step(const PoolView<Real> &v, const Real *H, const unsigned short *meta, const double *ih2,
-                                const Real *phi, Real *lam, Real *mu, unsigned char *flags, Real rho, double dt,
-                                double Dw, double *grad_acc, cudaStream_t s)
+cudaError_t launch_adjoint_fused(const PoolView<Real> &v, const Real *H, const unsigned short *meta,
+                                 const double *ih2, const Real *phi, Real *lam, const AdjBuffers &prev,
+                                 const AdjBuffers &out, int mode, Real rho, double dt, double Dw, double *grad_acc,
+                                 cudaStream_t s)
 {
     if (v.nblocks <= 0) return cudaSuccess;
-    unsigned char *status = flags + (int64_t)v.nblocks * kBS3;  // the flag buffer's per-block tail
-    unsigned char *lam_zero = status + v.nblocks;
-    cudaError_t e = launch_pdl(adj_mu_kernel<Real>, v.nblocks, 128, s, v, H, meta, ih2, phi, (const Real *)lam,
-                               (const unsigned char *)lam_zero, mu, flags, status, rho, dt, 1. / Dw, grad_acc);
-    if (e != cudaSuccess) return e;
-    return launch_pdl(adj_lambda_kernel<Real>, v.nblocks, 128, s, v, H, ih2, phi, (const Real *)mu,
-                      (const unsigned char *)flags, (const unsigned char *)status, lam, lam_zero, rho, dt);
-}
-
-template <typename Real>
-cudaError_t launch_adjoint_unsparse(const PoolView<Real> &v, const unsigned char *flags, Real *lam, cudaStream_t s)
-{
-    if (v.nblocks <= 0) return cudaSuccess;
-    adj_unsparse_kernel<Real><<<v.nblocks, 128, 0, s>>>(v, flags + (int64_t)v.nblocks * (kBS3 + 1), lam);
-    return cudaGetLastError();
+    const AdjSet a = {prev.mu, prev.self, prev.flags, prev.status}, b = {out.mu, out.self, out.flags, out.status};
+    if (mode == 1)
+        return launch_pdl(adj_fused_kernel<Real, 1>, v.nblocks, 128, s, v, H, meta, ih2, phi, lam, a, b, rho, dt,
+                          1. / Dw, grad_acc);
+    if (mode == 2)
+        return launch_pdl(adj_fused_kernel<Real, 2>, v.nblocks, 128, s, v, H, meta, ih2, phi, lam, a, b, rho, dt,
+                          1. / Dw, grad_acc);
+    return launch_pdl(adj_fused_kernel<Real, 0>, v.nblocks, 128, s, v, H, meta, ih2, phi, lam, a, b, rho, dt,
+                      1. / Dw, grad_acc);
 }
 
 // dL/du of loss = -(L_T1c + L_FLAIR) (HGG_Likelihood.cpp:136-156) on a
@@ -1299,11 +1309,10 @@ cudaError_t upload_ghost_table()
     template cudaError_t launch_faces<Real>(const PoolView<Real> &, Real, Real, Real *, unsigned short *,       \
                                             unsigned char *, cudaStream_t);                                   \
     template cudaError_t launch_rd_batch_step<Real>(const BatchView<Real> &, int, int, int, cudaStream_t);      \
-    template cudaError_t launch_adjoint_step<Real>(const PoolView<Real> &, const Real *, const unsigned short *,  \
-                                                   const double *, const Real *, Real *, Real *, unsigned char *, \
-                                                   Real, double, double, double *, cudaStream_t);            \
-    template cudaError_t launch_adjoint_unsparse<Real>(const PoolView<Real> &, const unsigned char *, Real *,      \
-                                                       cudaStream_t);                                             \
+    template cudaError_t launch_adjoint_fused<Real>(const PoolView<Real> &, const Real *, const unsigned short *,  \
+                                                    const double *, const Real *, Real *, const AdjBuffers &,      \
+                                                    const AdjBuffers &, int, Real, double, double, double *,       \
+                                                    cudaStream_t);                                                 \
     template cudaError_t launch_loss_grad<Real>(int, const Real *, const unsigned char *, const unsigned char *, \
                                                 double, double, double, Real *, cudaStream_t);               \
     template cudaError_t launch_gaussian_ic<Real>(int, const Real *, const Real *, const double *, double, Real *, \

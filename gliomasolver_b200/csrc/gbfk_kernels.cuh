@@ -165,21 +165,25 @@ cudaError_t launch_likelihood(const double *model, int n, const unsigned char *t
                               const double *pet, const int *roi, int nroi, const LikelihoodParams &p,
                               double *partial, int nparts, double *out, cudaStream_t s);
 
-// Discrete adjoint (uniform grids): one adjoint step through the step that
-// maps phi (input state) to the next state; lam holds dL/dphi' on entry and
-// dL/dphi on exit, block-sparse: a block whose lam_zero byte is 1 is zero in
-// every cell and its values in lam are not read (they are stale);
-// flags: nblocks * 512 + 2 * nblocks bytes of scratch (per-cell switches,
-// then the per-block status of the step, then lam_zero); grad_acc: nblocks *
-// 4 doubles (rho sum/comp, Dw sum/comp).  launch_adjoint_unsparse writes the
-// zeros of the lam_zero blocks into lam.
-constexpr int kAdjFlagBytesPerBlock = kBS3 + 2;
+// Discrete adjoint (uniform grids): one adjoint step per launch
+// (adj_fused_kernel).  The state of an adjoint step kept between launches,
+// double-buffered: per cell mu (Real), the self term (double) and the switch
+// flags, per block the status.  mode 1: the first step, lambda' from lam
+// (the loss gradient); mode 0: lambda' from prev; mode 2: no step, lambda
+// from prev written to lam (lambda_0).  grad_acc: nblocks * 4 doubles (rho
+// sum/comp, Dw sum/comp), accumulated per block.
+constexpr int kAdjFlagBytesPerBlock = kBS3 + 1;  // cell flags, then the block's status
+struct AdjBuffers {
+    void *mu;
+    double *self;
+    unsigned char *flags;
+    unsigned char *status;
+};
 template <typename Real>
-cudaError_t launch_adjoint_step(const PoolView<Real> &v, const Real *H, const unsigned short *meta, const double *ih2,
-                                const Real *phi, Real *lam, Real *mu, unsigned char *flags, Real rho, double dt,
-                                double Dw, double *grad_acc, cudaStream_t s);
-template <typename Real>
-cudaError_t launch_adjoint_unsparse(const PoolView<Real> &v, const unsigned char *flags, Real *lam, cudaStream_t s);
+cudaError_t launch_adjoint_fused(const PoolView<Real> &v, const Real *H, const unsigned short *meta,
+                                 const double *ih2, const Real *phi, Real *lam, const AdjBuffers &prev,
+                                 const AdjBuffers &out, int mode, Real rho, double dt, double Dw, double *grad_acc,
+                                 cudaStream_t s);
 template <typename Real>
 cudaError_t launch_loss_grad(int bpd, const Real *phi, const unsigned char *t1c, const unsigned char *flair,
                              double t1uc, double t2uc, double slope, Real *lam, cudaStream_t s);
