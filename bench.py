@@ -448,11 +448,10 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9, max
     import torch
 
     from gliomasolver_b200 import BlockPool
-    from gliomasolver_b200.anatomy import make_anatomy, tumor_ic
-    from gliomasolver_b200.tmcmc import sample_stage
+    from gliomasolver_b200.anatomy import tumor_ic
+    from gliomasolver_b200.gradcheck import config5_sample
 
     n = 8 * bpd
-    rng = np.random.default_rng(seed)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     t_total, steps_total, fwd_total, recs = 0.0, 0, 0, []
     peak, _ = measured_peak()
@@ -486,7 +485,7 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9, max
         torch.cuda.synchronize()
         return pool, cap_snap
 
-    def one(pool, cap_snap, prec, p_w, p_g, st, masks=None):
+    def one(pool, cap_snap, prec, p_w, p_g, st, rng, masks=None):
         R = np.float32 if prec == "f32" else np.float64
         s = make_schedule(st.Dw_cm2_day, st.rho_day, st.tend_day, L_CM, bpd, prec)
         if max_steps is not None and s.nsteps > max_steps:
@@ -518,9 +517,8 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9, max
     pool, cap32 = open_pool("f32")
     try:
         for i in range(nsamples):
-            p_w, p_g, _ = make_anatomy(n, seed + 100 + i, scale=float(rng.uniform(0.8, 1.2)))
-            st = sample_stage(1, p_w, seed=seed + 200 + i)[0]
-            res, t, k, masks, nsnap = one(pool, cap32, "f32", p_w, p_g, st)
+            p_w, p_g, st, rng = config5_sample(i, n, seed)
+            res, t, k, masks, nsnap = one(pool, cap32, "f32", p_w, p_g, st, rng)
             t_total += t
             steps_total += k
             fwd_total += res["forward_steps"]
@@ -533,7 +531,7 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9, max
     p_w, p_g, st, r32, masks = first
     pool, cap64 = open_pool("f64")
     try:
-        r64 = one(pool, cap64, "f64", p_w, p_g, st, masks)[0]
+        r64 = one(pool, cap64, "f64", p_w, p_g, st, None, masks)[0]
     finally:
         pool.close()
     rel = {k: abs(r32[k] - r64[k]) / max(abs(r64[k]), 1e-300) for k in ("loss", "dDw", "drho")}

@@ -75,6 +75,8 @@ struct gbfk_ctx {
     size_t model_bytes = 0;
     double *d_partial = nullptr;      // likelihood partial sums
     double *d_lik = nullptr;          // 4 results
+    int *d_roi_count = nullptr;       // n^3: how often the ROI lists each voxel (the adjoint's loss weights)
+    size_t roi_count_bytes = 0;
 
     unsigned short *d_meta = nullptr; // max_blocks * 512 meta words, indexed like the pool
     unsigned char *d_btype = nullptr; // nblocks block types
@@ -730,7 +732,8 @@ int gbfk_destroy(gbfk_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     release_topology(ctx);
     void *ptrs[] = {ctx->phi[0], ctx->phi[1], ctx->pw, ctx->pg, ctx->d_nan, ctx->d_stage, ctx->d_ints, ctx->d_meta,
-                    ctx->d_t1c, ctx->d_flair, ctx->d_pet, ctx->d_roi, ctx->d_model, ctx->d_partial, ctx->d_lik};
+                    ctx->d_t1c, ctx->d_flair, ctx->d_pet, ctx->d_roi, ctx->d_model, ctx->d_partial, ctx->d_lik,
+                    ctx->d_roi_count};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (void *p : ctx->adj_mem)
@@ -1556,13 +1559,28 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
         lp.slope = p->slope;
         lp.step_pet = 1;
         lp.step_mri = 1;
-        e = launch_likelihood(ctx->d_model, n, ctx->d_t1c, ctx->d_flair, nullptr, nullptr, 0, lp, ctx->d_partial,
-                              148 * 4, ctx->d_lik, ctx->stream);
+        // with a ROI (HGG_Likelihood.cpp:97-124) the loss sums over its voxels only
+        e = launch_likelihood(ctx->d_model, n, ctx->d_t1c, ctx->d_flair, nullptr, ctx->nroi ? ctx->d_roi : nullptr,
+                              ctx->nroi, lp, ctx->d_partial, 148 * 4, ctx->d_lik, ctx->stream);
         ctx->launches += 3;
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(lik, ctx->d_lik, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    int *roi_count = nullptr;
+    if (e == cudaSuccess && ctx->nroi) {
+        if (ctx->roi_count_bytes < (size_t)n * n * n * sizeof(int)) {
+            if (ctx->d_roi_count) cudaFree(ctx->d_roi_count);
+            ctx->d_roi_count = nullptr;
+            ctx->roi_count_bytes = 0;
+            e = cudaMalloc(&ctx->d_roi_count, (size_t)n * n * n * sizeof(int));
+            if (e == cudaSuccess) ctx->roi_count_bytes = (size_t)n * n * n * sizeof(int);
+        }
+        if (e == cudaSuccess) e = launch_roi_count(n, ctx->d_roi, ctx->nroi, ctx->d_roi_count, ctx->stream);
+        roi_count = ctx->d_roi_count;
+        ctx->launches++;
+    }
     if (e == cudaSuccess) {
-        e = launch_loss_grad<Real>(bpd, F, ctx->d_t1c, ctx->d_flair, p->t1_uc, p->t2_uc, p->slope, A.LAM, ctx->stream);
+        e = launch_loss_grad<Real>(bpd, F, ctx->d_t1c, ctx->d_flair, roi_count, p->t1_uc, p->t2_uc, p->slope, A.LAM,
+                                   ctx->stream);
         ctx->launches++;
     }
     // reverse sweep, then lambda_0 into LAM
@@ -1630,7 +1648,7 @@ extern "C" int gbfk_forward_adjoint(gbfk_ctx *ctx, const gbfk_adjoint_params *p,
     ctx->phi_clamped = false;
     if (!p || !out) return fail(ctx, GBFK_E_INVALID, "forward_adjoint: null argument");
     if (!ctx->uniform || !ctx->have_origin) return fail(ctx, GBFK_E_STATE, "forward_adjoint: needs a uniform power-of-two grid");
-    if (ctx->obs_n != 8 * ctx->bpd || ctx->nroi) return fail(ctx, GBFK_E_STATE, "forward_adjoint: observations must cover the grid (no ROI)");
+    if (ctx->obs_n != 8 * ctx->bpd) return fail(ctx, GBFK_E_STATE, "forward_adjoint: observations must be on the grid");
     if (p->nsteps < 0 || p->nsnapshots < 1 || !(p->slope != 0) || !(p->Dw > 0))
         return fail(ctx, GBFK_E_INVALID, "forward_adjoint: bad parameters");
     CK(cudaSetDevice(ctx->device));

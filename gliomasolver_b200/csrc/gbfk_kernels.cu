@@ -901,8 +901,8 @@ __device__ __forceinline__ double bernoulli_dlog(double u, double uc, double is2
 
 template <typename Real>
 __global__ void loss_grad_kernel(int bpd, const Real *__restrict__ phi, const unsigned char *__restrict__ t1c,
-                                 const unsigned char *__restrict__ flair, double t1uc, double t2uc, double is2,
-                                 Real *__restrict__ lam)
+                                 const unsigned char *__restrict__ flair, const int *__restrict__ roi_count,
+                                 double t1uc, double t2uc, double is2, Real *__restrict__ lam)
 {
     const int n = 8 * bpd;
     const int64_t N = (int64_t)n * n * n;
@@ -912,18 +912,38 @@ __global__ void loss_grad_kernel(int bpd, const Real *__restrict__ phi, const un
         const int bx = (int)(b % bpd), by = (int)((b / bpd) % bpd), bz = (int)(b / ((int64_t)bpd * bpd));
         const int64_t g = (bx * 8 + (c & 7)) + (int64_t)n * ((by * 8 + ((c >> 3) & 7)) + (int64_t)n * (bz * 8 + (c >> 6)));
         const double u = (double)phi[i];
-        lam[i] = (Real)(-(bernoulli_dlog(u, t1uc, is2, t1c[g] != 0) + bernoulli_dlog(u, t2uc, is2, flair[g] != 0)));
+        // a voxel counts as often as the ROI lists it (every voxel once without a ROI)
+        const double w = roi_count ? (double)roi_count[g] : 1.;
+        lam[i] = (Real)(-w * (bernoulli_dlog(u, t1uc, is2, t1c[g] != 0) + bernoulli_dlog(u, t2uc, is2, flair[g] != 0)));
     }
 }
 
 template <typename Real>
 cudaError_t launch_loss_grad(int bpd, const Real *phi, const unsigned char *t1c, const unsigned char *flair,
-                             double t1uc, double t2uc, double slope, Real *lam, cudaStream_t s)
+                             const int *roi_count, double t1uc, double t2uc, double slope, Real *lam, cudaStream_t s)
 {
     const int64_t N = (int64_t)512 * bpd * bpd * bpd;
     int64_t nb = (N + 255) / 256;
     if (nb > 148 * 32) nb = 148 * 32;
-    loss_grad_kernel<Real><<<(int)nb, 256, 0, s>>>(bpd, phi, t1c, flair, t1uc, t2uc, 1. / slope, lam);
+    loss_grad_kernel<Real><<<(int)nb, 256, 0, s>>>(bpd, phi, t1c, flair, roi_count, t1uc, t2uc, 1. / slope, lam);
+    return cudaGetLastError();
+}
+
+// How often each voxel of an n^3 grid appears in a list of (x, y, z) points
+// (count must be zeroed first).
+__global__ void roi_count_kernel(int n, const int *__restrict__ roi, int nroi, int *__restrict__ count)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nroi; k += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&count[roi[3 * k] + (int64_t)n * (roi[3 * k + 1] + (int64_t)n * roi[3 * k + 2])], 1);
+}
+
+cudaError_t launch_roi_count(int n, const int *roi, int nroi, int *count, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(count, 0, (size_t)n * n * n * sizeof(int), s);
+    if (e != cudaSuccess || nroi <= 0) return e;
+    int64_t nb = ((int64_t)nroi + 255) / 256;
+    if (nb > 148 * 32) nb = 148 * 32;
+    roi_count_kernel<<<(int)nb, 256, 0, s>>>(n, roi, nroi, count);
     return cudaGetLastError();
 }
 
@@ -1314,7 +1334,7 @@ cudaError_t upload_ghost_table()
                                                     const AdjBuffers &, int, Real, double, double, double *,       \
                                                     cudaStream_t);                                                 \
     template cudaError_t launch_loss_grad<Real>(int, const Real *, const unsigned char *, const unsigned char *, \
-                                                double, double, double, Real *, cudaStream_t);               \
+                                                const int *, double, double, double, Real *, cudaStream_t);  \
     template cudaError_t launch_gaussian_ic<Real>(int, const Real *, const Real *, const double *, double, Real *, \
                                                   cudaStream_t);                                             \
     template cudaError_t launch_x0_grad<Real>(int, const Real *, const Real *, const double *, double, double *, \

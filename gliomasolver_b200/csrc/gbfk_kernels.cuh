@@ -184,9 +184,12 @@ cudaError_t launch_adjoint_fused(const PoolView<Real> &v, const Real *H, const u
                                  const double *ih2, const Real *phi, Real *lam, const AdjBuffers &prev,
                                  const AdjBuffers &out, int mode, Real rho, double dt, double Dw, double *grad_acc,
                                  cudaStream_t s);
+// dL/dphi of loss = -(L_T1c + L_FLAIR) in pool order; roi_count: NULL (every
+// voxel once) or how often the ROI lists each voxel of the dense grid
 template <typename Real>
 cudaError_t launch_loss_grad(int bpd, const Real *phi, const unsigned char *t1c, const unsigned char *flair,
-                             double t1uc, double t2uc, double slope, Real *lam, cudaStream_t s);
+                             const int *roi_count, double t1uc, double t2uc, double slope, Real *lam, cudaStream_t s);
+cudaError_t launch_roi_count(int n, const int *roi, int nroi, int *count, cudaStream_t s);
 template <typename Real>
 cudaError_t launch_gaussian_ic(int bpd, const Real *pw, const Real *pg, const double x0[3], double sigma, Real *out,
                                cudaStream_t s);

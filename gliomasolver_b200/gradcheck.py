@@ -118,3 +118,18 @@ def synthetic_observations(pool: BlockPool, c0, Dw, rho, dt, nsteps, seed, t1_uc
         m[f] = 1 - m[f]
     pool.set_observations(*masks)
     return masks
+
+
+def config5_sample(i, n=256, seed=5):
+    """Sample i of the batched forward + adjoint workload (config 5): its own
+    seeded anatomy (brain scale U[0.8, 1.2]) and parameters drawn as for a
+    TMCMC stage (Dw log-U[0.02, 0.3] cm^2/day, rho log-U[0.002, 0.2] / day,
+    T U[30, 300] d, x0 a white-matter voxel).  Returns (p_w, p_g, sample,
+    rng), rng seeded for the sample (its label noise)."""
+    from .anatomy import make_anatomy
+    from .tmcmc import sample_stage
+
+    rng = np.random.default_rng([seed, i])
+    p_w, p_g, _ = make_anatomy(n, seed + 100 + i, scale=float(rng.uniform(0.8, 1.2)))
+    st = sample_stage(1, p_w, seed=seed + 200 + i)[0]
+    return p_w, p_g, st, rng

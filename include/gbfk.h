@@ -298,8 +298,9 @@ int gbfk_batch_log_likelihood(gbfk_batch *b, const gbfk_likelihood_params *param
  * differentiates).  Forward solve plus the hand-written discrete adjoint of
  * the fused step on the context's uniform grid, for the loss
  *   loss = -(L_T1c + L_FLAIR)        (HGG_Likelihood.cpp:77-156)
- * of the state at the horizon against the observations (gbfk_set_observations,
- * without ROI).  dt and the step count are held fixed; the piecewise-constant
+ * of the state at the horizon against the observations (gbfk_set_observations;
+ * with a ROI the sums run over its points, each as often as it is listed,
+ * as the likelihood's -bROI does, HGG_Likelihood.cpp:97-124).  dt and the step count are held fixed; the piecewise-constant
  * switches of the step (domain test, no-flux doubling, clamp) are held fixed.
  * States are kept with binomial checkpointing in nsnapshots device buffers;
  * these and seven work fields stay allocated in the context until

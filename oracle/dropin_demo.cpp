@@ -119,6 +119,13 @@ static void restore_phi(Grid<W, B> &grid, const FieldMap &m)
     }
 }
 
+static double now()
+{
+    timeval tv;
+    gettimeofday(&tv, NULL);
+    return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
 static long count_diff(const std::vector<Real> &a, const Real *b, int n)
 {
     long d = 0;
@@ -189,21 +196,48 @@ int main(int argc, char **argv)
         }
     }
 
-    /* 3. RD steps */
-    long step_mismatch_dropin = 0, step_mismatch_resident = 0;
+    /* 3. RD steps: the reference's step loop, the same loop through the drop-in
+     * policy (write-back after every step, then deferred to sync_host), and one
+     * resident gbfk_rd_step call */
+    long step_mismatch_dropin = 0, step_mismatch_deferred = 0, step_mismatch_resident = 0;
     int n_ghost_faces = 0;
+    double t_ref = 0, t_dropin = 0, t_deferred = 0;
+    long dropin_uploads = 0;
     {
+        typedef gbfk_mrag::BlockProcessing_CUDA<B> Policy;
         FieldMap phi0 = snapshot(grid, 0);
         BlockProcessing ref;
+        double t0 = now();
         for (int s = 0; s < steps; s++) rd_step(grid, ref, Dw, Dg, rho, dt);
+        t_ref = now() - t0;
         FieldMap phi_ref = snapshot(grid, 0);
 
         restore_phi(grid, phi0);
-        gbfk_mrag::BlockProcessing_CUDA<B> gpu;
+        Policy gpu;
+        Policy::invalidate();
+        rd_step(grid, gpu, Dw, Dg, rho, dt);  // first step: uploads the leaf set
+        restore_phi(grid, phi0);
+        Policy::invalidate();
+        const long up0 = Policy::uploads();
+        t0 = now();
         for (int s = 0; s < steps; s++) rd_step(grid, gpu, Dw, Dg, rho, dt);
+        t_dropin = now() - t0;
+        dropin_uploads = Policy::uploads() - up0;
         FieldMap phi_gpu = snapshot(grid, 0);
         for (int i = 0; i < nb; i++)
             step_mismatch_dropin += count_diff(phi_ref[vInfo[i].blockID], &phi_gpu[vInfo[i].blockID][0], 512);
+
+        restore_phi(grid, phi0);
+        Policy::invalidate();
+        Policy::deferred_writeback() = true;
+        t0 = now();
+        for (int s = 0; s < steps; s++) rd_step(grid, gpu, Dw, Dg, rho, dt);
+        Policy::sync_host(vInfo, grid.getBlockCollection());
+        t_deferred = now() - t0;
+        Policy::deferred_writeback() = false;
+        FieldMap phi_def = snapshot(grid, 0);
+        for (int i = 0; i < nb; i++)
+            step_mismatch_deferred += count_diff(phi_ref[vInfo[i].blockID], &phi_def[vInfo[i].blockID][0], 512);
 
         restore_phi(grid, phi0);
         dev.upload(vInfo, grid.getBlockCollection(), grid.getBoundaryInfo());
@@ -357,9 +391,12 @@ int main(int argc, char **argv)
     for (std::map<int, int>::iterator it = levels.begin(); it != levels.end(); ++it)
         printf("%s\"%d\": %d", it == levels.begin() ? "" : ", ", it->first, it->second);
     printf("}, \"coarse_fine_faces\": %d, \"fwt_max\": %.6e, \"fwt_mismatch\": %ld, \"steps\": %d, "
-           "\"step_mismatch_dropin\": %ld, \"step_mismatch_resident\": %ld, \"split_parents\": %d, "
+           "\"step_mismatch_dropin\": %ld, \"step_mismatch_deferred\": %ld, \"step_mismatch_resident\": %ld, "
+           "\"reference_step_seconds\": %.6f, \"dropin_step_seconds\": %.6f, \"deferred_step_seconds\": %.6f, "
+           "\"dropin_uploads\": %ld, \"split_parents\": %d, "
            "\"split_mismatch\": %ld, \"collapsed\": %d, \"collapse_mismatch\": %ld}\n",
-           n_ghost_faces, fwt_max, fwt_mismatch, steps, step_mismatch_dropin, step_mismatch_resident, n_split,
-           split_mismatch, n_collapse, collapse_mismatch);
+           n_ghost_faces, fwt_max, fwt_mismatch, steps, step_mismatch_dropin, step_mismatch_deferred,
+           step_mismatch_resident, t_ref, t_dropin, t_deferred, dropin_uploads, n_split, split_mismatch, n_collapse,
+           collapse_mismatch);
     return 0;
 }

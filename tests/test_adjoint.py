@@ -317,3 +317,40 @@ def test_autograd_initial_field():
     assert float(rho.grad) == 2.0 * ref["drho"]
     assert float(Dw.grad) == pytest.approx(2.0 * ref["dDw"] / L ** 2, rel=1e-14)
     pool.close()
+
+
+def test_adjoint_with_a_roi_matches_central_differences():
+    """With a ROI the loss sums over its points only, each as often as it is
+    listed (HGG_Likelihood.cpp:97-124): the FP64 gradients against central
+    differences (relative step 1e-4) of the same ROI loss, and dL/dc0 against
+    the oracle's adjoint of the count-weighted loss gradient."""
+    pool, pw, pg, sched, t1, fl, R = _setup("f64", seed=11)
+    rng = np.random.default_rng(12)
+    pts = rng.integers(0, N, (N ** 3 // 3, 3)).astype(np.int32)
+    roi = np.concatenate([pts, pts[: N ** 3 // 20]])          # some points listed twice
+    pool.set_observations(t1, fl, roi=roi)
+    c0 = tumor_ic(N, (0.51, 0.49, 0.5), pw, pg)
+    Dw, Dg = _coeffs(R, 0.16)
+    rho = 0.07
+    pool.upload_dense("phi", c0)
+    dev = pool.forward_adjoint(Dw, Dg, rho, sched.dt, NSTEPS, sigma=0.0, nsnapshots=5, grad_c0=True, **UC)
+
+    def loss(dw, rh):
+        pool.upload_dense("phi", c0)
+        pool.rd_step(dw, float(R(0.1 * np.float64(dw))), rh, sched.dt, NSTEPS)
+        lik = pool.log_likelihood(**UC)
+        return -(lik[1] + lik[2])
+
+    assert dev["loss"] == pytest.approx(loss(Dw, rho), rel=1e-13)
+    e = 1e-4 * Dw
+    assert dev["dDw"] == pytest.approx((loss(Dw + e, rho) - loss(Dw - e, rho)) / (2 * e), rel=1e-5)
+    e = 1e-4 * rho
+    assert dev["drho"] == pytest.approx((loss(Dw, rho + e) - loss(Dw, rho - e)) / (2 * e), rel=1e-5)
+    count = np.zeros((N, N, N))
+    np.add.at(count, (roi[:, 2], roi[:, 1], roi[:, 0]), 1.0)
+    u = O.rd_steps_dense(pw, pg, c0, Dw, Dg, rho, 1.0 / N, sched.dt, NSTEPS)
+    lam_t = count * O.loss_grad(u, t1, fl, UC["t1_uc"], UC["t2_uc"], UC["slope"])
+    lam0, drho, ddw = O.adjoint_dense(pw, pg, c0, Dw, Dg, rho, 1.0 / N, sched.dt, NSTEPS, lam_t)
+    assert np.linalg.norm(dev["grad_c0"] - lam0) <= 1e-13 * np.linalg.norm(lam0)
+    assert dev["dDw"] == pytest.approx(ddw, rel=1e-12)
+    pool.close()

@@ -41,7 +41,12 @@ def test_dropin_on_reference_adaptive_grid(gbfk_lib, prec):
     assert len(rec["levels"]) >= 2, rec
     assert rec["coarse_fine_faces"] > 0, rec
     assert rec["fwt_max"] > 0
-    for k in ("fwt_mismatch", "step_mismatch_dropin", "step_mismatch_resident", "split_mismatch",
-              "collapse_mismatch"):
+    for k in ("fwt_mismatch", "step_mismatch_dropin", "step_mismatch_deferred", "step_mismatch_resident",
+              "split_mismatch", "collapse_mismatch"):
         assert rec[k] == 0, (k, rec)
+    # the policy keeps phi on the device between topology changes: one upload
+    # of the leaf set for the whole loop
+    assert rec["dropin_uploads"] == 1, rec
+    print({k: rec[k] for k in ("blocks", "steps", "reference_step_seconds", "dropin_step_seconds",
+                               "deferred_step_seconds")})
     assert rec["split_parents"] > 0 and rec["collapsed"] == 1, rec
