@@ -28,7 +28,7 @@ STATUS_CODES = {v: k for k, v in STATUS.items()}
 GBFK_F64, GBFK_F32 = 0, 1
 GBFK_PHI, GBFK_PW, GBFK_PG = 0, 1, 2
 # step kernels (gbfk_set_step_kernel)
-STEP_KERNELS = {"auto": 0, "block": 1, "pipelined": 2}
+STEP_KERNELS = {"auto": 0, "block": 1, "pipelined": 2, "run": 3}
 
 # Every symbol include/gbfk.h declares (checked by the CPU test suite).
 EXPORTS = (

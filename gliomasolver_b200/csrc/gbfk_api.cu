@@ -96,6 +96,14 @@ struct gbfk_ctx {
     int *d_lists = nullptr;
     int n_heavy = 0, n_empty = 0;
     bool lists_valid = false;
+    std::vector<int> h_lists;  // host copy of d_lists
+    // runs of steps in one launch: the CTA count, per CTA the CTAs that own
+    // face neighbours of its blocks (d_run_nbr: offsets, then the lists) and
+    // the step flags
+    int run_ctas = 0;
+    bool run_layout_valid = false;
+    int *d_run_nbr = nullptr;
+    unsigned *d_run_flags = nullptr;
     // phi[cur] is the output of a step: every value +0 <= phi <= 1 or NaN
     // (set only by rd_step; every other writer of phi clears it)
     bool phi_clamped = false;
@@ -193,6 +201,7 @@ void free_topology(gbfk_ctx *c)
     c->static_ghosts_dirty = true;
     c->faces_valid = false;
     c->lists_valid = false;
+    c->run_layout_valid = false;
     c->phi_clamped = false;
 }
 
@@ -203,7 +212,7 @@ void release_topology(gbfk_ctx *c)
     void **ptrs[] = {(void **)&c->d_slot, (void **)&c->d_nbr, &c->d_h, (void **)&c->d_row_ptr, (void **)&c->d_src,
                      &c->d_w, (void **)&c->d_step_rows, (void **)&c->d_all_rows, &c->d_gpw, &c->d_gpg,
                      &c->d_gphi, (void **)&c->d_fwt, &c->d_H, (void **)&c->d_ih2, (void **)&c->d_btype, &c->d_origin,
-                     (void **)&c->d_lists};
+                     (void **)&c->d_lists, (void **)&c->d_run_nbr, (void **)&c->d_run_flags};
     for (void **p : ptrs) {
         if (*p) cudaFree(*p);
         *p = nullptr;
@@ -291,8 +300,9 @@ int ints_scratch(gbfk_ctx *ctx, size_t n)
 }
 
 // The pipelined step's error word (d_nan[1]: bit 0 a wait timed out, bit 1 a
-// work list overflowed); reading it synchronises the stream.  An error is
-// reported once and the word cleared.
+// work list overflowed, bits 3-8 the wait that timed out: launch_rd_run_tma);
+// reading it synchronises the stream.  An error is reported once and the
+// word cleared.
 int check_stage_timeout(gbfk_ctx *ctx)
 {
     unsigned flag = 0;
@@ -300,7 +310,9 @@ int check_stage_timeout(gbfk_ctx *ctx)
     CK(cudaStreamSynchronize(ctx->stream));
     if (flag) {
         CK(cudaMemsetAsync(ctx->d_nan + 1, 0, sizeof(unsigned), ctx->stream));
-        if (flag & 1u) return fail(ctx, GBFK_E_TIMEOUT, "rd_step: a wait of the pipelined step timed out (1 s)");
+        if (flag & (1u | 256u))
+            return fail(ctx, GBFK_E_TIMEOUT, "rd_step: a wait of the pipelined step timed out (1 s; error word 0x%x)",
+                        flag);
         return fail(ctx, GBFK_E_CUDA, "rd_step: a CTA's work list of the pipelined step overflowed");
     }
     return GBFK_OK;
@@ -493,6 +505,28 @@ int build_step_lists(gbfk_ctx *ctx)
     ctx->n_heavy = nh;
     ctx->n_empty = nb - nh;
     ctx->lists_valid = true;
+    ctx->h_lists.swap(lists);
+    ctx->run_layout_valid = false;
+    return GBFK_OK;
+}
+
+// The CTA layout of runs of steps over the current step lists.
+template <typename Real>
+int build_run_layout(gbfk_ctx *ctx, const PoolView<Real> &v)
+{
+    if (ctx->run_layout_valid) return GBFK_OK;
+    std::vector<int> off, nbr;
+    int G = 0;
+    CK(rd_run_layout<Real>(v, ctx->h_lists.data(), ctx->n_heavy, ctx->h_lists.data() + ctx->n_heavy, ctx->n_empty, G,
+                           off, nbr));
+    off.insert(off.end(), nbr.begin(), nbr.end());
+    int rc = topo_alloc(ctx, &ctx->d_run_nbr, off.size() * sizeof(int));
+    if (!rc) rc = topo_alloc(ctx, &ctx->d_run_flags, (size_t)G * kRunFlagStride * sizeof(unsigned));
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->d_run_nbr, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->run_ctas = G;
+    ctx->run_layout_valid = true;
     return GBFK_OK;
 }
 
@@ -503,9 +537,13 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
     if (rc) return rc;
     PoolView<Real> v = view<Real>(ctx);
     const bool eligible = tma_step_eligible<Real>(v);
-    if (ctx->step_pref == GBFK_STEP_PIPELINED && !eligible)
+    if ((ctx->step_pref == GBFK_STEP_PIPELINED || ctx->step_pref == GBFK_STEP_RUN) && !eligible)
         return fail(ctx, GBFK_E_STATE, "rd_step: the pipelined step needs a uniform power-of-two grid (gbfk_set_uniform)");
     const bool pipelined = eligible && ctx->step_pref != GBFK_STEP_BLOCK;
+    // runs of steps in one launch: on request only (on B200 they are within
+    // a few percent of one launch per step, which programmatic dependent
+    // launch already overlaps)
+    const bool runs = pipelined && ctx->step_pref == GBFK_STEP_RUN;
     double ih2 = 0;
     if (pipelined) {
         if (!ctx->tma_maps_ready) {
@@ -514,22 +552,42 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
             ctx->tma_maps_ready = true;
         }
         rc = build_step_lists(ctx);
+        if (!rc && runs) rc = build_run_layout<Real>(ctx, v);
         if (rc) return rc;
         // uniform grid: one h for every block, as upload_ih2 forms it
         const double h = sizeof(Real) == 8 ? ctx->h_h[0] : (double)(float)ctx->h_h[0];
         ih2 = 1. / (h * h);
     }
     if (check_nan) CK(cudaMemsetAsync(ctx->d_nan, 0, sizeof(unsigned), ctx->stream));
-    for (int s = 0; s < nsteps; s++) {
+    const BlockLists lists = {ctx->d_lists, ctx->n_heavy, ctx->d_lists + ctx->n_heavy, ctx->n_empty};
+    bool ran_run = false;
+    for (int s = 0; s < nsteps;) {
         const Real *in = (const Real *)ctx->phi[ctx->cur];
         Real *out = (Real *)ctx->phi[ctx->cur ^ 1];
+        const bool clamped = ctx->phi_clamped || s > 0;
+        const int left = nsteps - s;
+        if (runs && clamped && left >= 2) {
+            // phi[cur] -> phi[cur ^ 1] -> phi[cur] ..., k steps in one launch
+            const int k = left < kMaxRunSteps ? left : kMaxRunSteps;
+            Real *last = (Real *)ctx->phi[ctx->cur ^ (k & 1)];
+            CK(launch_rd_run_tma<Real>(v, lists, ctx->run_ctas, ctx->d_run_nbr, ctx->d_run_nbr + ctx->run_ctas + 1,
+                                       (const Real *)ctx->d_H, ctx->d_meta, ih2, in, out, (Real *)ctx->phi[ctx->cur],
+                                       last, k, (Real)rho, dt, ctx->d_nan, ctx->d_nan + 1, ctx->d_run_flags,
+                                       ctx->tma_maps[ctx->cur], ctx->tma_maps[ctx->cur ^ 1], ctx->tma_maps[ctx->cur],
+                                       ctx->stream));
+            ctx->launches++;
+            ctx->cur ^= (k & 1);
+            s += k;
+            ran_run = true;
+            continue;
+        }
         if (pipelined) {
-            const BlockLists lists = {ctx->d_lists, ctx->n_heavy, ctx->d_lists + ctx->n_heavy, ctx->n_empty};
-            CK(launch_rd_step_tma<Real>(v, lists, (const Real *)ctx->d_H, ctx->d_meta, ih2, in,
-                                        ctx->phi_clamped || s > 0, out, (Real)rho, dt, ctx->d_nan, ctx->d_nan + 1,
-                                        ctx->tma_maps[ctx->cur], ctx->stream));
+            CK(launch_rd_step_tma<Real>(v, lists, (const Real *)ctx->d_H, ctx->d_meta, ih2, in, clamped, out,
+                                        (Real)rho, dt, ctx->d_nan, ctx->d_nan + 1, ctx->tma_maps[ctx->cur],
+                                        ctx->stream));
             ctx->launches++;
             ctx->cur ^= 1;
+            s++;
             continue;
         }
         if (ctx->n_step_rows > 0) {
@@ -541,9 +599,10 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
                                 ctx->d_nan, ctx->stream));
         ctx->launches++;
         ctx->cur ^= 1;
+        s++;
     }
     if (nsteps > 0) {
-        ctx->step_used = pipelined ? GBFK_STEP_PIPELINED : GBFK_STEP_BLOCK;
+        ctx->step_used = ran_run ? GBFK_STEP_RUN : pipelined ? GBFK_STEP_PIPELINED : GBFK_STEP_BLOCK;
         ctx->phi_clamped = true;
     }
     if (check_nan) {
@@ -779,7 +838,7 @@ int gbfk_sync(gbfk_ctx *ctx)
 int gbfk_set_step_kernel(gbfk_ctx *ctx, int kind)
 {
     if (!ctx) return GBFK_E_INVALID;
-    if (kind != GBFK_STEP_AUTO && kind != GBFK_STEP_BLOCK && kind != GBFK_STEP_PIPELINED)
+    if (kind != GBFK_STEP_AUTO && kind != GBFK_STEP_BLOCK && kind != GBFK_STEP_PIPELINED && kind != GBFK_STEP_RUN)
         return fail(ctx, GBFK_E_INVALID, "set_step_kernel: unknown kernel %d", kind);
     ctx->step_pref = kind;
     return GBFK_OK;

@@ -1,5 +1,7 @@
 // Kernel launchers of the gbfk library (declarations shared by the C ABI).
 #pragma once
+
+#include <vector>
 #include <cstdint>
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -105,6 +107,30 @@ cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const BlockLists &lists,
                                Real *phi_out, Real rho, double dt, unsigned *nan_flag, unsigned *err_flag,
                                const CUtensorMap *maps, cudaStream_t s);
 cudaError_t make_pool_tensor_maps(void *base, int nslots, int real_bytes, CUtensorMap maps[3]);
+// A run of nsteps (2 .. kMaxRunSteps) steps of the pipelined step in one
+// cooperative launch: in0 (the output of a step) -> buf0 -> buf1 -> buf0 ...,
+// the last step into `last`; the results are those of nsteps launches.  Each
+// CTA keeps its blocks for the whole run and, between steps, waits only for
+// the CTAs that own face neighbours of its blocks (a step flag per CTA,
+// kRunFlagStride words apart; rd_run_layout gives the CTA count and the
+// neighbour lists, which the launch takes in device memory).  maps_*: the
+// face-box tensor maps of in0, buf0, buf1.  The error word of the pipelined
+// steps: bit 0 a copy or slot wait gave up (after about a second), bit 1 a
+// CTA's work list overflowed; the wait that gave up: bit 3 a consumer's
+// heavy slot, 4 its empty slot, 5 the producer's free heavy slot, 6 its
+// free empty slot, 7 a step boundary (this CTA's or a neighbour's), 8 the
+// wait for every consumer warp's stores.
+constexpr int kMaxRunSteps = 1 << 20;
+constexpr int kRunFlagStride = 32;
+template <typename Real>
+cudaError_t rd_run_layout(const PoolView<Real> &v, const int *heavy, int n_heavy, const int *empty, int n_empty,
+                          int &ctas, std::vector<int> &nbr_off, std::vector<int> &nbr);
+template <typename Real>
+cudaError_t launch_rd_run_tma(const PoolView<Real> &v, const BlockLists &lists, int ctas, const int *nbr_off,
+                              const int *nbr, const Real *H, const unsigned short *meta, double ih2, const Real *in0,
+                              Real *buf0, Real *buf1, Real *last, int nsteps, Real rho, double dt, unsigned *nan_flag,
+                              unsigned *err_flag, unsigned *flags, const CUtensorMap *maps_in0,
+                              const CUtensorMap *maps_buf0, const CUtensorMap *maps_buf1, cudaStream_t s);
 
 // The same for a step of a TMCMC batch: every active sample (positions
 // 0 .. nactive-1) of one uniform 2^log2_bpd grid.  Per-position fields are

@@ -40,9 +40,11 @@
 // the CTA exits.  No load uses cluster multicast.
 #include <cuda.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
+#include <vector>
 
 #include "gbfk.h"
 #include "gbfk_exact.cuh"
@@ -156,7 +158,7 @@ struct SmemLayout {
     static constexpr size_t heavy = 0;
     static constexpr size_t empty = heavy + (size_t)kHeavySlots * sizeof(HeavySlot<Real>);
     static constexpr size_t bars = empty + (size_t)kEmptySlots * kBS3 * sizeof(Real);
-    static constexpr size_t hdr = bars + (8 * (size_t)(2 * kHeavySlots + 2 * kEmptySlots) + 127) / 128 * 128;
+    static constexpr size_t hdr = bars + (8 * (size_t)(2 * kHeavySlots + 2 * kEmptySlots + 2) + 127) / 128 * 128;
     static constexpr size_t items = hdr + sizeof(SlotHdr) * (size_t)(kHeavySlots + kEmptySlots);
     static constexpr size_t bytes = items + kMaxItems * sizeof(int);
 };
@@ -213,6 +215,55 @@ __device__ __forceinline__ void vec_stg(Real *dst, const Real (&d)[N])
 #pragma unroll
         for (int i = 0; i < N; i++) dst[i] = d[i];
     }
+}
+
+// The face-box tensor maps (x, y, z faces) of one buffer of blocks, and the
+// maps a launch reads: one set for one step; for a run of steps, the sets of
+// the run's first input and of its two alternating buffers.
+struct TmaMapSet {
+    CUtensorMap m[3];
+};
+template <int N>
+struct TmaMaps {
+    TmaMapSet b[N];
+};
+
+// A run of steps in one launch (kMulti): step s reads in0 (s = 0) or
+// buf[(s - 1) & 1] and writes buf[s & 1], except the last step, which writes
+// last.  flags[c * kRunFlagStride]: the steps CTA c has stored (zero at
+// launch); nbr[nbr_off[c] .. nbr_off[c + 1]): the other CTAs that own a face
+// neighbour of one of CTA c's blocks.
+template <typename Real>
+struct StepRun {
+    const Real *in0;
+    Real *buf[2];
+    Real *last;
+    unsigned *flags;
+    const int *nbr_off, *nbr;
+    int nsteps;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Bounded wait, by the 32 lanes of a warp together, until every CTA in
+// nbr[j0 .. j1) has stored `target` steps (kWaitNs of device time, and
+// independently 2^24 polls of one flag); true when they all have.
+__device__ __noinline__ bool neighbours_done(const unsigned *flags, const int *nbr, int j0, int j1, unsigned target,
+                                             int lane)
+{
+    const unsigned long long t0 = global_ns();
+    for (int j = j0 + lane; j < j1; j += 32) {
+        const unsigned *f = flags + (int64_t)nbr[j] * kRunFlagStride;
+        int i = 0;
+        while (ld_acquire_gpu(f) < target)
+            if (++i > (1 << 24) || global_ns() - t0 > kWaitNs) return false;
+    }
+    return true;
 }
 
 // The fields of one sample that the rare slow paths read from global
@@ -422,14 +473,16 @@ __device__ __noinline__ Real empty_cell(const ItemCtx<Real> v, int blk, int c, R
     if (!(phi > (Real)0)) return dt_finite ? clamp01(phi) : cell_update(phi, (Real)0., dt);
     const int L = v.L;
     const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
+    // loads cached in L2 only: in a run of steps the buffer is rewritten
+    // between two of its reads by other CTAs
     const Real *b0 = phi_in + (int64_t)blk * kBS3;
     Real phn[6];
-    phn[0] = x > 0 ? b0[c - 1] : phi_in[(int64_t)nb_of(blk, L, 0) * kBS3 + c + 7];
-    phn[1] = x < 7 ? b0[c + 1] : phi_in[(int64_t)nb_of(blk, L, 1) * kBS3 + c - 7];
-    phn[2] = y > 0 ? b0[c - 8] : phi_in[(int64_t)nb_of(blk, L, 2) * kBS3 + c + 56];
-    phn[3] = y < 7 ? b0[c + 8] : phi_in[(int64_t)nb_of(blk, L, 3) * kBS3 + c - 56];
-    phn[4] = z > 0 ? b0[c - 64] : phi_in[(int64_t)nb_of(blk, L, 4) * kBS3 + c + 448];
-    phn[5] = z < 7 ? b0[c + 64] : phi_in[(int64_t)nb_of(blk, L, 5) * kBS3 + c - 448];
+    phn[0] = __ldcg(x > 0 ? &b0[c - 1] : &phi_in[(int64_t)nb_of(blk, L, 0) * kBS3 + c + 7]);
+    phn[1] = __ldcg(x < 7 ? &b0[c + 1] : &phi_in[(int64_t)nb_of(blk, L, 1) * kBS3 + c - 7]);
+    phn[2] = __ldcg(y > 0 ? &b0[c - 8] : &phi_in[(int64_t)nb_of(blk, L, 2) * kBS3 + c + 56]);
+    phn[3] = __ldcg(y < 7 ? &b0[c + 8] : &phi_in[(int64_t)nb_of(blk, L, 3) * kBS3 + c - 56]);
+    phn[4] = __ldcg(z > 0 ? &b0[c - 64] : &phi_in[(int64_t)nb_of(blk, L, 4) * kBS3 + c + 448]);
+    phn[5] = __ldcg(z < 7 ? &b0[c + 64] : &phi_in[(int64_t)nb_of(blk, L, 5) * kBS3 + c - 448]);
     const Real eps = (Real)0.1;
     bool low[6];
 #pragma unroll
@@ -458,12 +511,20 @@ __device__ __forceinline__ unsigned bits_or(double a)
 #define GBFK_TMA_MIN_BLOCKS_F64 3
 #endif
 
-template <typename Real, int kWarps, int kHeavySlots, int kEmptySlots, bool kClamped, typename Source>
+// kMulti: a run of run.nsteps steps in one cooperative launch (one pool, and
+// kClamped: every input of the run is the output of a step).  Each CTA keeps
+// its items for the whole run; after its consumers have stored step s, one
+// of them arrives on a grid barrier (a counter in global memory, waits
+// bounded like every other) and then releases the producer to issue step
+// s + 1, whose copies read what every CTA wrote in step s.  The step
+// arithmetic is the one-step kernel's: a run of n steps gives the bits of n
+// launches.
+template <typename Real, int kWarps, int kHeavySlots, int kEmptySlots, bool kClamped, bool kMulti, typename Source>
 __global__ void __launch_bounds__((kWarps + 1) * 32, kWarps == 8 ? (sizeof(Real) == 4 ? GBFK_TMA_MIN_BLOCKS_F32
                                                                                        : GBFK_TMA_MIN_BLOCKS_F64)
                                                                   : 1)
-rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __grid_constant__ CUtensorMap map_x,
-                   const __grid_constant__ CUtensorMap map_y, const __grid_constant__ CUtensorMap map_z)
+rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const StepRun<Real> run,
+                   const __grid_constant__ TmaMaps<kMulti ? 3 : 1> maps)
 {
     // Programmatic dependent launch: a step launched with it may be scheduled
     // while the previous grid on the stream still runs.  It lets the next
@@ -478,19 +539,24 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
     constexpr int kCells = kBS3 / kThreads;
     static_assert(kCells * kThreads == kBS3 && kCells >= 1 && kCells <= 8, "consumer warps per block");
     static_assert(kEmptySlots % kWarps == 0, "an empty slot must serve one warp");
+    static_assert(!kMulti || (kClamped && !Source::kSamples), "a run of steps: one pool, clamped inputs");
     constexpr int kVec = 16 / sizeof(Real);       // cells per 16-byte vector
     constexpr int kOwnVecs = kBS3 / (32 * kVec);  // vectors per lane of an empty block's warp
     extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ unsigned run_abort;  // kMulti: a grid barrier wait gave up
     HeavySlot<Real> *heavy = reinterpret_cast<HeavySlot<Real> *>(smem + Lay::heavy);
     Real *empties = reinterpret_cast<Real *>(smem + Lay::empty);
     uint64_t *hfull = reinterpret_cast<uint64_t *>(smem + Lay::bars);
     uint64_t *hfree = hfull + kHeavySlots;
     uint64_t *efull = hfree + kHeavySlots;
     uint64_t *efree = efull + kEmptySlots;
+    uint64_t *go = efree + kEmptySlots;  // kMulti, per step boundary: the producer may issue the next step
+    uint64_t *done = go + 1;             // kMulti, per step boundary: every consumer warp has stored the step
     SlotHdr *hhdr = reinterpret_cast<SlotHdr *>(smem + Lay::hdr);
     SlotHdr *ehdr = hhdr + kHeavySlots;
     const int t = threadIdx.x;
     const int c = blockIdx.x, G = gridDim.x;
+    const int nsteps = kMulti ? run.nsteps : 1;
     const int NH = src.total_heavy(), NE = src.total_empty();
     const int nh = NH > c ? (NH - 1 - c) / G + 1 : 0;
     // empty items: one pool counts them from the other end (CTA c takes
@@ -498,7 +564,7 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
     // item than others get no more empty ones; a batch: c, c + G, ...
     const int ce = Source::kSamples ? c : G - 1 - c;
     const int ne = NE > ce ? (NE - 1 - ce) / G + 1 : 0;
-    if (nh + ne == 0) return;  // uniform across the CTA
+    if (!kMulti && nh + ne == 0) return;  // uniform across the CTA (a run's CTAs all take the barriers)
     // one pool: the CTA's items staged in shared memory, issued by lane 0
     // alone; a batch: decoded 32 at a time by the producer warp
     constexpr bool kStaged = !Source::kSamples;
@@ -521,16 +587,32 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
             mbar_init(&efull[i], 1);
             mbar_init(&efree[i], 1);
         }
+        if (kMulti) {
+            mbar_init(go, 1);
+            mbar_init(done, kWarps);
+            run_abort = 0;
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();  // the only CTA-wide barrier
     asm volatile("griddepcontrol.wait;" ::: "memory");
 
+    // the buffers and tensor maps of step s
+    auto in_of = [&](int s) -> const Real * {
+        if (!kMulti) return src.phi_in;
+        return s == 0 ? run.in0 : run.buf[(s - 1) & 1];
+    };
+    auto out_of = [&](int s) -> Real * {
+        if (!kMulti) return src.phi_out;
+        return s == nsteps - 1 ? run.last : run.buf[s & 1];
+    };
+    auto maps_of = [&](int s) -> const TmaMapSet & { return maps.b[kMulti ? (s == 0 ? 0 : 1 + ((s - 1) & 1)) : 0]; };
+
     const int L = src.L;
     const int lane = t & 31;
     if (t >= kThreads) {
         // producer warp; lane 0 puts an item in flight in slot s
-        auto issue_heavy = [&](int s, int p, int e, double irho, double idt) {
+        auto issue_heavy = [&](int s, int p, int e, double irho, double idt, const Real *in, const TmaMapSet &ms) {
             const int blk = e >> 2, bt = e & 3;
             const int64_t s0 = src.slot0(p);
             if (Source::kSamples) {
@@ -545,18 +627,18 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
             uint32_t bytes = (kBS3 + 2 * 256 + 4 * 64 + kFacesPerBlock) * sizeof(Real);
             if (bt == kBlockMixed) bytes += kBS3 * sizeof(unsigned short);
             mbar_arrive_expect_tx(bar, bytes);
-            bulk_g2s(S.in, src.phi_in + (s0 + blk) * kBS3, kBS3 * sizeof(Real), bar);
-            box_g2s(S.xm, &map_x, 4, 0, 0, (int)(s0 + nb_of(blk, L, 0)), bar);
-            box_g2s(S.xp, &map_x, 0, 0, 0, (int)(s0 + nb_of(blk, L, 1)), bar);
-            box_g2s(S.ym, &map_y, 0, 7, 0, (int)(s0 + nb_of(blk, L, 2)), bar);
-            box_g2s(S.yp, &map_y, 0, 0, 0, (int)(s0 + nb_of(blk, L, 3)), bar);
-            box_g2s(S.zm, &map_z, 0, 0, 7, (int)(s0 + nb_of(blk, L, 4)), bar);
-            box_g2s(S.zp, &map_z, 0, 0, 0, (int)(s0 + nb_of(blk, L, 5)), bar);
+            bulk_g2s(S.in, in + (s0 + blk) * kBS3, kBS3 * sizeof(Real), bar);
+            box_g2s(S.xm, &ms.m[0], 4, 0, 0, (int)(s0 + nb_of(blk, L, 0)), bar);
+            box_g2s(S.xp, &ms.m[0], 0, 0, 0, (int)(s0 + nb_of(blk, L, 1)), bar);
+            box_g2s(S.ym, &ms.m[1], 0, 7, 0, (int)(s0 + nb_of(blk, L, 2)), bar);
+            box_g2s(S.yp, &ms.m[1], 0, 0, 0, (int)(s0 + nb_of(blk, L, 3)), bar);
+            box_g2s(S.zm, &ms.m[2], 0, 0, 7, (int)(s0 + nb_of(blk, L, 4)), bar);
+            box_g2s(S.zp, &ms.m[2], 0, 0, 0, (int)(s0 + nb_of(blk, L, 5)), bar);
             bulk_g2s(S.H, src.H_of(p) + (int64_t)blk * kFacesPerBlock, kFacesPerBlock * sizeof(Real), bar);
             if (bt == kBlockMixed)
                 bulk_g2s(S.meta, src.meta_of(p) + (int64_t)blk * kBS3, kBS3 * sizeof(unsigned short), bar);
         };
-        auto issue_empty = [&](int s, int p, int e, double irho, double idt) {
+        auto issue_empty = [&](int s, int p, int e, double irho, double idt, const Real *in) {
             if (Source::kSamples) {
                 ehdr[s].dt = idt;
                 ehdr[s].rho = irho;
@@ -565,34 +647,63 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
             ehdr[s].e = e;
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive_expect_tx(&efull[s], kBS3 * sizeof(Real));
-            bulk_g2s(empties + s * kBS3, src.phi_in + (src.slot0(p) + (e >> 2)) * kBS3, kBS3 * sizeof(Real),
-                     &efull[s]);
+            bulk_g2s(empties + s * kBS3, in + (src.slot0(p) + (e >> 2)) * kBS3, kBS3 * sizeof(Real), &efull[s]);
         };
-        int jh = 0, je = 0;
+        int jh = 0, je = 0;  // items issued, over all steps of a run
         bool ok = true;
+        unsigned site = 0;  // which wait gave up (error word bits 5..7)
         if (kStaged) {
-            if (lane != 0) return;
-            while (jh < nh || je < ne) {
-                if (heavy_next(jh, je, nh, ne)) {
-                    const int s = jh % kHeavySlots;
-                    if (jh >= kHeavySlots && !mbar_wait(&hfree[s], ((jh / kHeavySlots) - 1) & 1)) {
+            if (!kMulti && lane != 0) return;
+            for (int st = 0; st < nsteps && ok; st++) {
+                if (kMulti && st > 0) {
+                    // this CTA's consumers have stored step st - 1 (go), and
+                    // so have the CTAs that own the face neighbours of its
+                    // blocks: the inputs of step st are complete, and no
+                    // block that step st overwrites is still read
+                    bool w = mbar_wait(go, (st - 1) & 1) && !*(volatile unsigned *)&run_abort;
+                    if (w) w = neighbours_done(run.flags, run.nbr, run.nbr_off[c], run.nbr_off[c + 1], (unsigned)st, lane);
+                    if (!__all_sync(0xffffffffu, w)) {
                         ok = false;
+                        site = 128u;
                         break;
                     }
-                    issue_heavy(s, 0, items[jh], 0., 0.);
-                    jh++;
-                } else {
-                    const int s = je % kEmptySlots;
-                    if (je >= kEmptySlots && !mbar_wait(&efree[s], ((je / kEmptySlots) - 1) & 1)) {
-                        ok = false;
-                        break;
-                    }
-                    issue_empty(s, 0, items[nh + je], 0., 0.);
-                    je++;
+                    __syncwarp();
+                    if (lane == 0) asm volatile("fence.proxy.async.global;" ::: "memory");
                 }
+                const Real *in = in_of(st);
+                const TmaMapSet &ms = maps_of(st);
+                if (lane == 0) {
+                    int lh = 0, le = 0;  // items of this step
+                    while (lh < nh || le < ne) {
+                        if (heavy_next(lh, le, nh, ne)) {
+                            const int s = jh % kHeavySlots;
+                            if (jh >= kHeavySlots && !mbar_wait(&hfree[s], ((jh / kHeavySlots) - 1) & 1)) {
+                                ok = false;
+                                site = 32u;
+                                break;
+                            }
+                            issue_heavy(s, 0, items[lh], 0., 0., in, ms);
+                            lh++;
+                            jh++;
+                        } else {
+                            const int s = je % kEmptySlots;
+                            if (je >= kEmptySlots && !mbar_wait(&efree[s], ((je / kEmptySlots) - 1) & 1)) {
+                                ok = false;
+                                site = 64u;
+                                break;
+                            }
+                            issue_empty(s, 0, items[nh + le], 0., 0., in);
+                            le++;
+                            je++;
+                        }
+                    }
+                }
+                if (kMulti) ok = __shfl_sync(0xffffffffu, ok, 0);
             }
         } else {
             // the lanes decode 32 items of each kind at a time, lane 0 issues them
+            const Real *in = in_of(0);
+            const TmaMapSet &ms = maps_of(0);
             int hbase = 0, ebase = 0;
             int hp = 0, he = 0, ep = 0, ee = 0;
             double hrho = 0, hdt = 0, erho = 0, edt = 0;
@@ -621,9 +732,10 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
                     if (lane == 0 && jh >= kHeavySlots) w = mbar_wait(&hfree[s], ((jh / kHeavySlots) - 1) & 1);
                     if (!__shfl_sync(0xffffffffu, w, 0)) {
                         ok = false;
+                        site = 32u;
                         break;
                     }
-                    if (lane == 0) issue_heavy(s, p, e, irho, idt);
+                    if (lane == 0) issue_heavy(s, p, e, irho, idt, in, ms);
                     jh++;
                 } else {
                     if (je == ebase + 32) {
@@ -641,15 +753,16 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
                     if (lane == 0 && je >= kEmptySlots) w = mbar_wait(&efree[s], ((je / kEmptySlots) - 1) & 1);
                     if (!__shfl_sync(0xffffffffu, w, 0)) {
                         ok = false;
+                        site = 64u;
                         break;
                     }
-                    if (lane == 0) issue_empty(s, p, e, irho, idt);
+                    if (lane == 0) issue_empty(s, p, e, irho, idt, in);
                     je++;
                 }
             }
         }
         if (lane == 0) {
-            if (!ok) atomicOr(err_flag, 1u);
+            if (!ok) atomicOr(err_flag, 1u | site);
             // the CTA's shared memory must outlive every copy in flight (bounded)
             for (int j = jh - kHeavySlots > 0 ? jh - kHeavySlots : 0; j < jh; j++)
                 mbar_wait(&hfull[j % kHeavySlots], (j / kHeavySlots) & 1);
@@ -662,110 +775,153 @@ rd_step_tma_kernel(const Source src, double ih2, unsigned *err_flag, const __gri
     const int warp = t >> 5;
     const int x = t & 7, y = (t >> 3) & 7, z0 = (t >> 6) * kCells;
     const int c0 = x + kBS * (y + kBS * z0);
-    int jh = 0, je = warp;  // next heavy item; next empty item of this warp (j % kWarps == warp)
-    while (jh < nh || je < ne) {
-        if (heavy_next(jh, je, nh, ne)) {
-            const int s = jh % kHeavySlots;
-            if (!__all_sync(0xffffffffu, mbar_wait(&hfull[s], (jh / kHeavySlots) & 1))) {
-                if (lane == 0) atomicOr(err_flag, 1u);
-                break;
+    // items over all steps of a run: heavy item jh of step st is item
+    // st * nh + jh, empty item je of step st is st * ne + je; a warp takes the
+    // empty items whose run index is warp mod kWarps, so each empty slot
+    // keeps serving one warp
+    int next_e = warp;  // this warp's next empty item (run index)
+    for (int st = 0; st < nsteps; st++) {
+        const Real *in = in_of(st);
+        Real *out = out_of(st);
+        int jh = 0, je = next_e - st * ne;  // next heavy item; next empty item of this warp (this step)
+        while (jh < nh || je < ne) {
+            if (heavy_next(jh, je, nh, ne)) {
+                const int J = st * nh + jh;
+                const int s = J % kHeavySlots;
+                if (!__all_sync(0xffffffffu, mbar_wait(&hfull[s], (J / kHeavySlots) & 1))) {
+                    if (lane == 0) atomicOr(err_flag, 1u | 8u);
+                    return;
+                }
+                const int e = hhdr[s].e, blk = e >> 2;
+                int p = 0;
+                double dt;
+                Real rho;
+                if (Source::kSamples) {
+                    p = hhdr[s].p;
+                    dt = hhdr[s].dt;
+                    rho = (Real)hhdr[s].rho;
+                } else {
+                    dt = src.dt_of(0);
+                    rho = src.rho_of(0);
+                }
+                Real o[kCells];
+                if ((e & 3) == kBlockTissue)
+                    column_cells<Real, kCells, false, kClamped>(src, p, heavy[s], blk, x, y, z0, c0, rho, ih2, dt,
+                                                                isfinite(dt), o);
+                else
+                    column_cells<Real, kCells, true, kClamped>(src, p, heavy[s], blk, x, y, z0, c0, rho, ih2, dt,
+                                                               isfinite(dt), o);
+                // every shared read of this warp is done: release the slot
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&hfree[s], 1);
+                Real *ob = out + (src.slot0(p) + blk) * kBS3;
+                bool bad = false;
+#pragma unroll
+                for (int i = 0; i < kCells; i++) {
+                    bad |= (o[i] != o[i]);
+                    ob[c0 + 64 * i] = o[i];
+                }
+                if (bad) atomicOr(src.nan_of(p), 1u);
+                jh++;
+                continue;
             }
-            const int e = hhdr[s].e, blk = e >> 2;
-            int p = 0;
-            double dt;
-            Real rho;
-            if (Source::kSamples) {
-                p = hhdr[s].p;
-                dt = hhdr[s].dt;
-                rho = (Real)hhdr[s].rho;
-            } else {
-                dt = src.dt_of(0);
-                rho = src.rho_of(0);
+            const int j = je;
+            je += kWarps;
+            const int J = st * ne + j;
+            const int s = J % kEmptySlots;
+            if (!__all_sync(0xffffffffu, mbar_wait(&efull[s], (J / kEmptySlots) & 1))) {
+                if (lane == 0) atomicOr(err_flag, 1u | 16u);
+                return;
             }
-            Real out[kCells];
-            if ((e & 3) == kBlockTissue)
-                column_cells<Real, kCells, false, kClamped>(src, p, heavy[s], blk, x, y, z0, c0, rho, ih2, dt,
-                                                            isfinite(dt), out);
-            else
-                column_cells<Real, kCells, true, kClamped>(src, p, heavy[s], blk, x, y, z0, c0, rho, ih2, dt,
-                                                           isfinite(dt), out);
-            // every shared read of this warp is done: release the slot
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&hfree[s], 1);
-            Real *ob = src.phi_out + (src.slot0(p) + blk) * kBS3;
-            bool bad = false;
-#pragma unroll
-            for (int i = 0; i < kCells; i++) {
-                bad |= (out[i] != out[i]);
-                ob[c0 + 64 * i] = out[i];
-            }
-            if (bad) atomicOr(src.nan_of(p), 1u);
-            jh++;
-            continue;
-        }
-        const int j = je;
-        je += kWarps;
-        const int s = j % kEmptySlots;
-        if (!__all_sync(0xffffffffu, mbar_wait(&efull[s], (j / kEmptySlots) & 1))) {
-            if (lane == 0) atomicOr(err_flag, 1u);
-            break;
-        }
-        const Real *in = empties + s * kBS3;
-        const int blk = ehdr[s].e >> 2;
-        const int p = Source::kSamples ? ehdr[s].p : 0;
-        Real *ob = src.phi_out + (src.slot0(p) + blk) * kBS3;
-        Real pv[kOwnVecs][kVec];
-        unsigned bits = 0;
-#pragma unroll
-        for (int q = 0; q < kOwnVecs; q++) {
-            vec_lds<Real, kVec>(in + (q * 32 + lane) * kVec, pv[q]);
-#pragma unroll
-            for (int i = 0; i < kVec; i++) bits |= bits_or(pv[q][i]);
-        }
-        if (bits == 0) {
-            // every cell +0.0: outside the domain, and the clamp leaves +0.0
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&efree[s], 1);
-#pragma unroll
-            for (int q = 0; q < kOwnVecs; q++) vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, pv[q]);
-            continue;
-        }
-        const double dt = Source::kSamples ? ehdr[s].dt : src.dt_of(0);
-        const int dt_finite = isfinite(dt);
-        bool any = false, bad = false;
-#pragma unroll
-        for (int q = 0; q < kOwnVecs; q++)
-#pragma unroll
-            for (int i = 0; i < kVec; i++) any |= pv[q][i] > (Real)0;  // the domain test of a kEmpty cell
-        if (any) {
-            // tumour outside the anatomy: an empty block's slot holds no halo
-            // or coefficients, read them from global memory (rare)
-            const ItemCtx<Real> cx = src.ctx(p);
-            const Real rho = Source::kSamples ? (Real)ehdr[s].rho : src.rho_of(0);
-#pragma unroll 1
-            for (int q = 0; q < kOwnVecs * kVec; q++) {
-                const int cc = ((q / kVec) * 32 + lane) * kVec + q % kVec;
-                const Real o = empty_cell(cx, blk, cc, in[cc], rho, ih2, dt, dt_finite);
-                bad |= (o != o);
-                ob[cc] = o;
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&efree[s], 1);
-        } else {
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&efree[s], 1);
+            const Real *ein = empties + s * kBS3;
+            const int blk = ehdr[s].e >> 2;
+            const int p = Source::kSamples ? ehdr[s].p : 0;
+            Real *ob = out + (src.slot0(p) + blk) * kBS3;
+            Real pv[kOwnVecs][kVec];
+            unsigned bits = 0;
 #pragma unroll
             for (int q = 0; q < kOwnVecs; q++) {
-                Real o[kVec];
+                vec_lds<Real, kVec>(ein + (q * 32 + lane) * kVec, pv[q]);
 #pragma unroll
-                for (int i = 0; i < kVec; i++) {
-                    o[i] = dt_finite ? clamp01(pv[q][i]) : cell_update(pv[q][i], (Real)0., dt);
-                    bad |= (o[i] != o[i]);
+                for (int i = 0; i < kVec; i++) bits |= bits_or(pv[q][i]);
+            }
+            if (bits == 0) {
+                // every cell +0.0: outside the domain, and the clamp leaves +0.0
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&efree[s], 1);
+#pragma unroll
+                for (int q = 0; q < kOwnVecs; q++) vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, pv[q]);
+                continue;
+            }
+            const double dt = Source::kSamples ? ehdr[s].dt : src.dt_of(0);
+            const int dt_finite = isfinite(dt);
+            bool any = false, bad = false;
+#pragma unroll
+            for (int q = 0; q < kOwnVecs; q++)
+#pragma unroll
+                for (int i = 0; i < kVec; i++) any |= pv[q][i] > (Real)0;  // the domain test of a kEmpty cell
+            if (any) {
+                // tumour outside the anatomy: an empty block's slot holds no halo
+                // or coefficients, read them from global memory (rare)
+                ItemCtx<Real> cx = src.ctx(p);
+                cx.phi_in = in + src.slot0(p) * kBS3;
+                const Real rho = Source::kSamples ? (Real)ehdr[s].rho : src.rho_of(0);
+#pragma unroll 1
+                for (int q = 0; q < kOwnVecs * kVec; q++) {
+                    const int cc = ((q / kVec) * 32 + lane) * kVec + q % kVec;
+                    const Real o = empty_cell(cx, blk, cc, ein[cc], rho, ih2, dt, dt_finite);
+                    bad |= (o != o);
+                    ob[cc] = o;
                 }
-                vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, o);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&efree[s], 1);
+            } else {
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&efree[s], 1);
+#pragma unroll
+                for (int q = 0; q < kOwnVecs; q++) {
+                    Real o[kVec];
+#pragma unroll
+                    for (int i = 0; i < kVec; i++) {
+                        o[i] = dt_finite ? clamp01(pv[q][i]) : cell_update(pv[q][i], (Real)0., dt);
+                        bad |= (o[i] != o[i]);
+                    }
+                    vec_stg<Real, kVec>(ob + (q * 32 + lane) * kVec, o);
+                }
+            }
+            if (bad) atomicOr(src.nan_of(p), 1u);
+        }
+        next_e = st * ne + je;
+        if (kMulti && st + 1 < nsteps) {
+            // step boundary: each warp reports its stores of step st; thread 0
+            // waits for all of them (bounded: a warp that gave up never
+            // arrives), publishes this CTA's step count to the CTAs that
+            // read its blocks, and opens step st + 1 to the producer and to
+            // every consumer warp.  All warps wait for that: a warp with no
+            // item in step st + 1 would otherwise report step st + 1 before
+            // this boundary has passed.
+            __syncwarp();
+            if (lane == 0) mbar_arrive(done, 1);
+            if (t == 0) {
+                if (mbar_wait(done, st & 1)) {
+                    // the stores, then the flag; the TMA copies of the next
+                    // step (async proxy) read what the generic stores wrote
+                    asm volatile("fence.proxy.async.global;" ::: "memory");
+                    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(run.flags + (int64_t)c * kRunFlagStride),
+                                 "r"((unsigned)(st + 1))
+                                 : "memory");
+                } else {
+                    atomicOr(err_flag, 256u);
+                    run_abort = 1;
+                }
+                mbar_arrive(go, 1);
+            }
+            const bool opened = __all_sync(0xffffffffu, mbar_wait(go, st & 1));
+            if (!opened || *(volatile unsigned *)&run_abort) {
+                if (!opened && lane == 0) atomicOr(err_flag, 1u | 128u);
+                return;
             }
         }
-        if (bad) atomicOr(src.nan_of(p), 1u);
     }
 }
 
@@ -794,26 +950,40 @@ struct Shape {
     static constexpr int kThreads = (kWarps + 1) * 32;
     static constexpr size_t kSmem = SmemLayout<Real, kHeavySlots, kEmptySlots>::bytes;
 
-    // resident CTAs on this part for the kernels of one work source, taken
-    // once per process
-    template <typename Source>
+    // resident CTAs on this part for the kernels of one work source (kMulti:
+    // the run kernel), taken once per process
+    template <typename Source, bool kMulti = false>
     static cudaError_t grid(int &g)
     {
         static int cached = 0;
         static std::mutex mu;
         std::lock_guard<std::mutex> lk(mu);
         if (!cached) {
-            auto k = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false, Source>;
-            auto kc = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true, Source>;
-            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
-            if (e != cudaSuccess) return e;
-            e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
-            if (e != cudaSuccess) return e;
-            int dev = 0, sms = 0, per_sm = 0;
+            cudaError_t e;
+            int per_sm = 0;
+            if constexpr (kMulti) {
+                auto k = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true, true, Source>;
+                if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem)) !=
+                    cudaSuccess)
+                    return e;
+                if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, kSmem)) != cudaSuccess)
+                    return e;
+            } else {
+                auto k = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false, false, Source>;
+                auto kc = rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true, false, Source>;
+                if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem)) !=
+                    cudaSuccess)
+                    return e;
+                if ((e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem)) !=
+                    cudaSuccess)
+                    return e;
+                if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, kSmem)) != cudaSuccess)
+                    return e;
+            }
+            int dev = 0, sms = 0;
             if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
             if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, kSmem)) != cudaSuccess)
-                return e;
+            if (kMulti && per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
             cached = sms * (per_sm > 0 ? per_sm : 1);
         }
         g = cached;
@@ -828,8 +998,11 @@ struct Shape {
         cudaError_t e = grid<Source>(g);
         if (e != cudaSuccess) return e;
         const int nctas = items < g ? items : g;
-        auto k = clamped ? rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true, Source>
-                         : rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false, Source>;
+        auto k = clamped ? rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true, false, Source>
+                         : rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, false, false, Source>;
+        TmaMaps<1> m;
+        for (int i = 0; i < 3; i++) m.b[0].m[i] = maps[i];
+        const StepRun<Real> run = {};
         // one pool: launched with programmatic dependent launch, so that the
         // next step's launch overlaps this step's tail
         cudaLaunchConfig_t cfg = {};
@@ -842,7 +1015,56 @@ struct Shape {
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = Source::kSamples ? 0 : 1;
-        return cudaLaunchKernelEx(&cfg, k, src, ih2, err_flag, maps[0], maps[1], maps[2]);
+        return cudaLaunchKernelEx(&cfg, k, src, ih2, err_flag, run, m);
+    }
+
+    // CTAs of a run over `items` blocks: all that fit (GBFK_RUN_CTAS_PER_SM,
+    // a tuning knob, asks for fewer per SM)
+    static cudaError_t run_grid(int items, int &nctas)
+    {
+        int g = 0;
+        cudaError_t e = grid<PoolSource<Real>, true>(g);
+        if (e != cudaSuccess) return e;
+        static const int per_sm = [] {
+            const char *v = getenv("GBFK_RUN_CTAS_PER_SM");
+            return v ? atoi(v) : 0;
+        }();
+        if (per_sm > 0) {
+            int dev = 0, sms = 0;
+            if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            if (sms * per_sm < g) g = sms * per_sm;
+        }
+        if ((int64_t)items > (int64_t)g * (kMaxItems - 2)) return cudaErrorInvalidValue;
+        nctas = items < g ? items : g;
+        return cudaSuccess;
+    }
+
+    // a run of steps of one pool in one cooperative launch (every CTA
+    // resident: a CTA waits for the CTAs of its neighbours); the step flags
+    // are zeroed first
+    static cudaError_t launch_run(const PoolSource<Real> &src, int items, int ctas, double ih2, unsigned *err_flag,
+                                  const StepRun<Real> &run, const TmaMaps<3> &maps, cudaStream_t s)
+    {
+        int nctas = 0;
+        cudaError_t e = run_grid(items, nctas);
+        if (e != cudaSuccess) return e;
+        if (nctas != ctas) return cudaErrorInvalidValue;  // the neighbour lists were made for `ctas` CTAs
+        if ((e = cudaMemsetAsync(run.flags, 0, (size_t)nctas * kRunFlagStride * sizeof(unsigned), s)) != cudaSuccess)
+            return e;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(nctas);
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = kSmem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, rd_step_tma_kernel<Real, kWarps, kHeavySlots, kEmptySlots, true, true,
+                                                           PoolSource<Real>>,
+                                  src, ih2, err_flag, run, maps);
     }
 };
 
@@ -957,6 +1179,100 @@ cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const BlockLists &lists,
     });
 }
 
+// The CTAs of a run over a grid's step lists, and per CTA the other CTAs
+// that own a face neighbour of one of its blocks (CSR).  CTA c of G owns
+// heavy items c, c + G, ... and empty items G - 1 - c, 2G - 1 - c, ... (the
+// kernel's assignment).
+template <typename Real>
+cudaError_t rd_run_layout(const PoolView<Real> &v, const int *heavy, int n_heavy, const int *empty, int n_empty,
+                          int &ctas, std::vector<int> &nbr_off, std::vector<int> &nbr)
+{
+    const int nb = n_heavy + n_empty;
+    if (nb != v.nblocks || v.log2_bpd < 0) return cudaErrorInvalidValue;
+    int G = 0;
+    cudaError_t e = with_shape<Real>([&](auto sh) { return decltype(sh)::run_grid(nb, G); });
+    if (e != cudaSuccess) return e;
+    std::vector<int> owner(nb, -1);
+    for (int g = 0; g < n_heavy; g++) owner[heavy[g] >> 2] = g % G;
+    for (int g = 0; g < n_empty; g++) owner[empty[g]] = G - 1 - g % G;
+    for (int b = 0; b < nb; b++)
+        if (owner[b] < 0) return cudaErrorInvalidValue;
+    std::vector<std::vector<int>> sets(G);
+    const int L = v.log2_bpd, m = (1 << L) - 1;
+    for (int b = 0; b < nb; b++) {
+        const int bx = b & m, by = (b >> L) & m, bz = b >> (2 * L);
+        for (int f = 0; f < 6; f++) {
+            int x = bx, y = by, z = bz;
+            const int d = f >> 1, sg = (f & 1) ? 1 : -1;
+            if (d == 0) x = (x + sg) & m;
+            else if (d == 1) y = (y + sg) & m;
+            else z = (z + sg) & m;
+            const int o = owner[x | (y << L) | (z << (2 * L))];
+            if (o != owner[b]) sets[owner[b]].push_back(o);
+        }
+    }
+    nbr_off.assign(G + 1, 0);
+    nbr.clear();
+    for (int c = 0; c < G; c++) {
+        std::sort(sets[c].begin(), sets[c].end());
+        sets[c].erase(std::unique(sets[c].begin(), sets[c].end()), sets[c].end());
+        nbr.insert(nbr.end(), sets[c].begin(), sets[c].end());
+        nbr_off[c + 1] = (int)nbr.size();
+    }
+    ctas = G;
+    return cudaSuccess;
+}
+
+// A run of nsteps >= 2 steps of one pool in one launch: in0 (the output of
+// a step) -> buf0 -> buf1 -> buf0 ... and the last step into `last`; maps:
+// the face-box tensor maps of in0, buf0 and buf1; ctas, nbr_off, nbr: the
+// layout of rd_run_layout (nbr_off, nbr in device memory); flags: ctas *
+// kRunFlagStride words of device memory.
+template <typename Real>
+cudaError_t launch_rd_run_tma(const PoolView<Real> &v, const BlockLists &lists, int ctas, const int *nbr_off,
+                              const int *nbr, const Real *H, const unsigned short *meta, double ih2, const Real *in0,
+                              Real *buf0, Real *buf1, Real *last, int nsteps, Real rho, double dt, unsigned *nan_flag,
+                              unsigned *err_flag, unsigned *flags, const CUtensorMap *maps_in0,
+                              const CUtensorMap *maps_buf0, const CUtensorMap *maps_buf1, cudaStream_t s)
+{
+    if (lists.n_heavy + lists.n_empty <= 0) return cudaSuccess;
+    if (nsteps < 2 || nsteps > kMaxRunSteps || !flags || !nbr_off || !nbr) return cudaErrorInvalidValue;
+    if (!tma_step_eligible(v) || lists.n_heavy + lists.n_empty != v.nblocks) return cudaErrorInvalidValue;
+    PoolSource<Real> src;
+    src.heavy = lists.heavy;
+    src.empty = lists.empty;
+    src.nh = lists.n_heavy;
+    src.ne = lists.n_empty;
+    src.phi_in = in0;
+    src.phi_out = last;
+    src.H = H;
+    src.pw = v.pw;
+    src.pg = v.pg;
+    src.meta = meta;
+    src.rho = rho;
+    src.dt = dt;
+    src.L = v.log2_bpd;
+    src.nblocks = v.nblocks;
+    src.nan_flag = nan_flag;
+    StepRun<Real> run;
+    run.in0 = in0;
+    run.buf[0] = buf0;
+    run.buf[1] = buf1;
+    run.last = last;
+    run.flags = flags;
+    run.nbr_off = nbr_off;
+    run.nbr = nbr;
+    run.nsteps = nsteps;
+    TmaMaps<3> m;
+    for (int i = 0; i < 3; i++) {
+        m.b[0].m[i] = maps_in0[i];
+        m.b[1].m[i] = maps_buf0[i];
+        m.b[2].m[i] = maps_buf1[i];
+    }
+    return with_shape<Real>(
+        [&](auto sh) { return decltype(sh)::launch_run(src, v.nblocks, ctas, ih2, err_flag, run, m, s); });
+}
+
 template <typename Real>
 cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int total_items, int log2_bpd,
                                      int nblocks, const Real *phi_in, Real *phi_out, const Real *H, const Real *pw,
@@ -1026,6 +1342,20 @@ template cudaError_t launch_rd_step_tma<double>(const PoolView<double> &, const 
                                                 const unsigned short *, double, const double *, bool, double *,
                                                 double, double, unsigned *, unsigned *, const CUtensorMap *,
                                                 cudaStream_t);
+template cudaError_t rd_run_layout<float>(const PoolView<float> &, const int *, int, const int *, int, int &,
+                                          std::vector<int> &, std::vector<int> &);
+template cudaError_t rd_run_layout<double>(const PoolView<double> &, const int *, int, const int *, int, int &,
+                                           std::vector<int> &, std::vector<int> &);
+template cudaError_t launch_rd_run_tma<float>(const PoolView<float> &, const BlockLists &, int, const int *,
+                                              const int *, const float *, const unsigned short *, double,
+                                              const float *, float *, float *, float *, int, float, double,
+                                              unsigned *, unsigned *, unsigned *, const CUtensorMap *,
+                                              const CUtensorMap *, const CUtensorMap *, cudaStream_t);
+template cudaError_t launch_rd_run_tma<double>(const PoolView<double> &, const BlockLists &, int, const int *,
+                                               const int *, const double *, const unsigned short *, double,
+                                               const double *, double *, double *, double *, int, double, double,
+                                               unsigned *, unsigned *, unsigned *, const CUtensorMap *,
+                                               const CUtensorMap *, const CUtensorMap *, cudaStream_t);
 template cudaError_t launch_rd_batch_step_tma<float>(const BatchLists &, int, int, int, int, const float *, float *,
                                                      const float *, const float *, const float *,
                                                      const unsigned short *, const float *, const double *, double,

@@ -144,8 +144,10 @@ class BlockPool:
     @property
     def step_kernel(self) -> str:
         """Kernel of the last rd_step: "pipelined" (persistent TMA pipeline,
-        uniform power-of-two grids), "block" (one CTA per block) or "" before
-        any step.  Assign "auto", "block" or "pipelined" to choose."""
+        uniform power-of-two grids, one launch per step), "run" (the same
+        pipeline over all steps of the call in one launch), "block" (one CTA
+        per block) or "" before any step.  Assign "auto", "block",
+        "pipelined" or "run" to choose."""
         k = int(self.lib.gbfk_step_kernel(self.ctx))
         return {v: n for n, v in _lib.STEP_KERNELS.items()}.get(k, "") if k else ""
 

@@ -226,7 +226,51 @@ def test_pipelined_step_kernel_selection(gbfk_lib):
     with _pool(32, "f64", pw, pg, c0) as pool:
         pool.rd_step(1e-3, 1e-4, 0.1, 0.5, 2, check_nan=True)
         assert pool.step_kernel == "pipelined"
+        # runs of steps in one launch on request
+        pool.step_kernel = "run"
+        pool.rd_step(1e-3, 1e-4, 0.1, 0.5, 3, check_nan=True)
+        assert pool.step_kernel == "run"
         pool.sync()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("n,seed,steps", [(8, 3, 7), (32, 2, 2), (64, 9, 3), (64, 5, 40), (128, 1, 101)])
+def test_run_of_steps_equals_single_steps(gbfk_lib, prec, n, seed, steps):
+    """A run of steps in one launch (grid barrier between steps) gives the
+    bits of one pipelined launch per step: from an unclamped field (negative
+    values, values above 1; the run starts after one single step), with
+    tumour outside the anatomy (empty blocks whose cells read their
+    neighbours from global memory every step), odd and even step counts."""
+    R = np.float64 if prec == "f64" else np.float32
+    pw, pg, c0, _ = make_case(n, seed)
+    rng = np.random.default_rng(seed + 100)
+    c0 = np.maximum(c0, rng.uniform(0, 1, c0.shape) * (rng.uniform(0, 1, c0.shape) < 0.03))
+    c0[0, 0, :] = 1.7
+    c0[1, :, 2] = -0.3
+    pw[n // 2, :, : n // 3] = 0.0
+    pg[n // 2, :, : n // 3] = 0.0
+    pw, pg, c0 = (a.astype(R) for a in (pw, pg, c0))
+    s = make_schedule(0.3, 0.2, 300.0, 25.6, n // 8, prec)
+    with _pool(n, prec, pw, pg, c0) as a, _pool(n, prec, pw, pg, c0) as b:
+        a.step_kernel = "run"
+        b.step_kernel = "pipelined"
+        a.rd_step(s.Dw, s.Dg, s.rho, s.dt, steps, check_nan=True)
+        for _ in range(steps):
+            b.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1)
+        # (two steps from an unclamped field are two single steps)
+        assert a.step_kernel == ("run" if steps > 2 else "pipelined") and b.step_kernel == "pipelined"
+        x = a.download_dense("phi")
+        assert np.array_equal(x, b.download_dense("phi"))
+        # a clamped field: the whole call is one run; twice in a row
+        for _ in range(2):
+            a.rd_step(s.Dw, s.Dg, s.rho, s.dt, steps, check_nan=True)
+            for _ in range(steps):
+                b.rd_step(s.Dw, s.Dg, s.rho, s.dt, 1)
+            assert a.step_kernel == "run"
+            assert np.array_equal(a.download_dense("phi"), b.download_dense("phi"))
+    if n <= 32:
+        want = O.rd_steps_dense(pw, pg, c0, s.Dw, s.Dg, s.rho, s.h, s.dt, steps)
+        assert np.array_equal(x, want)
 
 
 @pytest.mark.parametrize("prec", ["f32", "f64"])
