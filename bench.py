@@ -346,6 +346,9 @@ def batched_stage(args, stream, local, nsamples=512, bpd=16, seed=1):
         "speedup_vs_sequential": t_seq / t_batch,
         "samples_per_cta": spc, "tile_shape": tile, "cuda_graphs": graphs, "batched_launches": batch_launches,
         "ranks": world,
+        "empty_blocks": "the batch steps the empty blocks (no tissue in them or their face halos; +0 from the "
+                        "initial condition on) once, then skips them: both state buffers hold their final +0; "
+                        "the sequential solves step every block",
         "timing": "CUDA events on the stream: batched = face coefficients + initial conditions + all steps; "
                   "sequential = per sample an H2D of c0, face coefficients and its steps",
     }

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <numeric>
@@ -68,6 +69,10 @@ struct gbfk_batch {
     int2 *d_dec = nullptr;       // decoded heavy items, then decoded empty items
     size_t dec_cap = 0;
     BatchLists bl{};
+    std::vector<int> h_hpref;    // host copy of bl.hpref
+    // every sample's empty blocks hold +0 in both state buffers after the
+    // first step and keep it (see batch_prepare); later steps skip them
+    bool empties_static = false;
     void *d_rho = nullptr;
     double *d_dt = nullptr;
     double ih2 = 0;
@@ -255,6 +260,7 @@ int batch_lists(gbfk_batch *b)
     BK(cudaStreamSynchronize(b->stream));
     b->bl.hdec = b->d_dec;
     b->bl.edec = b->d_dec + hpref[ns];
+    b->h_hpref.swap(hpref);
     return GBFK_OK;
 }
 
@@ -370,6 +376,15 @@ int batch_prepare(gbfk_batch *b)
     BK(cudaMemsetAsync(b->d_nan, 0, b->max_samples * sizeof(unsigned), b->stream));
     BK(cudaMemsetAsync(b->d_err, 0, sizeof(unsigned), b->stream));
     BK(cudaStreamSynchronize(b->stream));
+    // An empty block (no tissue in it or its face halos: p_w = p_g = 0) starts
+    // at +0 -- both initial conditions write +0 wherever p_w + p_g is not
+    // positive -- and, with a finite dt, a kEmpty cell at +0 is outside the
+    // domain and stays +0 (the update clamps it).  The first step writes
+    // those +0 into the other state buffer; from then on both buffers hold
+    // the final bits of every empty block, and the pipelined step skips them.
+    b->empties_static = true;
+    for (int k = 0; k < b->nsamples; k++)
+        if (!std::isfinite(b->params[b->order[k]].dt)) b->empties_static = false;
     return b->log2_bpd >= 0 ? batch_lists(b) : GBFK_OK;
 }
 
@@ -380,8 +395,10 @@ cudaError_t batch_step(gbfk_batch *b, const BatchView<Real> &bv, int nactive, in
 {
     if (spc > 0) return launch_rd_batch_step<Real>(bv, nactive, step, spc, b->stream);
     const int par = step & 1;
+    const bool skip = b->empties_static && step > 0;
+    const int items = skip ? b->h_hpref[nactive] : nactive * b->nblocks;
     return launch_rd_batch_step_tma<Real>(
-        b->bl, nactive, nactive * b->nblocks, b->log2_bpd, b->nblocks, (const Real *)b->phi_all[par],
+        b->bl, nactive, items, skip, b->log2_bpd, b->nblocks, (const Real *)b->phi_all[par],
         (Real *)b->phi_all[par ^ 1], (const Real *)b->H_all, (const Real *)b->pw_all, (const Real *)b->pg_all,
         b->meta_all, (const Real *)b->d_rho, b->d_dt, b->ih2, step > 0, b->d_nan, b->d_err, b->maps[par], shape,
         b->stream);

@@ -138,7 +138,9 @@ cudaError_t launch_rd_run_tma(const PoolView<Real> &v, const BlockLists &lists, 
 // too (pw, pg, meta).  bl: per-anatomy heavy/empty block lists and the
 // prefix sums of their lengths over the positions; total_items = blocks of
 // all active samples; rho, dt, nan_flags per position; maps: the face-box
-// tensor maps of the phi_in buffer (all positions).
+// tensor maps of the phi_in buffer (all positions).  skip_empty: the empty
+// blocks of every active sample already hold their output in phi_out (and
+// phi_in); total_items then counts the heavy blocks only.
 struct BatchLists {
     const int *lists;     // per anatomy: heavy entries (block * 4 + type), then empty entries (block)
     const int *list_off;  // [2a]: offset of anatomy a's heavy entries, [2a + 1]: of its empty entries
@@ -150,11 +152,11 @@ struct BatchLists {
     const int2 *hdec, *edec;
 };
 template <typename Real>
-cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int total_items, int log2_bpd,
-                                     int nblocks, const Real *phi_in, Real *phi_out, const Real *H, const Real *pw,
-                                     const Real *pg, const unsigned short *meta, const Real *rho, const double *dt,
-                                     double ih2, bool clamped, unsigned *nan_flags, unsigned *err_flag,
-                                     const CUtensorMap *maps, int shape, cudaStream_t s);
+cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int total_items, bool skip_empty,
+                                     int log2_bpd, int nblocks, const Real *phi_in, Real *phi_out, const Real *H,
+                                     const Real *pw, const Real *pg, const unsigned short *meta, const Real *rho,
+                                     const double *dt, double ih2, bool clamped, unsigned *nan_flags,
+                                     unsigned *err_flag, const CUtensorMap *maps, int shape, cudaStream_t s);
 // launch shapes of the pipelined step a batch may use: codes
 // consumer warps * 1000 + heavy slots * 100 + empty slots (shape -1 above:
 // the default, or GBFK_TMA_SHAPE); returns how many were written

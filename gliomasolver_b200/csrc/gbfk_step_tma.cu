@@ -342,9 +342,10 @@ struct BatchSource {
     const double *dt;       // per position
     int L, nblocks;
     unsigned *nan_flags;    // per position
+    bool skip_empty;        // the empty blocks already hold their output
 
     __device__ int total_heavy() const { return hpref[nactive]; }
-    __device__ int total_empty() const { return epref[nactive]; }
+    __device__ int total_empty() const { return skip_empty ? 0 : epref[nactive]; }
     const int2 *hdec, *edec;
     __device__ void heavy_item(int g, int &p, int &e) const
     {
@@ -1274,11 +1275,11 @@ cudaError_t launch_rd_run_tma(const PoolView<Real> &v, const BlockLists &lists, 
 }
 
 template <typename Real>
-cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int total_items, int log2_bpd,
-                                     int nblocks, const Real *phi_in, Real *phi_out, const Real *H, const Real *pw,
-                                     const Real *pg, const unsigned short *meta, const Real *rho, const double *dt,
-                                     double ih2, bool clamped, unsigned *nan_flags, unsigned *err_flag,
-                                     const CUtensorMap *maps, int shape, cudaStream_t s)
+cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int total_items, bool skip_empty,
+                                     int log2_bpd, int nblocks, const Real *phi_in, Real *phi_out, const Real *H,
+                                     const Real *pw, const Real *pg, const unsigned short *meta, const Real *rho,
+                                     const double *dt, double ih2, bool clamped, unsigned *nan_flags,
+                                     unsigned *err_flag, const CUtensorMap *maps, int shape, cudaStream_t s)
 {
     if (nactive <= 0 || total_items <= 0) return cudaSuccess;
     if (log2_bpd < 0) return cudaErrorInvalidValue;
@@ -1300,6 +1301,7 @@ cudaError_t launch_rd_batch_step_tma(const BatchLists &bl, int nactive, int tota
     src.L = log2_bpd;
     src.nblocks = nblocks;
     src.nan_flags = nan_flags;
+    src.skip_empty = skip_empty;
     return with_shape_code<Real>(shape < 0 ? tma_shape_code() : shape, [&](auto sh) {
         return decltype(sh)::template launch<BatchSource<Real>>(src, total_items, ih2, clamped, err_flag, maps, s);
     });
@@ -1356,12 +1358,12 @@ template cudaError_t launch_rd_run_tma<double>(const PoolView<double> &, const B
                                                const double *, double *, double *, double *, int, double, double,
                                                unsigned *, unsigned *, unsigned *, const CUtensorMap *,
                                                const CUtensorMap *, const CUtensorMap *, cudaStream_t);
-template cudaError_t launch_rd_batch_step_tma<float>(const BatchLists &, int, int, int, int, const float *, float *,
-                                                     const float *, const float *, const float *,
+template cudaError_t launch_rd_batch_step_tma<float>(const BatchLists &, int, int, bool, int, int, const float *,
+                                                     float *, const float *, const float *, const float *,
                                                      const unsigned short *, const float *, const double *, double,
                                                      bool, unsigned *, unsigned *, const CUtensorMap *, int,
                                                      cudaStream_t);
-template cudaError_t launch_rd_batch_step_tma<double>(const BatchLists &, int, int, int, int, const double *,
+template cudaError_t launch_rd_batch_step_tma<double>(const BatchLists &, int, int, bool, int, int, const double *,
                                                       double *, const double *, const double *, const double *,
                                                       const unsigned short *, const double *, const double *, double,
                                                       bool, unsigned *, unsigned *, const CUtensorMap *, int,
