@@ -451,6 +451,7 @@ def adjoint_sample(stream, local, bpd=16, nsnap=64, check=True):
                     "between the two runs of a quotient",
             "adjoint": a64, "fd": chk["fd"], "rel_err": chk["rel_err"], "crossings": chk["crossings"],
             "fd_resolution": chk["fd_resolution"], "chain_rule_rel_err": chk["chain_rule_rel_err"],
+            "term_cancellation": chk["term_cancellation"],
             "forward_steps_run": chk["forward_steps"]}
         out["fp32_vs_fp64_rel"] = rel32
     return out
@@ -508,7 +509,7 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9, max
         torch.cuda.synchronize()
         return pool, cap_snap
 
-    def one(pool, cap_snap, prec, p_w, p_g, st, rng, masks=None):
+    def one(pool, cap_snap, prec, p_w, p_g, st, rng, masks=None, magnitudes=False):
         R = np.float32 if prec == "f32" else np.float64
         s = make_schedule(st.Dw_cm2_day, st.rho_day, st.tend_day, L_CM, bpd, prec)
         if max_steps is not None and s.nsteps > max_steps:
@@ -531,7 +532,7 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9, max
         e0, e1 = ev(), ev()
         e0.record(stream)
         res = pool.forward_adjoint(Dw, Dg, st.rho_day * 0.9, s.dt, s.nsteps, x0=st.x0, sigma=2.0 / n,
-                                   nsnapshots=max(1, nsnap))
+                                   nsnapshots=max(1, nsnap), term_magnitudes=magnitudes)
         e1.record(stream)
         torch.cuda.synchronize()
         return res, e0.elapsed_time(e1) / 1e3, s.nsteps, masks, nsnap
@@ -554,10 +555,14 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9, max
     p_w, p_g, st, r32, masks = first
     pool, cap64 = open_pool("f64")
     try:
-        r64 = one(pool, cap64, "f64", p_w, p_g, st, None, masks)[0]
+        r64 = one(pool, cap64, "f64", p_w, p_g, st, None, masks, magnitudes=True)[0]
     finally:
         pool.close()
     rel = {k: abs(r32[k] - r64[k]) / max(abs(r64[k]), 1e-300) for k in ("loss", "dDw", "drho")}
+    # sum of |term| over |sum of terms| in the FP64 run: a relative change e of
+    # the terms moves a gradient by up to e times this, relatively
+    cancel = {"dDw": r64["dDw_abs"] / max(abs(r64["dDw"]), 1e-300),
+              "drho": r64["drho_abs"] / max(abs(r64["drho"]), 1e-300)}
     alg = 9 * 4 * (n ** 3) * steps_total  # (4 forward + 5 adjoint) words per cell and step, FP32
     return {
         "workload": f"{nsamples} samples, forward + discrete adjoint at {n}^3, FP32 state, own anatomy each "
@@ -569,7 +574,9 @@ def adjoint_batch(stream, local, nsamples=16, bpd=32, seed=5, hbm_cap=160e9, max
         "gradient_samples_per_s": nsamples / t_total,
         "roofline": {"achieved": alg / t_total / 1e9, "peak": peak, "unit": "GB/s", "frac": alg / t_total / 1e9 / peak,
                      "algorithmic_bytes": "9 words (forward 4 + adjoint 5) x cells x steps; recomputation not counted"},
-        "fp32_vs_fp64_rel": rel, "per_sample": recs,
+        "fp32_vs_fp64_rel": rel, "term_cancellation_fp64": cancel,
+        "fp32_vs_fp64_rel_over_cancellation": {k: rel[k] / cancel[k] for k in cancel},
+        "per_sample": recs,
     }
 
 

@@ -102,6 +102,9 @@ class Sample(ctypes.Structure):
 # initial conditions of a batch sample (enum gbfk_ic)
 IC_KINDS = {"gaussian": 0, "ball": 1}
 
+# gbfk_adjoint_params.flags
+ADJ_TERM_MAGNITUDES = 1
+
 
 class AdjointParams(ctypes.Structure):
     _fields_ = [
@@ -109,6 +112,7 @@ class AdjointParams(ctypes.Structure):
         ("nsteps", ctypes.c_int), ("nsnapshots", ctypes.c_int),
         ("x0", ctypes.c_double * 3), ("sigma", ctypes.c_double),
         ("t1_uc", ctypes.c_double), ("t2_uc", ctypes.c_double), ("slope", ctypes.c_double),
+        ("flags", ctypes.c_int),
     ]
 
 
@@ -116,6 +120,7 @@ class AdjointResult(ctypes.Structure):
     _fields_ = [
         ("loss", ctypes.c_double), ("dDw", ctypes.c_double), ("drho", ctypes.c_double),
         ("dx0", ctypes.c_double * 3), ("forward_steps", ctypes.c_int64), ("adjoint_steps", ctypes.c_int64),
+        ("dDw_abs", ctypes.c_double), ("drho_abs", ctypes.c_double),
     ]
 
 

@@ -1331,6 +1331,7 @@ struct Adjoint {
     Real *T0, *T1, *T2, *LAM;
     std::vector<Real *> slots;
     double *grad_acc;
+    bool abs_terms = false;  // also sum the magnitudes of the gradient terms
     Real rho;
     double dt, Dw;
     int64_t fsteps = 0, asteps = 0;
@@ -1399,7 +1400,8 @@ struct Adjoint {
     {
         if (err != cudaSuccess) return;
         err = launch_adjoint_fused<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, phi_k, LAM, sets[latest],
-                                         sets[latest ^ 1], asteps == 0 ? 1 : 0, rho, dt, Dw, grad_acc, ctx->stream);
+                                         sets[latest ^ 1], asteps == 0 ? 1 : 0, abs_terms, rho, dt, Dw, grad_acc,
+                                         ctx->stream);
         latest ^= 1;
         ctx->launches++;
         asteps++;
@@ -1409,7 +1411,7 @@ struct Adjoint {
     {
         if (err != cudaSuccess || asteps == 0) return;
         err = launch_adjoint_fused<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, nullptr, LAM,
-                                         sets[latest], sets[latest ^ 1], 2, rho, dt, Dw, grad_acc, ctx->stream);
+                                         sets[latest], sets[latest ^ 1], 2, false, rho, dt, Dw, grad_acc, ctx->stream);
         ctx->launches++;
     }
     static double beta(int c, int r)  // C(c + r, c) = C(c + r, r), capped; 0 for r < 0
@@ -1563,6 +1565,7 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     e = cudaMemsetAsync(A.grad_acc, 0, (size_t)nb * kGradSlots * sizeof(double), ctx->stream);
     // forward steps on the pipelined kernel where it applies (bit-identical)
     A.X0 = X0;
+    A.abs_terms = (p->flags & GBFK_ADJ_TERM_MAGNITUDES) != 0;
     if (e == cudaSuccess && tma_step_eligible<Real>(A.v) && ctx->step_pref != GBFK_STEP_BLOCK) {
         rc = build_step_lists(ctx);
         if (rc) {
@@ -1692,6 +1695,12 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     res->loss = -(lik[1] + lik[2]);
     res->drho = nsum(acc.data(), kGradSlots, nb);
     res->dDw = nsum(acc.data() + 2, kGradSlots, nb);
+    res->drho_abs = res->dDw_abs = 0;
+    if (A.abs_terms)
+        for (int b = 0; b < nb; b++) {
+            res->drho_abs += acc[(size_t)b * kGradSlots + 4];
+            res->dDw_abs += acc[(size_t)b * kGradSlots + 5];
+        }
     for (int d = 0; d < 3; d++) res->dx0[d] = p->sigma > 0 ? nsum(xp.data() + 2 * d, 6, xparts) : 0.0;
     res->forward_steps = A.fsteps;
     res->adjoint_steps = A.asteps;
@@ -1708,7 +1717,8 @@ extern "C" int gbfk_forward_adjoint(gbfk_ctx *ctx, const gbfk_adjoint_params *p,
     if (!p || !out) return fail(ctx, GBFK_E_INVALID, "forward_adjoint: null argument");
     if (!ctx->uniform || !ctx->have_origin) return fail(ctx, GBFK_E_STATE, "forward_adjoint: needs a uniform power-of-two grid");
     if (ctx->obs_n != 8 * ctx->bpd) return fail(ctx, GBFK_E_STATE, "forward_adjoint: observations must be on the grid");
-    if (p->nsteps < 0 || p->nsnapshots < 1 || !(p->slope != 0) || !(p->Dw > 0))
+    if (p->nsteps < 0 || p->nsnapshots < 1 || !(p->slope != 0) || !(p->Dw > 0) ||
+        (p->flags & ~GBFK_ADJ_TERM_MAGNITUDES) != 0)
         return fail(ctx, GBFK_E_INVALID, "forward_adjoint: bad parameters");
     CK(cudaSetDevice(ctx->device));
     return ctx->precision == GBFK_F64 ? forward_adjoint_impl<double>(ctx, p, out, grad_c0)

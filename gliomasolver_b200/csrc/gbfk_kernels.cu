@@ -589,7 +589,9 @@ __device__ __forceinline__ int lab_a(int x, int y, int z) { return (x + 1) + kAP
 #define GBFK_ADJ_MIN_BLOCKS 8
 #endif
 
-template <typename Real, int kMode>  // kMode: 0 middle, 1 first (lambda_N given), 2 last (write lambda_0)
+// kMode: 0 middle, 1 first (lambda_N given), 2 last (write lambda_0); kAbs:
+// also sum the magnitudes of the gradient terms (grad_acc slots 4, 5)
+template <typename Real, int kMode, bool kAbs>
 __global__ void __launch_bounds__(128, sizeof(Real) == 4 ? GBFK_ADJ_MIN_BLOCKS : 8)
 adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
                  const double *__restrict__ ih2blk, const Real *__restrict__ phi, Real *__restrict__ lam,
@@ -598,7 +600,7 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
     __shared__ __align__(16) Real sm[kALab];  // phase A: mu of step k+1; phase B: phi_k
     __shared__ unsigned char sfl[kALab];
     __shared__ unsigned char sst[8];
-    __shared__ double red[4][4];
+    __shared__ double red[kAbs ? 6 : 4][4];
     pdl_wait_then_release();
     const int blk = blockIdx.x, t = threadIdx.x;
     const int64_t base = slot_of(v, blk) * kBS3;
@@ -756,6 +758,7 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
     __syncthreads();
     const Real eps = (Real)0.1;
     double grho = 0, grho_c = 0, gdw = 0, gdw_c = 0;
+    double arho = 0, adw = 0;  // kAbs
     bool nz = false;
     Real o[4];
     unsigned char fl[4];
@@ -822,8 +825,14 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
         fl[i] = f;
         sfo[i] = dom ? (double)mv * (-ih2 * sdf + (double)rho * (1. - 2. * (double)ph0)) : 0.;
         if (dom && pass) {
-            neumaier_add(grho, grho_c, (double)mv * dt * (double)ph0 * (1. - (double)ph0));
-            neumaier_add(gdw, gdw_c, (double)mv * dt * flux_diff * inv_Dw);
+            const double tr = (double)mv * dt * (double)ph0 * (1. - (double)ph0);
+            const double td = (double)mv * dt * flux_diff * inv_Dw;
+            neumaier_add(grho, grho_c, tr);
+            neumaier_add(gdw, gdw_c, td);
+            if (kAbs) {
+                arho += fabs(tr);
+                adw += fabs(td);
+            }
         }
     }
     // a block whose mu is zero everywhere writes neither mu, flags nor self terms
@@ -845,12 +854,20 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
         neumaier_add(grho, grho_c, a1);
         neumaier_add(gdw, gdw_c, b0);
         neumaier_add(gdw, gdw_c, b1);
+        if (kAbs) {
+            arho += __shfl_down_sync(0xffffffffu, arho, off);
+            adw += __shfl_down_sync(0xffffffffu, adw, off);
+        }
     }
     if ((t & 31) == 0) {
         red[0][t >> 5] = grho;
         red[1][t >> 5] = grho_c;
         red[2][t >> 5] = gdw;
         red[3][t >> 5] = gdw_c;
+        if constexpr (kAbs) {
+            red[4][t >> 5] = arho;
+            red[5][t >> 5] = adw;
+        }
     }
     __syncthreads();
     if (t == 0) {
@@ -865,25 +882,27 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
         neumaier_add(acc[0], acc[1], red[1][0]);
         neumaier_add(acc[2], acc[3], red[2][0]);
         neumaier_add(acc[2], acc[3], red[3][0]);
+        if constexpr (kAbs) {
+            acc[4] += red[4][0] + red[4][1] + red[4][2] + red[4][3];
+            acc[5] += red[5][0] + red[5][1] + red[5][2] + red[5][3];
+        }
     }
 }
 
 template <typename Real>
 cudaError_t launch_adjoint_fused(const PoolView<Real> &v, const Real *H, const unsigned short *meta,
                                  const double *ih2, const Real *phi, Real *lam, const AdjBuffers &prev,
-                                 const AdjBuffers &out, int mode, Real rho, double dt, double Dw, double *grad_acc,
-                                 cudaStream_t s)
+                                 const AdjBuffers &out, int mode, bool abs_terms, Real rho, double dt, double Dw,
+                                 double *grad_acc, cudaStream_t s)
 {
     if (v.nblocks <= 0) return cudaSuccess;
     const AdjSet a = {prev.mu, prev.self, prev.flags, prev.status}, b = {out.mu, out.self, out.flags, out.status};
-    if (mode == 1)
-        return launch_pdl(adj_fused_kernel<Real, 1>, v.nblocks, 128, s, v, H, meta, ih2, phi, lam, a, b, rho, dt,
-                          1. / Dw, grad_acc);
-    if (mode == 2)
-        return launch_pdl(adj_fused_kernel<Real, 2>, v.nblocks, 128, s, v, H, meta, ih2, phi, lam, a, b, rho, dt,
-                          1. / Dw, grad_acc);
-    return launch_pdl(adj_fused_kernel<Real, 0>, v.nblocks, 128, s, v, H, meta, ih2, phi, lam, a, b, rho, dt,
-                      1. / Dw, grad_acc);
+    auto go = [&](auto kernel) {
+        return launch_pdl(kernel, v.nblocks, 128, s, v, H, meta, ih2, phi, lam, a, b, rho, dt, 1. / Dw, grad_acc);
+    };
+    if (mode == 1) return abs_terms ? go(adj_fused_kernel<Real, 1, true>) : go(adj_fused_kernel<Real, 1, false>);
+    if (mode == 2) return go(adj_fused_kernel<Real, 2, false>);  // no step: no gradient terms
+    return abs_terms ? go(adj_fused_kernel<Real, 0, true>) : go(adj_fused_kernel<Real, 0, false>);
 }
 
 // dL/du of loss = -(L_T1c + L_FLAIR) (HGG_Likelihood.cpp:136-156) on a
@@ -1331,7 +1350,7 @@ cudaError_t upload_ghost_table()
     template cudaError_t launch_rd_batch_step<Real>(const BatchView<Real> &, int, int, int, cudaStream_t);      \
     template cudaError_t launch_adjoint_fused<Real>(const PoolView<Real> &, const Real *, const unsigned short *,  \
                                                     const double *, const Real *, Real *, const AdjBuffers &,      \
-                                                    const AdjBuffers &, int, Real, double, double, double *,       \
+                                                    const AdjBuffers &, int, bool, Real, double, double, double *, \
                                                     cudaStream_t);                                                 \
     template cudaError_t launch_loss_grad<Real>(int, const Real *, const unsigned char *, const unsigned char *, \
                                                 const int *, double, double, double, Real *, cudaStream_t);  \

@@ -15,7 +15,8 @@ constexpr int kLab3 = 1000;
 constexpr int kLabGhosts = 488;
 constexpr int kFaceCells = 64;
 constexpr int kFacesPerBlock = 3 * 576;  // x, y, z faces of a block incl. its boundary faces
-constexpr int kGradSlots = 4;            // adjoint gradient partials per block: rho (sum, comp), Dw (sum, comp)
+constexpr int kGradSlots = 6;            // adjoint gradient partials per block: rho (sum, comp), Dw (sum, comp),
+                                         // and the sums of the magnitudes of their terms (rho, Dw)
 
 // cell classes for the step's exact shortcuts (see cell_class)
 constexpr unsigned char kEmpty = 0, kTissue = 1, kOther = 2;
@@ -198,8 +199,9 @@ cudaError_t launch_likelihood(const double *model, int n, const unsigned char *t
 // double-buffered: per cell mu (Real), the self term (double) and the switch
 // flags, per block the status.  mode 1: the first step, lambda' from lam
 // (the loss gradient); mode 0: lambda' from prev; mode 2: no step, lambda
-// from prev written to lam (lambda_0).  grad_acc: nblocks * 4 doubles (rho
-// sum/comp, Dw sum/comp), accumulated per block.
+// from prev written to lam (lambda_0).  grad_acc: nblocks * kGradSlots
+// doubles (rho sum/comp, Dw sum/comp, and with abs_terms the sums of the
+// terms' magnitudes for rho and Dw), accumulated per block.
 constexpr int kAdjFlagBytesPerBlock = kBS3 + 1;  // cell flags, then the block's status
 struct AdjBuffers {
     void *mu;
@@ -210,8 +212,8 @@ struct AdjBuffers {
 template <typename Real>
 cudaError_t launch_adjoint_fused(const PoolView<Real> &v, const Real *H, const unsigned short *meta,
                                  const double *ih2, const Real *phi, Real *lam, const AdjBuffers &prev,
-                                 const AdjBuffers &out, int mode, Real rho, double dt, double Dw, double *grad_acc,
-                                 cudaStream_t s);
+                                 const AdjBuffers &out, int mode, bool abs_terms, Real rho, double dt, double Dw,
+                                 double *grad_acc, cudaStream_t s);
 // dL/dphi of loss = -(L_T1c + L_FLAIR) in pool order; roi_count: NULL (every
 // voxel once) or how often the ROI lists each voxel of the dense grid
 template <typename Real>

@@ -59,11 +59,15 @@ def check_gradients(pool: BlockPool, p_w, p_g, Dw, rho, dt, nsteps, x0, sigma, n
     R = pool.dtype
     Dg = float(R(0.1 * np.float64(Dw)))
     adj = pool.forward_adjoint(Dw, Dg, rho, dt, nsteps, x0=x0, sigma=sigma, nsnapshots=nsnapshots, t1_uc=t1_uc,
-                               t2_uc=t2_uc, slope=slope, grad_c0=True)
+                               t2_uc=t2_uc, slope=slope, grad_c0=True, term_magnitudes=True)
     n = pool.n
     c0 = gaussian_ic(n, x0, sigma, p_w, p_g)
     out = {"loss": adj["loss"], "adjoint": {"dDw": adj["dDw"], "drho": adj["drho"], "dx0": list(adj["dx0"])},
-           "forward_steps": adj["forward_steps"], "fd": {}, "rel_err": {}, "crossings": {}}
+           "forward_steps": adj["forward_steps"], "fd": {}, "rel_err": {}, "crossings": {},
+           # sum of |term| over |sum of terms|: how much a relative change of the
+           # terms (FP32 states) can move each gradient, relatively
+           "term_cancellation": {"dDw": adj["dDw_abs"] / max(abs(adj["dDw"]), 1e-300),
+                                 "drho": adj["drho_abs"] / max(abs(adj["drho"]), 1e-300)}}
     # dL/dx0 = sum_i dL/dc0_i * dc0_i/dx0 with dc0/dx0_d = c0 (x_d - x0_d) / sigma^2: the origin
     # gradient against the adjoint state at t = 0
     x = np.arange(n, dtype=np.float64) / n

@@ -234,18 +234,22 @@ class BlockPool:
 
     # -- discrete adjoint ---------------------------------------------------
     def forward_adjoint(self, Dw, Dg, rho, dt, nsteps, x0=(0.0, 0.0, 0.0), sigma=0.0, nsnapshots=64, t1_uc=0.7,
-                        t2_uc=0.25, slope=2.0, grad_c0=False):
+                        t2_uc=0.25, slope=2.0, grad_c0=False, term_magnitudes=False):
         """Loss -(L_T1c + L_FLAIR) at the horizon and its gradients (gbfk_forward_adjoint).
-        Returns a dict; with grad_c0 the dense d loss / d c0 is included."""
+        Returns a dict; with grad_c0 the dense d loss / d c0 is included, with
+        term_magnitudes the sums of the magnitudes of the dDw and drho terms
+        ("dDw_abs", "drho_abs")."""
         p = _lib.AdjointParams(float(Dw), float(Dg), float(rho), float(dt), int(nsteps), int(nsnapshots),
                                (ctypes.c_double * 3)(*[float(v) for v in x0]), float(sigma), float(t1_uc),
-                               float(t2_uc), float(slope))
+                               float(t2_uc), float(slope), _lib.ADJ_TERM_MAGNITUDES if term_magnitudes else 0)
         r = _lib.AdjointResult()
         g = np.empty((self.n, self.n, self.n), dtype=self.dtype) if grad_c0 else None
         self._check(self.lib.gbfk_forward_adjoint(self.ctx, ctypes.byref(p), ctypes.byref(r),
                                                   None if g is None else _ptr(g)))
         out = {"loss": r.loss, "dDw": r.dDw, "drho": r.drho, "dx0": np.array(list(r.dx0)),
                "forward_steps": int(r.forward_steps), "adjoint_steps": int(r.adjoint_steps)}
+        if term_magnitudes:
+            out["dDw_abs"], out["drho_abs"] = r.dDw_abs, r.drho_abs
         if g is not None:
             out["grad_c0"] = g
         return out

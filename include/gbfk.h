@@ -321,13 +321,20 @@ typedef struct {
     double sigma;           /* > 0: c0 = exp(-|x-x0|^2/(2 sigma^2)) where p_w+p_g > 0;
                                <= 0: c0 = the context's current phi */
     double t1_uc, t2_uc, slope; /* Bernoulli loss parameters */
+    int flags;              /* 0, or GBFK_ADJ_TERM_MAGNITUDES */
 } gbfk_adjoint_params;
+/* Also sum the magnitudes of the terms of dDw and drho (one per domain cell
+ * and step): |dDw| / dDw_abs near 0 means the terms cancel, and a relative
+ * change e of the terms (the rounding of FP32 states) can move dDw by up to
+ * e * dDw_abs. */
+#define GBFK_ADJ_TERM_MAGNITUDES 1
 typedef struct {
     double loss;            /* -(L_T1c + L_FLAIR) at the horizon */
     double dDw, drho;       /* d loss / d Dw (with Dg = 0.1 Dw), d loss / d rho */
     double dx0[3];          /* d loss / d x0 (0 when sigma <= 0) */
     int64_t forward_steps;  /* forward steps run, recomputation included */
     int64_t adjoint_steps;
+    double dDw_abs, drho_abs; /* with GBFK_ADJ_TERM_MAGNITUDES: the sums of the terms' magnitudes; else 0 */
 } gbfk_adjoint_result;
 /* grad_c0_dense: NULL, or n^3 Real (x fastest) receiving d loss / d c0. */
 int gbfk_forward_adjoint(gbfk_ctx *ctx, const gbfk_adjoint_params *params, gbfk_adjoint_result *out,

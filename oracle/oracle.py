@@ -179,10 +179,11 @@ def log_likelihood(model, t1c, flair, pet=None, roi=None, pet_sigma2=0.000361, p
     return np.array([float(out[0]), float(out[1]), float(out[2])])
 
 
-def adjoint_dense(pw, pg, phi0, Dw, Dg, rho, h, dt, nsteps, lam_final):
+def adjoint_dense(pw, pg, phi0, Dw, Dg, rho, h, dt, nsteps, lam_final, magnitudes=False):
     """The discrete adjoint of nsteps FP64 steps (orc_adjoint_step_dense_f64,
     every state stored): returns (dL/dphi0, dL/drho, dL/dDw) for a loss whose
-    gradient with respect to the final state is lam_final."""
+    gradient with respect to the final state is lam_final; with magnitudes
+    also the sums of the magnitudes of the dL/drho and dL/dDw terms."""
     L = lib()
     n = phi0.shape[0]
     pw, pg = (np.ascontiguousarray(a, dtype=np.float64) for a in (pw, pg))
@@ -190,11 +191,13 @@ def adjoint_dense(pw, pg, phi0, Dw, Dg, rho, h, dt, nsteps, lam_final):
     for _ in range(nsteps):
         states.append(rd_steps_dense(pw, pg, states[-1], Dw, Dg, rho, h, dt, 1))
     lam = np.array(lam_final, dtype=np.float64, copy=True)
-    grad = np.zeros(2)
+    grad = np.zeros(4)
     scratch = np.empty(8 * n ** 3)
     for k in range(nsteps - 1, -1, -1):
         L.orc_adjoint_step_dense_f64(n, _p(pw), _p(pg), _p(states[k]), float(Dw), float(Dg), float(rho), float(h),
                                      float(dt), _p(lam), _p(grad), _p(scratch))
+    if magnitudes:
+        return lam, float(grad[0]), float(grad[1]), float(grad[2]), float(grad[3])
     return lam, float(grad[0]), float(grad[1])
 
 

@@ -498,7 +498,7 @@ ORC_MAP_ANATOMY(f32, float, sqrtf)
  * phi is the state the step maps forward; lam holds dL/dphi' on entry and
  * dL/dphi on exit; scratch holds 8 n^3 doubles. */
 void orc_adjoint_step_dense_f64(int n, const double *pw, const double *pg, const double *phi, double Dw,
-                                double Dg, double rho, double h, double dt, double *lam, double grad[2],
+                                double Dg, double rho, double h, double dt, double *lam, double grad[4],
                                 double *scratch)
 {
     const int64_t nn = n, N = nn * nn * nn;
@@ -542,8 +542,11 @@ void orc_adjoint_step_dense_f64(int n, const double *pw, const double *pg, const
                 dom[c] = d;
                 for (int k = 0; k < 6; k++) dfs[6 * c + k] = df[k];
                 if (d && pass) {
-                    grad[0] += mu[c] * dt * p[0] * (1. - p[0]);
-                    grad[1] += mu[c] * dt * diff / Dw;
+                    const double tr = mu[c] * dt * p[0] * (1. - p[0]), td = mu[c] * dt * diff / Dw;
+                    grad[0] += tr;
+                    grad[1] += td;
+                    grad[2] += fabs(tr);
+                    grad[3] += fabs(td);
                 }
             }
     for (int iz = 0; iz < n; iz++)

@@ -131,10 +131,10 @@ void orc_map_anatomy_f32(int bpd, int sx, int sy, int sz, const double *gm, cons
 
 /* One step of the discrete adjoint of the fused step, FP64, dense periodic
  * grid (switches held fixed; see rd_oracle.c): lam holds dL/dphi' on entry,
- * dL/dphi on exit; grad[0] += dL/drho, grad[1] += dL/dDw (Dg = 0.1 Dw);
- * scratch: 8 n^3 doubles. */
+ * dL/dphi on exit; grad[0] += dL/drho, grad[1] += dL/dDw (Dg = 0.1 Dw),
+ * grad[2], grad[3] += the magnitudes of those terms; scratch: 8 n^3 doubles. */
 void orc_adjoint_step_dense_f64(int n, const double *pw, const double *pg, const double *phi, double Dw,
-                                double Dg, double rho, double h, double dt, double *lam, double grad[2],
+                                double Dg, double rho, double h, double dt, double *lam, double grad[4],
                                 double *scratch);
 /* dL/du of loss = -(L_T1c + L_FLAIR) (HGG_Likelihood.cpp:136-156). */
 void orc_loss_grad_f64(int64_t ncells, const double *u, const double *t1c, const double *flair, double t1uc,

@@ -202,6 +202,15 @@ def test_adjoint_equals_the_oracle_adjoint():
     assert np.linalg.norm(g - lam0) <= 1e-13 * np.linalg.norm(lam0)
     assert dev["drho"] == pytest.approx(drho, rel=1e-12)
     assert dev["dDw"] == pytest.approx(ddw, rel=1e-12)
+    # the magnitudes of the gradient terms (GBFK_ADJ_TERM_MAGNITUDES): the same
+    # gradients bit for bit, and the oracle's sums of |term|
+    pool.upload_dense("phi", c0)
+    dev_m = pool.forward_adjoint(Dw, Dg, rho, sched.dt, NSTEPS, sigma=0.0, nsnapshots=6, term_magnitudes=True, **UC)
+    assert all(dev_m[k] == dev[k] for k in ("loss", "dDw", "drho"))
+    _, _, _, arho, adw = O.adjoint_dense(pw, pg, c0, Dw, Dg, rho, 1.0 / N, sched.dt, NSTEPS, lam_t, magnitudes=True)
+    assert arho >= abs(drho) and adw >= abs(ddw)
+    assert dev_m["drho_abs"] == pytest.approx(arho, rel=1e-12)
+    assert dev_m["dDw_abs"] == pytest.approx(adw, rel=1e-12)
     # the origin: c0 = exp(-|x - x0|^2 / (2 sigma^2)), dc0/dx0_d = c0 (x_d - x0_d) / sigma^2
     dev_x = pool.forward_adjoint(Dw, Dg, rho, sched.dt, NSTEPS, x0=x0, sigma=sigma, nsnapshots=6, **UC)
     want = [np.sum(lam0 * c0 * (xs[d] - x0[d])) / sigma ** 2 for d in range(3)]

@@ -88,3 +88,25 @@ def test_origin_gradient_through_the_initial_condition():
         e[d] = 1e-7
         fd = (loss(x0 + e) - loss(x0 - e)) / 2e-7
         assert abs(fd - grad[d]) <= 1e-5 * abs(fd) + 1e-6, (d, fd, grad[d])
+
+
+def test_transposed_step_amplifies_next_to_the_no_flux_switch():
+    """Why config 5's gradients are ill-conditioned: the no-flux switch
+    (ReactionDiffusionOperator.h:166-181) doubles the coefficient opposite a
+    neighbour whose chf is below 0.1, so the step's transpose is not a
+    contraction.  With the state positive in every tissue cell (mu = lambda
+    there), one adjoint step of lambda = 1 gives the column sums of the step's
+    Jacobian: they exceed 1 + dt rho (the bound of its row sums) next to
+    those faces, and repeated steps grow lambda."""
+    n = 32
+    pw, pg, _, _ = make_case(n, 3)
+    s = make_schedule(0.23, 0.0057, 250.0, 25.6, n // 8, "f64")
+    tissue = (pw + pg) > 0
+    phi = np.where(tissue, 1e-300, 0.0)
+    lam = np.ones_like(phi)
+    col = O.adjoint_dense(pw, pg, phi, s.Dw, s.Dg, s.rho, s.h, s.dt, 1, lam)[0]
+    bound = 1.0 + s.dt * s.rho
+    assert col[tissue].max() > 1.04 * bound
+    assert np.count_nonzero(col[tissue] > bound * (1 + 1e-12)) > 1000
+    lam = O.adjoint_dense(pw, pg, phi, s.Dw, s.Dg, s.rho, s.h, s.dt, 200, np.ones_like(phi))[0]
+    assert lam.max() > 2.0
