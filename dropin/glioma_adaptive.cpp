@@ -13,6 +13,7 @@
  * end.
  *
  *   glioma_adaptive <in.bin> <maxlevel> <refine_tol> <compress_tol> <nsteps> <every> <out.bin>
+ *                   [<Dw cm^2/day> <rho /day>]
  *
  * in.bin: int32 n, then p_w, p_g, phi as n^3 float64 each, x fastest,
  * n = 8 * 2^maxlevel.  The grid starts at level 2 (4^3 blocks, periodic,
@@ -22,16 +23,21 @@
  * Science::AutomaticCompression (the driver's set-up before its time loop,
  * :311-313); the leaves then move to the GPU.  Then <nsteps> RD steps; after
  * every <every> steps one loop of refinement (the driver's in-loop call,
- * :325) and compression to convergence (its commented-out call, :326).
- * Coefficients: Dw = 0.2 cm^2/day on L = 25.6 cm, Dg = Dw/10, rho = 0.05/day,
- * dt = the reference's CFL formula (:304-307) with h of the finest level
- * (the driver's h of the initial grid is unstable once blocks reach level 5).
+ * :325) and compression to convergence (its commented-out call, :326);
+ * <every> = 0 keeps the set-up's grid for the whole run.
+ * Coefficients: Dw = 0.2 cm^2/day (or the optional argument) on L = 25.6 cm,
+ * Dg = Dw/10, rho = 0.05/day (or the optional argument), dt = the
+ * reference's CFL formula (:304-307) with h of the finest level (the
+ * driver's h of the initial grid is unstable once blocks reach level 5).
  *
  * Prints one JSON line: blocks and an FNV-1a hash of the sorted
  * (level, index) leaf list after every adaptation; seconds of device stepping,
  * of the adaptation and of its parts; the decisions whose detail lay within
  * 1e-6 (relative) of its tolerance.  Writes phi sampled on the finest uniform
- * grid as int32 n + n^3 float64, x fastest.
+ * grid as int32 n + n^3 float64, x fastest (each leaf cell's value on the r^3
+ * finest cells it covers, r = 2^(maxlevel - level), its own position
+ * origin + h * index being the first of them), and the leaves' levels on
+ * the same grid to <out.bin>.levels (n^3 int8).
  */
 #include <algorithm>
 #include <cmath>
@@ -49,6 +55,15 @@ typedef Grid<W, B> GridT;
 static int maxStencil[2][3] = {{-1, -1, -1}, {+2, +2, +2}};
 static int g_n = 0;
 static std::vector<double> g_pw, g_pg, g_phi;
+
+/* %.6e, or null for a value JSON cannot hold (a margin no decision set) */
+static std::string json_number(double v)
+{
+    if (!std::isfinite(v)) return "null";
+    char b[32];
+    snprintf(b, sizeof b, "%.6e", v);
+    return b;
+}
 
 static void die(const std::string &m)
 {
@@ -120,6 +135,7 @@ static void write_finest(GridT &grid, int maxLevel, const char *path)
 {
     const int n = g_n;
     std::vector<double> out((size_t)n * n * n, 0.0);
+    std::vector<signed char> lev((size_t)n * n * n, -1);
     std::vector<BlockInfo> vInfo = grid.getBlocksInfo();
     for (size_t i = 0; i < vInfo.size(); i++) {
         const BlockInfo &info = vInfo[i];
@@ -133,8 +149,11 @@ static void write_finest(GridT &grid, int maxLevel, const char *path)
                               z0 = (info.index[2] * 8 + iz) * r;
                     for (int dz = 0; dz < r; dz++)
                         for (int dy = 0; dy < r; dy++)
-                            for (int dx = 0; dx < r; dx++)
-                                out[(size_t)(x0 + dx) + (size_t)n * ((y0 + dy) + (size_t)n * (z0 + dz))] = v;
+                            for (int dx = 0; dx < r; dx++) {
+                                const size_t q = (size_t)(x0 + dx) + (size_t)n * ((y0 + dy) + (size_t)n * (z0 + dz));
+                                out[q] = v;
+                                lev[q] = (signed char)info.level;
+                            }
                 }
     }
     FILE *f = fopen(path, "wb");
@@ -142,18 +161,26 @@ static void write_finest(GridT &grid, int maxLevel, const char *path)
     fwrite(&n, sizeof(int), 1, f);
     fwrite(&out[0], 8, out.size(), f);
     fclose(f);
+    const std::string lp = std::string(path) + ".levels";
+    f = fopen(lp.c_str(), "wb");
+    if (!f) die("cannot write the level map");
+    fwrite(&lev[0], 1, lev.size(), f);
+    fclose(f);
 }
 
 int main(int argc, char **argv)
 {
-    if (argc != 8)
-        die("usage: glioma_adaptive <in.bin> <maxlevel> <refine_tol> <compress_tol> <nsteps> <every> <out.bin>");
+    if (argc != 8 && argc != 10)
+        die("usage: glioma_adaptive <in.bin> <maxlevel> <refine_tol> <compress_tol> <nsteps> <every> <out.bin> "
+            "[<Dw cm^2/day> <rho /day>]");
     read_dense(argv[1]);
     const int maxLevel = atoi(argv[2]);
     const double rtol = atof(argv[3]), ctol = atof(argv[4]);
     const int nsteps = atoi(argv[5]), every = atoi(argv[6]);
     if (g_n != 8 << maxLevel) die("the dense input must have 8 * 2^maxlevel cells per direction");
-    if (every <= 0 || nsteps < 0) die("bad arguments");
+    if (every < 0 || nsteps < 0) die("bad arguments");
+    const double Dw_day = argc == 10 ? atof(argv[8]) : 0.2, rho_day = argc == 10 ? atof(argv[9]) : 0.05;
+    if (!(Dw_day > 0) || !(rho_day >= 0)) die("bad coefficients");
 
     try {
         Refiner_SpaceExtension refiner(1, maxLevel);
@@ -167,9 +194,9 @@ int main(int argc, char **argv)
         Science::AutomaticCompression<0, 0>(grid, blockfwt, ctol, -1, NULL);
 
         const Real L = (Real)25.6;
-        const Real Dw = (Real)((Real)0.2 / (L * L));
+        const Real Dw = (Real)((Real)Dw_day / (L * L));
         const Real Dg = (Real)(0.1 * Dw);
-        const Real rho = (Real)0.05;
+        const Real rho = (Real)rho_day;
         const Real h = (Real)(1. / (8 << maxLevel));
         const Real dt = (Real)(0.99 * h * h / (2. * 3 * (Dw >= Dg ? Dw : Dg)));
 
@@ -193,13 +220,14 @@ int main(int argc, char **argv)
         long long cell_updates = 0;
         int changes = 0;
         for (int done = 0; done < nsteps;) {
-            const int k = std::min(every, nsteps - done);
+            const int k = every > 0 ? std::min(every, nsteps - done) : nsteps - done;
             const std::vector<BlockInfo> vInfo = rg.sync(grid);
             const double t0 = gbfk_mrag::wall_seconds();
             gbfk_mrag::ok(rg.ctx, gbfk_rd_step(rg.ctx, Dw, Dg, rho, dt, k, 1), "gbfk_rd_step");
             t_step += gbfk_mrag::wall_seconds() - t0;
             cell_updates += (long long)k * (long long)vInfo.size() * 512;
             done += k;
+            if (every == 0) break;  // the set-up's grid for the whole run
             const double ta = gbfk_mrag::wall_seconds();
             rg.adaptation++;
             gbfk_mrag::AutomaticRefinement(grid, rg, rtol, maxLevel, 1);
@@ -219,10 +247,11 @@ int main(int argc, char **argv)
                "\"topology_changes\": %d, \"uploads\": %d, \"upload_seconds\": %.6f, \"detail_sweeps\": %d, "
                "\"details_seconds\": %.6f, \"plan_seconds\": %.6f, \"splits\": %d, \"split_seconds\": %.6f, "
                "\"collapses\": %d, \"collapse_seconds\": %.6f, \"cell_updates\": %lld, "
-               "\"min_margin_refine\": %.6e, \"min_margin_compress\": %.6e, \"near_decisions\": %d, \"near\": [",
+               "\"min_margin_refine\": %s, \"min_margin_compress\": %s, \"near_decisions\": %d, \"near\": [",
                (int)sizeof(Real), maxLevel, nsteps, every, (double)dt, t_step, t_adapt, t_first_upload, changes,
                st.uploads, st.t_upload, st.detail_sweeps, st.t_details, st.t_plan, st.splits, st.t_split,
-               st.collapses, st.t_collapse, cell_updates, rg.min_margin_refine, rg.min_margin_compress,
+               st.collapses, st.t_collapse, cell_updates, json_number(rg.min_margin_refine).c_str(),
+               json_number(rg.min_margin_compress).c_str(),
                (int)rg.near.size());
         for (size_t i = 0; i < rg.near.size() && i < 200; i++) {
             const gbfk_mrag::NearDecision &d = rg.near[i];
