@@ -1332,6 +1332,10 @@ struct Adjoint {
     std::vector<Real *> slots;
     double *grad_acc;
     bool abs_terms = false;  // also sum the magnitudes of the gradient terms
+    // the blocks the adjoint steps run (NULL: all): every block that can hold
+    // a domain cell, and their face neighbours
+    const int *blocks = nullptr;
+    int nlaunch = 0;
     Real rho;
     double dt, Dw;
     int64_t fsteps = 0, asteps = 0;
@@ -1400,8 +1404,8 @@ struct Adjoint {
     {
         if (err != cudaSuccess) return;
         err = launch_adjoint_fused<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, phi_k, LAM, sets[latest],
-                                         sets[latest ^ 1], asteps == 0 ? 1 : 0, abs_terms, rho, dt, Dw, grad_acc,
-                                         ctx->stream);
+                                         sets[latest ^ 1], asteps == 0 ? 1 : 0, abs_terms, blocks, nlaunch, rho, dt,
+                                         Dw, grad_acc, ctx->stream);
         latest ^= 1;
         ctx->launches++;
         asteps++;
@@ -1410,8 +1414,12 @@ struct Adjoint {
     void finish()
     {
         if (err != cudaSuccess || asteps == 0) return;
+        // the blocks that are not run hold lambda_0 = 0
+        if (blocks) err = cudaMemsetAsync(LAM, 0, fbytes, ctx->stream);
+        if (err != cudaSuccess) return;
         err = launch_adjoint_fused<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, nullptr, LAM,
-                                         sets[latest], sets[latest ^ 1], 2, false, rho, dt, Dw, grad_acc, ctx->stream);
+                                         sets[latest], sets[latest ^ 1], 2, false, blocks, nlaunch, rho, dt, Dw,
+                                         grad_acc, ctx->stream);
         ctx->launches++;
     }
     static double beta(int c, int r)  // C(c + r, c) = C(c + r, r), capped; 0 for r < 0
@@ -1520,10 +1528,11 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     // sets; kept in the context between calls
     const int xparts = 148 * 4;
     const size_t selfbytes = (size_t)nb * kBS3 * sizeof(double);
-    const size_t sizes[15] = {A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes,
+    const size_t sizes[16] = {A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes, A.fbytes,
                               (size_t)nb * kAdjFlagBytesPerBlock, (size_t)nb * kGradSlots * sizeof(double),
                               (size_t)xparts * 6 * sizeof(double), 0, A.fbytes,
-                              (size_t)nb * kAdjFlagBytesPerBlock, selfbytes, selfbytes};
+                              (size_t)nb * kAdjFlagBytesPerBlock, selfbytes, selfbytes,
+                              (size_t)nb * (sizeof(int) + 1)};
     auto release = [&]() {
         cudaStreamSynchronize(ctx->stream);
         for (void *q : ctx->adj_mem)
@@ -1536,8 +1545,8 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     if (ctx->adj_fbytes != A.fbytes || ctx->adj_nblocks != nb || ctx->adj_nsnap < p->nsnapshots) {
         release();
         // the work fields one by one, the checkpoints in one allocation
-        ctx->adj_mem.assign(15, nullptr);
-        for (size_t i = 0; i < 15 && e == cudaSuccess; i++)
+        ctx->adj_mem.assign(16, nullptr);
+        for (size_t i = 0; i < 16 && e == cudaSuccess; i++)
             e = cudaMalloc(&ctx->adj_mem[i], i != 10 ? sizes[i] : A.fbytes * (size_t)p->nsnapshots);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -1590,6 +1599,46 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
             ctx->launches++;
         } else {
             e = cudaMemcpyAsync(X0, ctx->phi[ctx->cur], A.fbytes, cudaMemcpyDeviceToDevice, ctx->stream);
+        }
+    }
+    // the blocks the adjoint steps run: a block can hold a domain cell only if
+    // it has tissue (a heavy block) or a positive initial value (a kEmpty cell
+    // at +0 stays +0 and outside the domain); those and their face neighbours
+    // (whose lambda they feed).  The others keep status kAdjMuZero in both
+    // sets and lambda 0.
+    if (e == cudaSuccess && ctx->identity_slots) {
+        int *d_list = (int *)ctx->adj_mem[15];
+        unsigned char *d_pos = (unsigned char *)(d_list + nb);
+        std::vector<unsigned char> bt(nb), pos(nb);
+        std::vector<int> nbr((size_t)nb * 6);
+        e = launch_block_any_positive<Real>(X0, nb, d_pos, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(pos.data(), d_pos, nb, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(bt.data(), ctx->d_btype, nb, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(nbr.data(), ctx->d_nbr, nbr.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        ctx->launches++;
+        if (e == cudaSuccess) {
+            std::vector<unsigned char> run(nb, 0);
+            for (int b = 0; b < nb; b++) {
+                if (bt[b] == kBlockEmpty && !pos[b]) continue;
+                run[b] = 1;
+                for (int f = 0; f < 6; f++) {
+                    const int q = nbr[(size_t)b * 6 + f];
+                    if (q >= 0 && q < nb) run[q] = 1;
+                }
+            }
+            std::vector<int> list;
+            for (int b = 0; b < nb; b++)
+                if (run[b]) list.push_back(b);
+            if (!list.empty() && (int)list.size() < nb) {
+                e = cudaMemcpyAsync(d_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                    ctx->stream);
+                for (int k = 0; k < 2 && e == cudaSuccess; k++)
+                    e = cudaMemsetAsync(A.sets[k].status, kAdjMuZero, nb, ctx->stream);
+                A.blocks = d_list;
+                A.nlaunch = (int)list.size();
+            }
         }
     }
     // forward to the horizon (storing the first chain of checkpoints), loss and its gradient

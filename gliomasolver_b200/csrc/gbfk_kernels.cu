@@ -558,12 +558,6 @@ __device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
     s = t;
 }
 
-// Per-block status of an adjoint step: exactly one of 0 (mu not zero, no
-// domain cell), kAdjDom (mu not zero, a domain cell) and kAdjMuZero (mu is
-// zero in every cell; its mu values, cell flags and self terms are not
-// written, and the block contributes nothing to any lambda).
-constexpr unsigned char kAdjDom = 1;
-constexpr unsigned char kAdjMuZero = 2;
 
 struct AdjSet {
     void *mu;               // Real per cell (pool order)
@@ -595,14 +589,15 @@ template <typename Real, int kMode, bool kAbs>
 __global__ void __launch_bounds__(128, sizeof(Real) == 4 ? GBFK_ADJ_MIN_BLOCKS : 8)
 adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
                  const double *__restrict__ ih2blk, const Real *__restrict__ phi, Real *__restrict__ lam,
-                 AdjSet prev, AdjSet out, Real rho, double dt, double inv_Dw, double *__restrict__ grad_acc)
+                 AdjSet prev, AdjSet out, const int *__restrict__ blocks, Real rho, double dt, double inv_Dw,
+                 double *__restrict__ grad_acc)
 {
     __shared__ __align__(16) Real sm[kALab];  // phase A: mu of step k+1; phase B: phi_k
     __shared__ unsigned char sfl[kALab];
     __shared__ unsigned char sst[8];
     __shared__ double red[kAbs ? 6 : 4][4];
     pdl_wait_then_release();
-    const int blk = blockIdx.x, t = threadIdx.x;
+    const int blk = blocks ? blocks[blockIdx.x] : (int)blockIdx.x, t = threadIdx.x;
     const int64_t base = slot_of(v, blk) * kBS3;
     const int x = t & 7, y = (t >> 3) & 7, z0 = (t >> 6) * 4;
     const int c0 = x + kBS * (y + kBS * z0);  // cell i is c0 + 64 i
@@ -892,13 +887,14 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
 template <typename Real>
 cudaError_t launch_adjoint_fused(const PoolView<Real> &v, const Real *H, const unsigned short *meta,
                                  const double *ih2, const Real *phi, Real *lam, const AdjBuffers &prev,
-                                 const AdjBuffers &out, int mode, bool abs_terms, Real rho, double dt, double Dw,
-                                 double *grad_acc, cudaStream_t s)
+                                 const AdjBuffers &out, int mode, bool abs_terms, const int *blocks, int nlaunch,
+                                 Real rho, double dt, double Dw, double *grad_acc, cudaStream_t s)
 {
-    if (v.nblocks <= 0) return cudaSuccess;
+    const int grid = blocks ? nlaunch : v.nblocks;
+    if (grid <= 0) return cudaSuccess;
     const AdjSet a = {prev.mu, prev.self, prev.flags, prev.status}, b = {out.mu, out.self, out.flags, out.status};
     auto go = [&](auto kernel) {
-        return launch_pdl(kernel, v.nblocks, 128, s, v, H, meta, ih2, phi, lam, a, b, rho, dt, 1. / Dw, grad_acc);
+        return launch_pdl(kernel, grid, 128, s, v, H, meta, ih2, phi, lam, a, b, blocks, rho, dt, 1. / Dw, grad_acc);
     };
     if (mode == 1) return abs_terms ? go(adj_fused_kernel<Real, 1, true>) : go(adj_fused_kernel<Real, 1, false>);
     if (mode == 2) return go(adj_fused_kernel<Real, 2, false>);  // no step: no gradient terms
@@ -1341,6 +1337,27 @@ cudaError_t upload_ghost_table()
     return cudaMemcpyToSymbol(c_ghost_id, table, sizeof(table));
 }
 
+// out[b] = 1 when a cell of block b (pool order, identity slots) is > 0
+template <typename Real>
+__global__ void block_any_positive_kernel(const Real *__restrict__ phi, int nblocks, unsigned char *__restrict__ out)
+{
+    for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+        const Real *q = phi + (int64_t)b * kBS3;
+        bool any = false;
+        for (int c = threadIdx.x; c < kBS3; c += blockDim.x) any |= q[c] > (Real)0;
+        any = __syncthreads_or(any);
+        if (threadIdx.x == 0) out[b] = any ? 1 : 0;
+    }
+}
+
+template <typename Real>
+cudaError_t launch_block_any_positive(const Real *phi, int nblocks, unsigned char *out, cudaStream_t s)
+{
+    if (nblocks <= 0) return cudaSuccess;
+    block_any_positive_kernel<Real><<<nblocks < 148 * 16 ? nblocks : 148 * 16, 128, 0, s>>>(phi, nblocks, out);
+    return cudaGetLastError();
+}
+
 #define GBFK_INSTANTIATE(Real)                                                                               \
     template cudaError_t launch_rd_step<Real>(const PoolView<Real> &, const Real *, const unsigned short *,    \
                                               const double *, const Real *, Real *, Real *, Real, double,     \
@@ -1350,8 +1367,9 @@ cudaError_t upload_ghost_table()
     template cudaError_t launch_rd_batch_step<Real>(const BatchView<Real> &, int, int, int, cudaStream_t);      \
     template cudaError_t launch_adjoint_fused<Real>(const PoolView<Real> &, const Real *, const unsigned short *,  \
                                                     const double *, const Real *, Real *, const AdjBuffers &,      \
-                                                    const AdjBuffers &, int, bool, Real, double, double, double *, \
-                                                    cudaStream_t);                                                 \
+                                                    const AdjBuffers &, int, bool, const int *, int, Real, double, \
+                                                    double, double *, cudaStream_t);                               \
+    template cudaError_t launch_block_any_positive<Real>(const Real *, int, unsigned char *, cudaStream_t);      \
     template cudaError_t launch_loss_grad<Real>(int, const Real *, const unsigned char *, const unsigned char *, \
                                                 const int *, double, double, double, Real *, cudaStream_t);  \
     template cudaError_t launch_gaussian_ic<Real>(int, const Real *, const Real *, const double *, double, Real *, \

@@ -199,10 +199,20 @@ cudaError_t launch_likelihood(const double *model, int n, const unsigned char *t
 // double-buffered: per cell mu (Real), the self term (double) and the switch
 // flags, per block the status.  mode 1: the first step, lambda' from lam
 // (the loss gradient); mode 0: lambda' from prev; mode 2: no step, lambda
-// from prev written to lam (lambda_0).  grad_acc: nblocks * kGradSlots
+// from prev written to lam (lambda_0).  blocks: NULL (one CTA per block) or
+// the nlaunch blocks to run, one CTA each; every other block must hold
+// status kAdjMuZero in both sets and contribute nothing to the listed ones'
+// lambda (the caller's list: every block that can hold a domain cell, and
+// their face neighbours).  grad_acc: nblocks * kGradSlots
 // doubles (rho sum/comp, Dw sum/comp, and with abs_terms the sums of the
 // terms' magnitudes for rho and Dw), accumulated per block.
 constexpr int kAdjFlagBytesPerBlock = kBS3 + 1;  // cell flags, then the block's status
+// Per-block status of an adjoint step: exactly one of 0 (mu not zero, no
+// domain cell), kAdjDom (mu not zero, a domain cell) and kAdjMuZero (mu is
+// zero in every cell; its mu values, cell flags and self terms are not
+// written, and the block contributes nothing to any lambda).
+constexpr unsigned char kAdjDom = 1;
+constexpr unsigned char kAdjMuZero = 2;
 struct AdjBuffers {
     void *mu;
     double *self;
@@ -212,8 +222,11 @@ struct AdjBuffers {
 template <typename Real>
 cudaError_t launch_adjoint_fused(const PoolView<Real> &v, const Real *H, const unsigned short *meta,
                                  const double *ih2, const Real *phi, Real *lam, const AdjBuffers &prev,
-                                 const AdjBuffers &out, int mode, bool abs_terms, Real rho, double dt, double Dw,
-                                 double *grad_acc, cudaStream_t s);
+                                 const AdjBuffers &out, int mode, bool abs_terms, const int *blocks, int nlaunch,
+                                 Real rho, double dt, double Dw, double *grad_acc, cudaStream_t s);
+// out[b] = 1 when a cell of block b (identity slots) is > 0
+template <typename Real>
+cudaError_t launch_block_any_positive(const Real *phi, int nblocks, unsigned char *out, cudaStream_t s);
 // dL/dphi of loss = -(L_T1c + L_FLAIR) in pool order; roi_count: NULL (every
 // voxel once) or how often the ROI lists each voxel of the dense grid
 template <typename Real>
