@@ -1628,9 +1628,13 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
                     if (q >= 0 && q < nb) run[q] = 1;
                 }
             }
+            // blocks with tissue first: their CTAs do the long work, and the
+            // empty neighbours' short CTAs fill the slots they leave
             std::vector<int> list;
             for (int b = 0; b < nb; b++)
-                if (run[b]) list.push_back(b);
+                if (run[b] && bt[b] != kBlockEmpty) list.push_back(b);
+            for (int b = 0; b < nb; b++)
+                if (run[b] && bt[b] == kBlockEmpty) list.push_back(b);
             if (!list.empty() && (int)list.size() < nb) {
                 e = cudaMemcpyAsync(d_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice,
                                     ctx->stream);
