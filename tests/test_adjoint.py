@@ -159,7 +159,7 @@ def test_autograd_function():
     loss.backward()
     Dwr, Dgr = _coeffs(R, 0.16)
     ref = pool.forward_adjoint(Dwr, Dgr, 0.09, sched.dt, NSTEPS, x0=(0.5, 0.46, 0.5), sigma=2.0 / N, **UC)
-    assert float(loss) == ref["loss"]
+    assert float(loss.detach()) == ref["loss"]
     assert float(Dw.grad) == pytest.approx(ref["dDw"] / L ** 2, rel=1e-14)
     assert float(rho.grad) == ref["drho"]
     assert np.allclose(x0.grad.numpy(), ref["dx0"], rtol=1e-14)
@@ -362,7 +362,7 @@ def test_autograd_initial_field():
     Dwr, Dgr = _coeffs(R, 0.15)
     pool.upload_dense("phi", c0n)
     ref = pool.forward_adjoint(Dwr, Dgr, 0.08, sched.dt, NSTEPS, sigma=0.0, nsnapshots=7, grad_c0=True, **UC)
-    assert float(loss) == ref["loss"]
+    assert float(loss.detach()) == ref["loss"]
     assert np.array_equal(c0.grad.numpy(), 2.0 * ref["grad_c0"])
     assert float(rho.grad) == 2.0 * ref["drho"]
     assert float(Dw.grad) == pytest.approx(2.0 * ref["dDw"] / L ** 2, rel=1e-14)
