@@ -3,6 +3,8 @@
 #include "gbfk_exact.cuh"
 #include "gbfk_kernels.cuh"
 
+#include <type_traits>
+
 namespace gbfk {
 
 // Programmatic dependent launch (kernels launched by launch_pdl): wait until
@@ -578,15 +580,19 @@ constexpr int kALab = kAPlane * kLab;
 
 __device__ __forceinline__ int lab_a(int x, int y, int z) { return (x + 1) + kAPitch * (y + 1) + kAPlane * (z + 1); }
 
-// resident CTAs per SM the fused adjoint step's register allocation targets
-#ifndef GBFK_ADJ_MIN_BLOCKS
-#define GBFK_ADJ_MIN_BLOCKS 8
-#endif
+// Resident CTAs per SM the fused adjoint step's register allocation targets
+// (kCtas).  Measured on a B200 in FP32: 8 CTAs (64 registers, no spills) is
+// fastest while the fields stay in L2 (128^3: 0.299 s per config-4 gradient,
+// against 0.333 s with 10 and 0.355 s with 12); 12 CTAs (40 registers, a few
+// spilled) hide more DRAM latency on larger grids (16 x 256^3: 5.86 s against
+// 6.18 s with 8).  FP64 keeps 8.
+constexpr int kAdjCtasL2 = 8, kAdjCtasDram = 12;
+constexpr int kAdjDramBlocks = 16384;  // grids of at least this many blocks (FP32) use kAdjCtasDram
 
 // kMode: 0 middle, 1 first (lambda_N given), 2 last (write lambda_0); kAbs:
 // also sum the magnitudes of the gradient terms (grad_acc slots 4, 5)
-template <typename Real, int kMode, bool kAbs>
-__global__ void __launch_bounds__(128, sizeof(Real) == 4 ? GBFK_ADJ_MIN_BLOCKS : 8)
+template <typename Real, int kMode, bool kAbs, int kCtas>
+__global__ void __launch_bounds__(128, kCtas)
 adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned short *__restrict__ meta,
                  const double *__restrict__ ih2blk, const Real *__restrict__ phi, Real *__restrict__ lam,
                  AdjSet prev, AdjSet out, const int *__restrict__ blocks, Real rho, double dt, double inv_Dw,
@@ -896,9 +902,16 @@ cudaError_t launch_adjoint_fused(const PoolView<Real> &v, const Real *H, const u
     auto go = [&](auto kernel) {
         return launch_pdl(kernel, grid, 128, s, v, H, meta, ih2, phi, lam, a, b, blocks, rho, dt, 1. / Dw, grad_acc);
     };
-    if (mode == 1) return abs_terms ? go(adj_fused_kernel<Real, 1, true>) : go(adj_fused_kernel<Real, 1, false>);
-    if (mode == 2) return go(adj_fused_kernel<Real, 2, false>);  // no step: no gradient terms
-    return abs_terms ? go(adj_fused_kernel<Real, 0, true>) : go(adj_fused_kernel<Real, 0, false>);
+    auto pick = [&](auto ctas) {
+        constexpr int C = decltype(ctas)::value;
+        if (mode == 1)
+            return abs_terms ? go(adj_fused_kernel<Real, 1, true, C>) : go(adj_fused_kernel<Real, 1, false, C>);
+        if (mode == 2) return go(adj_fused_kernel<Real, 2, false, C>);  // no step: no gradient terms
+        return abs_terms ? go(adj_fused_kernel<Real, 0, true, C>) : go(adj_fused_kernel<Real, 0, false, C>);
+    };
+    if constexpr (sizeof(Real) == 4)
+        if (v.nblocks >= kAdjDramBlocks) return pick(std::integral_constant<int, kAdjCtasDram>());
+    return pick(std::integral_constant<int, kAdjCtasL2>());
 }
 
 // dL/du of loss = -(L_T1c + L_FLAIR) (HGG_Likelihood.cpp:136-156) on a
