@@ -134,16 +134,28 @@ def test_checkpoint_count_changes_cost_not_result():
 
 
 def test_fp32_state_against_fp64():
+    """FP32 state against FP64 on the same problem.  A gradient is a sum of
+    terms over cells and steps; a relative change e of the terms (the FP32
+    state's rounding) moves it by up to e * sum|term|, so the bound is scaled
+    by the cancellation sum|term| / |sum term| measured in FP64
+    (GBFK_ADJ_TERM_MAGNITUDES)."""
     res = {}
     for prec in ("f64", "f32"):
         pool, pw, pg, sched, t1, fl, R = _setup(prec, seed=5)
         Dw, Dg = _coeffs(R, 0.18)
         res[prec] = pool.forward_adjoint(Dw, Dg, 0.07, make_schedule(0.2, 0.1, 100.0, L, BPD, "f64").dt, NSTEPS,
-                                         x0=(0.5, 0.5, 0.5), sigma=2.0 / N, nsnapshots=8, **UC)
+                                         x0=(0.5, 0.5, 0.5), sigma=2.0 / N, nsnapshots=8,
+                                         term_magnitudes=prec == "f64", **UC)
         pool.close()
-    for k in ("loss", "dDw", "drho"):
-        assert res["f32"][k] == pytest.approx(res["f64"][k], rel=2e-3), k
-    assert np.allclose(res["f32"]["dx0"], res["f64"]["dx0"], rtol=2e-3, atol=1e-3 * np.abs(res["f64"]["dx0"]).max())
+    a, b = res["f64"], res["f32"]
+    cancel = {k: a[k + "_abs"] / abs(a[k]) for k in ("dDw", "drho")}
+    rel = {k: abs(b[k] - a[k]) / abs(a[k]) for k in ("loss", "dDw", "drho")}
+    print(cancel, rel)
+    assert rel["loss"] <= 1e-5
+    for k in ("dDw", "drho"):
+        assert cancel[k] >= 1.0
+        assert rel[k] <= 1e-5 * cancel[k], k
+    assert np.allclose(b["dx0"], a["dx0"], rtol=2e-3, atol=1e-3 * np.abs(a["dx0"]).max())
 
 
 def test_autograd_function():
