@@ -598,18 +598,28 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
                  AdjSet prev, AdjSet out, const int *__restrict__ blocks, Real rho, double dt, double inv_Dw,
                  double *__restrict__ grad_acc)
 {
+    // FP32: the block's face coefficients in shared memory, copied before the
+    // wait for the previous launch (they are fixed for the whole run, and so
+    // are the block list and 1/h^2); FP64 reads them from global memory
+    constexpr bool kHsm = sizeof(Real) == 4;
     __shared__ __align__(16) Real sm[kALab];  // phase A: mu of step k+1; phase B: phi_k
+    __shared__ __align__(16) Real sH[kHsm ? kFacesPerBlock : 1];
     __shared__ unsigned char sfl[kALab];
     __shared__ unsigned char sst[8];
     __shared__ double red[kAbs ? 6 : 4][4];
-    pdl_wait_then_release();
     const int blk = blocks ? blocks[blockIdx.x] : (int)blockIdx.x, t = threadIdx.x;
+    const double ih2 = ih2blk[blk];
+    if constexpr (kHsm) {
+        static_assert(kFacesPerBlock % 4 == 0, "float4 copies");
+        const float4 *src = reinterpret_cast<const float4 *>(H + (int64_t)blk * kFacesPerBlock);
+        for (int q = t; q < kFacesPerBlock / 4; q += blockDim.x) reinterpret_cast<float4 *>(sH)[q] = src[q];
+    }
+    pdl_wait_then_release();
     const int64_t base = slot_of(v, blk) * kBS3;
     const int x = t & 7, y = (t >> 3) & 7, z0 = (t >> 6) * 4;
     const int c0 = x + kBS * (y + kBS * z0);  // cell i is c0 + 64 i
     const int l0 = lab_a(x, y, z0);            // lab cell i is l0 + kAPlane i
-    const double ih2 = ih2blk[blk];
-    const Real *Hb = H + (int64_t)blk * kFacesPerBlock;
+    const Real *Hb = kHsm ? sH : H + (int64_t)blk * kFacesPerBlock;
     const int ln[6] = {-1, 1, -kAPitch, kAPitch, -kAPlane, kAPlane};
 
     // ---- phase A: lambda_{k+1} of this block -------------------------------
