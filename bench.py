@@ -436,6 +436,8 @@ def adjoint_sample(stream, local, bpd=16, nsnap=64, check=True):
         "gradient_s": t_adj, "gradient_samples_per_s": 1.0 / t_adj,
         "plain_forward_s": t_fwd, "plain_forward_samples_per_s": 1.0 / t_fwd,
         "gradient_cost_in_forward_solves": t_adj / t_fwd,
+        "forward_steps_note": "the gradient's forward steps run only the blocks with tissue once every empty block "
+                              "holds its final +0; the plain forward solve steps every block",
         "all_states": None if all_states is None else dict(
             all_states, gradient_cost_in_forward_solves=all_states["gradient_s"] / t_fwd),
         "loss": res["loss"], "dDw": res["dDw"], "drho": res["drho"], "dx0": list(res["dx0"]),

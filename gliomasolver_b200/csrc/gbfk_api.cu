@@ -7,12 +7,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 namespace gbfk {
@@ -118,6 +120,11 @@ struct gbfk_ctx {
     std::vector<void *> adj_mem;
     size_t adj_fbytes = 0;
     int adj_nblocks = 0, adj_nsnap = 0;
+    // the adjoint's state buffers whose empty blocks hold +0 (forward steps
+    // into them may skip those blocks), valid for the step lists of
+    // generation adj_clean_gen
+    std::unordered_set<const void *> adj_clean;
+    int64_t lists_gen = 0, adj_clean_gen = -1;
     // gbfk_rd_step_host: an input and an output copy stream, two sets of
     // staging buffers and their events (set k & 1 serves call k)
     cudaStream_t io_in_stream = nullptr, io_out_stream = nullptr;
@@ -505,6 +512,7 @@ int build_step_lists(gbfk_ctx *ctx)
     ctx->n_heavy = nh;
     ctx->n_empty = nb - nh;
     ctx->lists_valid = true;
+    ctx->lists_gen++;
     ctx->h_lists.swap(lists);
     ctx->run_layout_valid = false;
     return GBFK_OK;
@@ -583,7 +591,7 @@ int rd_step_impl(gbfk_ctx *ctx, double Dw, double Dg, double rho, double dt, int
         }
         if (pipelined) {
             CK(launch_rd_step_tma<Real>(v, lists, (const Real *)ctx->d_H, ctx->d_meta, ih2, in, clamped, out,
-                                        (Real)rho, dt, ctx->d_nan, ctx->d_nan + 1, ctx->tma_maps[ctx->cur],
+                                        (Real)rho, dt, ctx->d_nan, ctx->d_nan + 1, ctx->tma_maps[ctx->cur], false,
                                         ctx->stream));
             ctx->launches++;
             ctx->cur ^= 1;
@@ -1366,14 +1374,22 @@ struct Adjoint {
         return it == map_index.end() ? nullptr : maps[it->second].m;
     }
 
+    // skip_empty: every empty block of the initial condition holds +0 (and
+    // dt is finite), so every step writes +0 there; a step then runs only the
+    // heavy blocks when its output buffer's empty blocks already hold +0
+    // (ctx->adj_clean), which every full step into a buffer establishes
+    bool skip_empty = false;
+    bool clean(const void *b) const { return skip_empty && (b == X0 || ctx->adj_clean.count(b) != 0); }
     void step(const Real *in, Real *out)
     {
         if (err != cudaSuccess) return;
         const CUtensorMap *m = pipelined ? maps_of(in) : nullptr;
-        if (m)
+        if (m) {
+            const bool skip = skip_empty && clean(in) && clean(out);
             err = launch_rd_step_tma<Real>(v, lists, (const Real *)ctx->d_H, ctx->d_meta, ih2, in, in != X0, out, rho,
-                                           dt, ctx->d_nan, ctx->d_nan + 1, m, ctx->stream);
-        else
+                                           dt, ctx->d_nan, ctx->d_nan + 1, m, skip, ctx->stream);
+            if (skip_empty) ctx->adj_clean.insert(out);
+        } else
             err = launch_rd_step<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, in, out, nullptr, rho, dt,
                                        ctx->d_nan, ctx->stream);
         fsteps++;
@@ -1385,7 +1401,11 @@ struct Adjoint {
     {
         if (err != cudaSuccess) return;
         if (k == 0) {
-            if (src != dst) err = cudaMemcpyAsync(dst, src, fbytes, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (src != dst) {
+                err = cudaMemcpyAsync(dst, src, fbytes, cudaMemcpyDeviceToDevice, ctx->stream);
+                if (clean(src)) ctx->adj_clean.insert(dst);
+                else ctx->adj_clean.erase(dst);
+            }
             return;
         }
         const Real *cur = src;
@@ -1540,8 +1560,10 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
         ctx->adj_mem.clear();
         ctx->adj_fbytes = 0;
         ctx->adj_nblocks = ctx->adj_nsnap = 0;
+        ctx->adj_clean.clear();
     };
     cudaError_t e = cudaSuccess;
+    bool fresh = false;  // buffers allocated (and zeroed) by this call
     if (ctx->adj_fbytes != A.fbytes || ctx->adj_nblocks != nb || ctx->adj_nsnap < p->nsnapshots) {
         release();
         // the work fields one by one, the checkpoints in one allocation
@@ -1556,6 +1578,16 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
         ctx->adj_fbytes = A.fbytes;
         ctx->adj_nblocks = nb;
         ctx->adj_nsnap = p->nsnapshots;
+        // the forward states start at +0 everywhere: every later step into
+        // them may skip the empty blocks (see Adjoint::skip_empty)
+        for (int i : {0, 1, 2, 3, 4})
+            if (e == cudaSuccess) e = cudaMemsetAsync(ctx->adj_mem[i], 0, A.fbytes, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->adj_mem[10], 0, A.fbytes * (size_t)p->nsnapshots, ctx->stream);
+        if (e != cudaSuccess) {
+            release();
+            return fail(ctx, GBFK_E_CUDA, "forward_adjoint: %s", cudaGetErrorString(e));
+        }
+        fresh = true;
     }
     auto cleanup = [&]() { cudaStreamSynchronize(ctx->stream); };
     Real *X0 = (Real *)ctx->adj_mem[0], *F = (Real *)ctx->adj_mem[1];
@@ -1582,6 +1614,16 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
             return rc;
         }
         A.lists = {ctx->d_lists, ctx->n_heavy, ctx->d_lists + ctx->n_heavy, ctx->n_empty};
+        // which blocks are empty changes with the lists: buffers known to hold
+        // +0 in the old empty blocks are not known to in the new ones
+        if (ctx->adj_clean_gen != ctx->lists_gen) {
+            ctx->adj_clean.clear();
+            ctx->adj_clean_gen = ctx->lists_gen;
+        }
+        if (fresh) {
+            ctx->adj_clean.insert({(const void *)F, (const void *)A.T0, (const void *)A.T1, (const void *)A.T2});
+            for (Real *b : A.slots) ctx->adj_clean.insert(b);
+        }
         const double h = sizeof(Real) == 8 ? ctx->h_h[0] : (double)(float)ctx->h_h[0];
         A.ih2 = 1. / (h * h);
         const Real *inputs[] = {X0, A.T0, A.T1};
@@ -1606,6 +1648,7 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     // at +0 stays +0 and outside the domain); those and their face neighbours
     // (whose lambda they feed).  The others keep status kAdjMuZero in both
     // sets and lambda 0.
+    bool ic_clean = false;  // every empty block of the initial condition holds +0
     if (e == cudaSuccess && ctx->identity_slots) {
         int *d_list = (int *)ctx->adj_mem[15];
         unsigned char *d_pos = (unsigned char *)(d_list + nb);
@@ -1619,6 +1662,9 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         ctx->launches++;
         if (e == cudaSuccess) {
+            ic_clean = true;
+            for (int b = 0; b < nb; b++)
+                if (bt[b] == kBlockEmpty && pos[b]) ic_clean = false;
             std::vector<unsigned char> run(nb, 0);
             for (int b = 0; b < nb; b++) {
                 if (bt[b] == kBlockEmpty && !pos[b]) continue;
@@ -1645,6 +1691,11 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
             }
         }
     }
+    // forward steps skip the empty blocks where that gives the same bits; a
+    // tumour outside the anatomy (or a non-finite dt) may write into them,
+    // after which no buffer is known to hold +0 there
+    A.skip_empty = e == cudaSuccess && A.pipelined && ic_clean && std::isfinite(p->dt);
+    if (!A.skip_empty) ctx->adj_clean.clear();  // full steps: nothing is tracked
     // forward to the horizon (storing the first chain of checkpoints), loss and its gradient
     if (e == cudaSuccess) {
         A.sweep(X0, F, p->nsteps, p->nsnapshots);

@@ -93,7 +93,9 @@ cudaError_t launch_rd_step(const PoolView<Real> &v, const Real *H, const unsigne
 // phi_in (make_pool_tensor_maps); ih2: the grid's 1/(h*h); clamped: phi_in
 // is the output of a step (every value +0 <= phi <= 1 or NaN), which lets
 // the kernel skip the negativity tests; err_flag: set when a wait of the
-// pipeline timed out.
+// pipeline timed out; skip_empty: the empty blocks of phi_in and phi_out
+// already hold +0 (and the step would keep it: dt finite), so only the heavy
+// blocks run.
 struct BlockLists {
     const int *heavy;
     int n_heavy;
@@ -106,7 +108,7 @@ template <typename Real>
 cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const BlockLists &lists, const Real *H,
                                const unsigned short *meta, double ih2, const Real *phi_in, bool clamped,
                                Real *phi_out, Real rho, double dt, unsigned *nan_flag, unsigned *err_flag,
-                               const CUtensorMap *maps, cudaStream_t s);
+                               const CUtensorMap *maps, bool skip_empty, cudaStream_t s);
 cudaError_t make_pool_tensor_maps(void *base, int nslots, int real_bytes, CUtensorMap maps[3]);
 // A run of nsteps (2 .. kMaxRunSteps) steps of the pipelined step in one
 // cooperative launch: in0 (the output of a step) -> buf0 -> buf1 -> buf0 ...,

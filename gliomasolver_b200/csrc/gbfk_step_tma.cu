@@ -1155,15 +1155,16 @@ template <typename Real>
 cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const BlockLists &lists, const Real *H,
                                const unsigned short *meta, double ih2, const Real *phi_in, bool clamped,
                                Real *phi_out, Real rho, double dt, unsigned *nan_flag, unsigned *err_flag,
-                               const CUtensorMap *maps, cudaStream_t s)
+                               const CUtensorMap *maps, bool skip_empty, cudaStream_t s)
 {
     if (lists.n_heavy + lists.n_empty <= 0) return cudaSuccess;
     if (!tma_step_eligible(v) || lists.n_heavy + lists.n_empty != v.nblocks) return cudaErrorInvalidValue;
+    if (skip_empty && lists.n_heavy <= 0) return cudaSuccess;
     PoolSource<Real> src;
     src.heavy = lists.heavy;
     src.empty = lists.empty;
     src.nh = lists.n_heavy;
-    src.ne = lists.n_empty;
+    src.ne = skip_empty ? 0 : lists.n_empty;
     src.phi_in = phi_in;
     src.phi_out = phi_out;
     src.H = H;
@@ -1175,8 +1176,9 @@ cudaError_t launch_rd_step_tma(const PoolView<Real> &v, const BlockLists &lists,
     src.L = v.log2_bpd;
     src.nblocks = v.nblocks;
     src.nan_flag = nan_flag;
+    const int items = src.nh + src.ne;
     return with_shape<Real>([&](auto sh) {
-        return decltype(sh)::template launch<PoolSource<Real>>(src, v.nblocks, ih2, clamped, err_flag, maps, s);
+        return decltype(sh)::template launch<PoolSource<Real>>(src, items, ih2, clamped, err_flag, maps, s);
     });
 }
 
@@ -1339,10 +1341,11 @@ template bool tma_step_eligible<float>(const PoolView<float> &);
 template bool tma_step_eligible<double>(const PoolView<double> &);
 template cudaError_t launch_rd_step_tma<float>(const PoolView<float> &, const BlockLists &, const float *,
                                                const unsigned short *, double, const float *, bool, float *, float,
-                                               double, unsigned *, unsigned *, const CUtensorMap *, cudaStream_t);
+                                               double, unsigned *, unsigned *, const CUtensorMap *, bool,
+                                               cudaStream_t);
 template cudaError_t launch_rd_step_tma<double>(const PoolView<double> &, const BlockLists &, const double *,
                                                 const unsigned short *, double, const double *, bool, double *,
-                                                double, double, unsigned *, unsigned *, const CUtensorMap *,
+                                                double, double, unsigned *, unsigned *, const CUtensorMap *, bool,
                                                 cudaStream_t);
 template cudaError_t rd_run_layout<float>(const PoolView<float> &, const int *, int, const int *, int, int &,
                                           std::vector<int> &, std::vector<int> &);

@@ -232,23 +232,28 @@ def test_adjoint_equals_the_oracle_adjoint():
 
 
 def test_adjoint_with_empty_blocks_skipped_equals_the_oracle():
-    """At 64^3 most blocks outside the brain hold neither tissue nor tumour;
-    the adjoint steps run only the blocks that can hold a domain cell and
-    their face neighbours, the rest keep lambda = 0.  Against the oracle's
-    dense adjoint, with tumour planted in a block outside the anatomy (a
-    kEmpty cell with phi > 0 is inside the domain): dL/dc0 as a whole field,
-    dL/dDw, dL/drho."""
+    """At 64^3 most blocks outside the brain hold neither tissue nor tumour.
+    The adjoint steps run only the blocks that can hold a domain cell and
+    their face neighbours (the rest keep lambda = 0), and, when every empty
+    block of the initial condition holds +0, the forward steps of the sweep
+    run only the heavy blocks (the empty ones keep their +0).  Against the
+    oracle's dense adjoint on one pool, in turn: tumour planted in a block
+    outside the anatomy (a kEmpty cell with phi > 0 is inside the domain; no
+    forward step skips), then the same anatomy without it (the forward steps
+    skip, into buffers the first call wrote), then the first case again:
+    dL/dc0 as a whole field, dL/dDw, dL/drho."""
     from gliomasolver_b200 import BlockPool
 
     n, bpd, nsteps = 64, 8, 30
     pw, pg, _ = make_anatomy(n, 4)
-    c0 = tumor_ic(n, (0.5, 0.5, 0.5), pw, pg)
+    clean = tumor_ic(n, (0.5, 0.5, 0.5), pw, pg)
     out = (pw + pg) == 0
     assert out[2:6, 2:6, 2:6].all() and out[:8, :8, :8].all()
-    c0[2:6, 2:6, 2:6] = 0.3          # tumour outside the anatomy, in corner block 0
+    planted = clean.copy()
+    planted[2:6, 2:6, 2:6] = 0.3     # tumour outside the anatomy, in corner block 0
     sched = make_schedule(0.2, 0.1, 100.0, L, bpd, "f64")
-    u = O.rd_steps_dense(pw, pg, c0, sched.Dw, sched.Dg, sched.rho, 1.0 / n, sched.dt, nsteps)
     rng = np.random.default_rng(3)
+    u = O.rd_steps_dense(pw, pg, planted, sched.Dw, sched.Dg, sched.rho, 1.0 / n, sched.dt, nsteps)
     t1, fl = (u > 0.7).astype(float), (u > 0.25).astype(float)
     for m in (t1, fl):
         flip = rng.random(m.shape) < 0.02
@@ -258,18 +263,22 @@ def test_adjoint_with_empty_blocks_skipped_equals_the_oracle():
         pool.upload_dense("p_w", pw)
         pool.upload_dense("p_g", pg)
         pool.set_observations(t1, fl)
-        pool.upload_dense("phi", c0)
-        dev = pool.forward_adjoint(sched.Dw, sched.Dg, sched.rho, sched.dt, nsteps, sigma=0.0, nsnapshots=5,
-                                   grad_c0=True, **UC)
-    lam_t = O.loss_grad(u, t1, fl, UC["t1_uc"], UC["t2_uc"], UC["slope"])
-    lam0, drho, ddw = O.adjoint_dense(pw, pg, c0, sched.Dw, sched.Dg, sched.rho, 1.0 / n, sched.dt, nsteps, lam_t)
-    g = dev["grad_c0"]
-    assert np.count_nonzero(lam0[:8, :8, :8]) > 0      # the planted tumour's block carries an adjoint
-    assert np.count_nonzero(lam0 == 0) > n ** 3 // 4    # and most of the outside none
-    assert np.linalg.norm(g - lam0) <= 1e-13 * np.linalg.norm(lam0)
-    assert np.array_equal(g == 0, lam0 == 0)
-    assert dev["drho"] == pytest.approx(drho, rel=1e-12)
-    assert dev["dDw"] == pytest.approx(ddw, rel=1e-12)
+        for c0 in (planted, clean, planted):
+            pool.upload_dense("phi", c0)
+            dev = pool.forward_adjoint(sched.Dw, sched.Dg, sched.rho, sched.dt, nsteps, sigma=0.0, nsnapshots=5,
+                                       grad_c0=True, **UC)
+            u = O.rd_steps_dense(pw, pg, c0, sched.Dw, sched.Dg, sched.rho, 1.0 / n, sched.dt, nsteps)
+            lam_t = O.loss_grad(u, t1, fl, UC["t1_uc"], UC["t2_uc"], UC["slope"])
+            lam0, drho, ddw = O.adjoint_dense(pw, pg, c0, sched.Dw, sched.Dg, sched.rho, 1.0 / n, sched.dt, nsteps,
+                                              lam_t)
+            g = dev["grad_c0"]
+            if c0 is planted:
+                assert np.count_nonzero(lam0[:8, :8, :8]) > 0  # the planted tumour's block carries an adjoint
+            assert np.count_nonzero(lam0 == 0) > n ** 3 // 4    # and most of the outside none
+            assert np.linalg.norm(g - lam0) <= 1e-13 * np.linalg.norm(lam0)
+            assert np.array_equal(g == 0, lam0 == 0)
+            assert dev["drho"] == pytest.approx(drho, rel=1e-12)
+            assert dev["dDw"] == pytest.approx(ddw, rel=1e-12)
 
 
 @pytest.mark.skipif(not O.ref_available("f64"), reason="oracle/_ref is built only where the reference sources are")
