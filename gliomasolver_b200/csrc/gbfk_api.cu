@@ -9,8 +9,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -125,6 +127,12 @@ struct gbfk_ctx {
     // generation adj_clean_gen
     std::unordered_set<const void *> adj_clean;
     int64_t lists_gen = 0, adj_clean_gen = -1;
+    // the forward steps of gbfk_forward_adjoint run on adj_fstream, the
+    // adjoint steps on `stream`; per state buffer one event for its last
+    // forward write and one for its last adjoint read, and a fork/join event
+    cudaStream_t adj_fstream = nullptr;
+    std::unordered_map<const void *, cudaEvent_t> adj_ev_write, adj_ev_read;
+    cudaEvent_t adj_ev_join = nullptr;
     // gbfk_rd_step_host: an input and an output copy stream, two sets of
     // staging buffers and their events (set k & 1 serves call k)
     cudaStream_t io_in_stream = nullptr, io_out_stream = nullptr;
@@ -816,6 +824,13 @@ int gbfk_destroy(gbfk_ctx *ctx)
         cudaStreamDestroy(ctx->io_in_stream);
         cudaStreamDestroy(ctx->io_out_stream);
     }
+    if (ctx->adj_fstream) {
+        cudaStreamSynchronize(ctx->adj_fstream);
+        cudaStreamDestroy(ctx->adj_fstream);
+    }
+    for (auto *m : {&ctx->adj_ev_write, &ctx->adj_ev_read})
+        for (auto &kv : *m) cudaEventDestroy(kv.second);
+    if (ctx->adj_ev_join) cudaEventDestroy(ctx->adj_ev_join);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return GBFK_OK;
@@ -1380,6 +1395,61 @@ struct Adjoint {
     // (ctx->adj_clean), which every full step into a buffer establishes
     bool skip_empty = false;
     bool clean(const void *b) const { return skip_empty && (b == X0 || ctx->adj_clean.count(b) != 0); }
+
+    // Two streams: forward steps on fs, adjoint steps on ctx->stream, so that
+    // the recomputation of the states ahead can overlap the adjoint steps
+    // (both are latency-bound on small grids).  The only buffers both touch
+    // are the states the adjoint steps read: an adjoint step waits for the
+    // forward write of its state, a forward write waits for the adjoint reads
+    // before it (one event per buffer and kind, re-recorded; a wait binds the
+    // record before it).  fs == ctx->stream runs everything in one stream.
+    cudaStream_t fs = nullptr;
+    std::unordered_set<const void *> wait_write, wait_read;  // records not yet waited for
+    cudaEvent_t event_of(std::unordered_map<const void *, cudaEvent_t> &m, const void *b)
+    {
+        auto it = m.find(b);
+        if (it != m.end()) return it->second;
+        cudaEvent_t e = nullptr;
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        if (err != cudaSuccess) return nullptr;
+        m[b] = e;
+        return e;
+    }
+    void forward_writes(const void *dst)  // before a forward op writes dst
+    {
+        if (fs == ctx->stream || err != cudaSuccess || !wait_read.erase(dst)) return;
+        cudaEvent_t e = event_of(ctx->adj_ev_read, dst);
+        if (e) err = cudaStreamWaitEvent(fs, e, 0);
+    }
+    void forward_wrote(const void *dst)
+    {
+        if (fs == ctx->stream || err != cudaSuccess) return;
+        cudaEvent_t e = event_of(ctx->adj_ev_write, dst);
+        if (e) err = cudaEventRecord(e, fs);
+        wait_write.insert(dst);
+    }
+    void adjoint_reads(const void *b)  // before an op on ctx->stream reads b
+    {
+        if (fs == ctx->stream || err != cudaSuccess || !wait_write.erase(b)) return;
+        cudaEvent_t e = event_of(ctx->adj_ev_write, b);
+        if (e) err = cudaStreamWaitEvent(ctx->stream, e, 0);
+    }
+    void adjoint_read(const void *b)
+    {
+        if (fs == ctx->stream || err != cudaSuccess) return;
+        cudaEvent_t e = event_of(ctx->adj_ev_read, b);
+        if (e) err = cudaEventRecord(e, ctx->stream);
+        wait_read.insert(b);
+    }
+    // `to` waits for everything enqueued on `from` so far
+    void join(cudaStream_t from, cudaStream_t to)
+    {
+        if (from == to || err != cudaSuccess) return;
+        if (!ctx->adj_ev_join) err = cudaEventCreateWithFlags(&ctx->adj_ev_join, cudaEventDisableTiming);
+        if (err == cudaSuccess) err = cudaEventRecord(ctx->adj_ev_join, from);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(to, ctx->adj_ev_join, 0);
+    }
+
     void step(const Real *in, Real *out)
     {
         if (err != cudaSuccess) return;
@@ -1387,11 +1457,11 @@ struct Adjoint {
         if (m) {
             const bool skip = skip_empty && clean(in) && clean(out);
             err = launch_rd_step_tma<Real>(v, lists, (const Real *)ctx->d_H, ctx->d_meta, ih2, in, in != X0, out, rho,
-                                           dt, ctx->d_nan, ctx->d_nan + 1, m, skip, ctx->stream);
+                                           dt, ctx->d_nan, ctx->d_nan + 1, m, skip, fs);
             if (skip_empty) ctx->adj_clean.insert(out);
         } else
             err = launch_rd_step<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, in, out, nullptr, rho, dt,
-                                       ctx->d_nan, ctx->stream);
+                                       ctx->d_nan, fs);
         fsteps++;
         ctx->launches++;
     }
@@ -1402,19 +1472,38 @@ struct Adjoint {
         if (err != cudaSuccess) return;
         if (k == 0) {
             if (src != dst) {
-                err = cudaMemcpyAsync(dst, src, fbytes, cudaMemcpyDeviceToDevice, ctx->stream);
+                forward_writes(dst);
+                if (err == cudaSuccess) err = cudaMemcpyAsync(dst, src, fbytes, cudaMemcpyDeviceToDevice, fs);
                 if (clean(src)) ctx->adj_clean.insert(dst);
                 else ctx->adj_clean.erase(dst);
+                forward_wrote(dst);
             }
             return;
         }
+        forward_writes(dst);
         const Real *cur = src;
         for (int s = 0; s < k; s++) {
             Real *out = (s == k - 1) ? dst : (cur == T0 ? T1 : T0);
             step(cur, out);
             cur = out;
         }
+        forward_wrote(dst);
     }
+    // The checkpoint buffers the schedule may fill, first in, first out (the
+    // buffer released longest ago, whose adjoint reads are most likely done).
+    // The schedule never holds more than the checkpoint count.
+    std::deque<Real *> free_slots;
+    Real *take_slot()
+    {
+        if (free_slots.empty()) {
+            if (err == cudaSuccess) err = cudaErrorInvalidValue;
+            return T2;
+        }
+        Real *s = free_slots.front();
+        free_slots.pop_front();
+        return s;
+    }
+    void release_slot(Real *s) { free_slots.push_back(s); }
     // the adjoint state between launches (double-buffered); `latest` is the
     // set the last launch wrote
     AdjBuffers sets[2];
@@ -1423,9 +1512,12 @@ struct Adjoint {
     void adjoint_step(const Real *phi_k)
     {
         if (err != cudaSuccess) return;
+        adjoint_reads(phi_k);
+        if (err != cudaSuccess) return;
         err = launch_adjoint_fused<Real>(v, (const Real *)ctx->d_H, ctx->d_meta, ctx->d_ih2, phi_k, LAM, sets[latest],
                                          sets[latest ^ 1], asteps == 0 ? 1 : 0, abs_terms, blocks, nlaunch, rho, dt,
                                          Dw, grad_acc, ctx->stream);
+        adjoint_read(phi_k);
         latest ^= 1;
         ctx->launches++;
         asteps++;
@@ -1488,9 +1580,11 @@ struct Adjoint {
             c--;
         }
         advance(cur, F, nsteps - pos);
+        free_slots.assign(slots.begin(), slots.begin() + c);
     }
     // reverse() along the chain stored by sweep(): slots[c-1] already holds
-    // the state a + split(b - a, c, true).
+    // the state a + split(b - a, c, true); that buffer is free once the part
+    // of the chain after it is reversed.
     void reverse_chain(int a, int b, int c, Real *X)
     {
         const int l = b - a;
@@ -1501,10 +1595,11 @@ struct Adjoint {
         const int l1 = split(l, c, true);
         Real *S = slots[c - 1];
         reverse_chain(a + l1, b, c - 1, S);
+        release_slot(S);
         reverse(a, a + l1, c, X);
     }
     // X holds phi_a; LAM holds dL/dphi_b on entry and dL/dphi_a on exit;
-    // slots[0..c) are free.
+    // c checkpoint buffers are free.
     void reverse(int a, int b, int c, Real *X)
     {
         const int l = b - a;
@@ -1522,9 +1617,10 @@ struct Adjoint {
             return;
         }
         const int l1 = split(l, c, false);
-        Real *S = slots[c - 1];
+        Real *S = take_slot();
         advance(X, S, l1);
         reverse(a + l1, b, c - 1, S);
+        release_slot(S);
         reverse(a, a + l1, c, X);
     }
 };
@@ -1555,6 +1651,7 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
                               (size_t)nb * (sizeof(int) + 1)};
     auto release = [&]() {
         cudaStreamSynchronize(ctx->stream);
+        if (ctx->adj_fstream) cudaStreamSynchronize(ctx->adj_fstream);
         for (void *q : ctx->adj_mem)
             if (q) cudaFree(q);
         ctx->adj_mem.clear();
@@ -1589,7 +1686,20 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
         }
         fresh = true;
     }
-    auto cleanup = [&]() { cudaStreamSynchronize(ctx->stream); };
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(ctx->stream);
+        if (ctx->adj_fstream) cudaStreamSynchronize(ctx->adj_fstream);
+    };
+    // the forward steps' own stream (GBFK_ADJ_STREAMS=1: everything on ctx->stream)
+    A.fs = ctx->stream;
+    if (const char *s = getenv("GBFK_ADJ_STREAMS"); !(s && atoi(s) == 1)) {
+        if (!ctx->adj_fstream) e = cudaStreamCreateWithFlags(&ctx->adj_fstream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            ctx->adj_fstream = nullptr;
+            return fail(ctx, GBFK_E_CUDA, "forward_adjoint: %s", cudaGetErrorString(e));
+        }
+        A.fs = ctx->adj_fstream;
+    }
     Real *X0 = (Real *)ctx->adj_mem[0], *F = (Real *)ctx->adj_mem[1];
     A.T0 = (Real *)ctx->adj_mem[2];
     A.T1 = (Real *)ctx->adj_mem[3];
@@ -1645,42 +1755,34 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     }
     // the blocks the adjoint steps run: a block can hold a domain cell only if
     // it has tissue (a heavy block) or a positive initial value (a kEmpty cell
-    // at +0 stays +0 and outside the domain); those and their face neighbours
-    // (whose lambda they feed).  The others keep status kAdjMuZero in both
-    // sets and lambda 0.
+    // at +0 stays +0 and outside the domain).  The others have lambda = mu = 0
+    // at every step: their cells are outside the domain with phi = +0, so
+    // mu = lambda' [0 < phi <= 1] = 0, and every face coefficient that
+    // couples them to a neighbour is exactly 0 (a kBlockEmpty block's cells
+    // and face halos have p_w = p_g = 0, so both diffusivities of such a face
+    // are 0 and its harmonic mean is 0), so no neighbour feeds their lambda.
+    // They keep status kAdjMuZero in both sets and lambda 0.
     bool ic_clean = false;  // every empty block of the initial condition holds +0
     if (e == cudaSuccess && ctx->identity_slots) {
         int *d_list = (int *)ctx->adj_mem[15];
         unsigned char *d_pos = (unsigned char *)(d_list + nb);
         std::vector<unsigned char> bt(nb), pos(nb);
-        std::vector<int> nbr((size_t)nb * 6);
         e = launch_block_any_positive<Real>(X0, nb, d_pos, ctx->stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(pos.data(), d_pos, nb, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(bt.data(), ctx->d_btype, nb, cudaMemcpyDeviceToHost, ctx->stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(nbr.data(), ctx->d_nbr, nbr.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         ctx->launches++;
         if (e == cudaSuccess) {
             ic_clean = true;
             for (int b = 0; b < nb; b++)
                 if (bt[b] == kBlockEmpty && pos[b]) ic_clean = false;
-            std::vector<unsigned char> run(nb, 0);
-            for (int b = 0; b < nb; b++) {
-                if (bt[b] == kBlockEmpty && !pos[b]) continue;
-                run[b] = 1;
-                for (int f = 0; f < 6; f++) {
-                    const int q = nbr[(size_t)b * 6 + f];
-                    if (q >= 0 && q < nb) run[q] = 1;
-                }
-            }
-            // blocks with tissue first: their CTAs do the long work, and the
-            // empty neighbours' short CTAs fill the slots they leave
+            // blocks with tissue first, then empty blocks with a positive
+            // initial value (a tumour outside the anatomy)
             std::vector<int> list;
             for (int b = 0; b < nb; b++)
-                if (run[b] && bt[b] != kBlockEmpty) list.push_back(b);
+                if (bt[b] != kBlockEmpty) list.push_back(b);
             for (int b = 0; b < nb; b++)
-                if (run[b] && bt[b] == kBlockEmpty) list.push_back(b);
+                if (bt[b] == kBlockEmpty && pos[b]) list.push_back(b);
             if (!list.empty() && (int)list.size() < nb) {
                 e = cudaMemcpyAsync(d_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice,
                                     ctx->stream);
@@ -1698,7 +1800,9 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     if (!A.skip_empty) ctx->adj_clean.clear();  // full steps: nothing is tracked
     // forward to the horizon (storing the first chain of checkpoints), loss and its gradient
     if (e == cudaSuccess) {
+        A.join(ctx->stream, A.fs);
         A.sweep(X0, F, p->nsteps, p->nsnapshots);
+        A.adjoint_reads(F);
         e = A.err;
     }
     double lik[4] = {0, 0, 0, 0};
@@ -1756,6 +1860,7 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     }
     if (e == cudaSuccess) {
         A.finish();
+        A.join(A.fs, ctx->stream);
         e = A.err;
     }
     // parameter gradients
