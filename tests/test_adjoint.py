@@ -133,6 +133,31 @@ def test_checkpoint_count_changes_cost_not_result():
     pool.close()
 
 
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_forward_stream_of_its_own_gives_the_same_bits(prec, monkeypatch):
+    """The reverse sweep's recomputation on a stream of its own (the default)
+    and on the caller's stream (GBFK_ADJ_STREAMS=1) give the same bits, with
+    few checkpoint buffers (much recomputation, buffers reused first-in
+    first-out) and with every state kept."""
+    pool, pw, pg, sched, t1, fl, R = _setup(prec, seed=6)
+    Dw, Dg = _coeffs(R, 0.2)
+
+    def run(k):
+        return pool.forward_adjoint(Dw, Dg, 0.1, sched.dt, NSTEPS, x0=(0.5, 0.45, 0.5), sigma=2.0 / N,
+                                    nsnapshots=k, grad_c0=True, **UC)
+
+    for k in (2, 5, 64):
+        monkeypatch.delenv("GBFK_ADJ_STREAMS", raising=False)
+        two = run(k)
+        monkeypatch.setenv("GBFK_ADJ_STREAMS", "1")
+        one = run(k)
+        assert two["forward_steps"] == one["forward_steps"]
+        for key in ("loss", "dDw", "drho"):
+            assert two[key] == one[key], (k, key)
+        assert np.array_equal(two["dx0"], one["dx0"]) and np.array_equal(two["grad_c0"], one["grad_c0"])
+    pool.close()
+
+
 def test_fp32_state_against_fp64():
     """FP32 state against FP64 on the same problem.  A gradient is a sum of
     terms over cells and steps; a relative change e of the terms (the FP32
