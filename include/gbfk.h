@@ -312,7 +312,11 @@ int gbfk_batch_log_likelihood(gbfk_batch *b, const gbfk_likelihood_params *param
  * States are kept with binomial checkpointing in nsnapshots device buffers;
  * these and seven work fields stay allocated in the context until
  * gbfk_destroy, so that later calls on the same grid with at most as many
- * checkpoints allocate nothing. */
+ * checkpoints allocate nothing.  The forward steps of the reverse sweep run
+ * on a second stream of the context (created at the first call, ordered
+ * after the work already on the context's stream) next to the adjoint steps;
+ * the call returns when both are done.  GBFK_ADJ_STREAMS=1 keeps everything
+ * on the context's stream (the same results). */
 typedef struct {
     double Dw, Dg, rho, dt; /* rescaled Real coefficients and the time step */
     int nsteps;             /* steps to the horizon */
