@@ -722,8 +722,11 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
                 acc += sf[i];
 #pragma unroll
                 for (int k = 0; k < 6; k++) {
+                    // a neighbour outside the domain has mu = +0 (phi <= 0
+                    // there, so pre = phi fails 0 < pre), and ih2 H (+0) = +0
+                    // leaves acc (never -0: it starts at +0) unchanged, so its
+                    // domain bit need not be tested
                     const unsigned fi = sfl[l + ln[k]];
-                    if (!(fi & 1u)) continue;
                     const double hik = ((fi >> (1 + (k ^ 1))) & 1u) ? 2. * hf[k] : hf[k];
                     acc += ih2 * hik * (double)sm[l + ln[k]];
                 }
@@ -812,7 +815,10 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
 #pragma unroll
             for (int k = 0; k < 6; k++) {
                 bool slow;
-                if ((mw[i] >> (2 + k)) & 1u) {
+                if (bt == kBlockTissue) {  // block-uniform: every neighbour is kTissue
+                    low[k] = false;
+                    slow = !(phn[k] >= (Real)0);
+                } else if ((mw[i] >> (2 + k)) & 1u) {
                     low[k] = phn[k] < eps;
                     slow = false;
                 } else {
