@@ -560,6 +560,16 @@ __device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
     s = t;
 }
 
+// (s, c) += (xs, xc) for compensated sums: s + xs = t + e exactly (Knuth's
+// TwoSum, no branch), the rounding error e joins the compensation terms
+__device__ __forceinline__ void two_sum_add(double &s, double &c, double xs, double xc)
+{
+    const double t = s + xs;
+    const double bp = t - s;
+    const double e = (s - (t - bp)) + (xs - bp);
+    s = t;
+    c += xc + e;
+}
 
 struct AdjSet {
     void *mu;               // Real per cell (pool order)
@@ -865,8 +875,8 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
         if (dom && pass) {
             const double tr = (double)mv * dt * (double)ph0 * (1. - (double)ph0);
             const double td = (double)mv * dt * flux_diff * inv_Dw;
-            neumaier_add(grho, grho_c, tr);
-            neumaier_add(gdw, gdw_c, td);
+            two_sum_add(grho, grho_c, tr, 0.);
+            two_sum_add(gdw, gdw_c, td, 0.);
             if (kAbs) {
                 arho += fabs(tr);
                 adw += fabs(td);
@@ -888,10 +898,8 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
     for (int off = 16; off > 0; off >>= 1) {
         const double a0 = __shfl_down_sync(0xffffffffu, grho, off), a1 = __shfl_down_sync(0xffffffffu, grho_c, off);
         const double b0 = __shfl_down_sync(0xffffffffu, gdw, off), b1 = __shfl_down_sync(0xffffffffu, gdw_c, off);
-        neumaier_add(grho, grho_c, a0);
-        neumaier_add(grho, grho_c, a1);
-        neumaier_add(gdw, gdw_c, b0);
-        neumaier_add(gdw, gdw_c, b1);
+        two_sum_add(grho, grho_c, a0, a1);
+        two_sum_add(gdw, gdw_c, b0, b1);
         if (kAbs) {
             arho += __shfl_down_sync(0xffffffffu, arho, off);
             adw += __shfl_down_sync(0xffffffffu, adw, off);
