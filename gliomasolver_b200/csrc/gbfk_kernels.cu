@@ -599,6 +599,36 @@ __device__ __forceinline__ int lab_a(int x, int y, int z) { return (x + 1) + kAP
 constexpr int kAdjCtasL2 = 8, kAdjCtasDram = 12;
 constexpr int kAdjDramBlocks = 16384;  // grids of at least this many blocks (FP32) use kAdjCtasDram
 
+// Face-halo cell i (0..2) of thread t of the adjoint's 128-thread CTA: cell
+// t & 63 of face f = 2 i + (t >> 6) (i = 0: x-, x+; 1: y-, y+; 2: z-, z+),
+// the cell face_cell(f, t & 63) gives, with its lab position, its cell in the
+// neighbour and the neighbour face_neighbour(v, blk, f) gives.  Written with
+// the direction i explicit, which the unrolled loops make a constant.
+template <typename Real>
+__device__ __forceinline__ void adj_halo(const PoolView<Real> &v, int blk, int i, int t, int &f, int &lab, int &sc,
+                                         int &nb)
+{
+    const int plus = (t >> 6) & 1, a = t & 7, b = (t >> 3) & 7;
+    f = 2 * i + plus;
+    const int cl = plus ? kBS : -1, cs = plus ? 0 : kBS - 1;
+    if (i == 0) {
+        lab = lab_a(cl, a, b);
+        sc = cs + kBS * (a + kBS * b);
+    } else if (i == 1) {
+        lab = lab_a(a, cl, b);
+        sc = a + kBS * (cs + kBS * b);
+    } else {
+        lab = lab_a(a, b, cl);
+        sc = a + kBS * (b + kBS * cs);
+    }
+    if (v.log2_bpd >= 0) {  // bx | by << L | bz << 2L, periodic
+        const int L = v.log2_bpd, m = (1 << L) - 1, s = plus ? 1 : -1, sh = i * L;
+        nb = (blk & ~(m << sh)) | ((((blk >> sh) + s) & m) << sh);
+    } else {
+        nb = v.nbr[blk * 6 + f];
+    }
+}
+
 // phi_k of the four cells of thread t and its three face-halo cells
 template <typename Real>
 __device__ __forceinline__ void adj_load_phi(const PoolView<Real> &v, int blk, const Real *__restrict__ phi,
@@ -608,12 +638,20 @@ __device__ __forceinline__ void adj_load_phi(const PoolView<Real> &v, int blk, c
     for (int i = 0; i < 4; i++) p[i] = phi[base + c0 + 64 * i];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        const int q = t + 128 * i;
-        int lx, ly, lz, sc;
-        face_cell(q >> 6, q & 63, lx, ly, lz, sc);
-        halo[i] = phi[(int64_t)face_neighbour(v, blk, q >> 6) * kBS3 + sc];
+        int f, lab, sc, nb;
+        adj_halo(v, blk, i, t, f, lab, sc, nb);
+        halo[i] = phi[(int64_t)nb * kBS3 + sc];
     }
 }
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // kMode: 0 middle, 1 first (lambda_N given), 2 last (write lambda_0); kAbs:
 // also sum the magnitudes of the gradient terms (grad_acc slots 4, 5)
@@ -633,7 +671,18 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
     __shared__ unsigned char sfl[kALab];
     __shared__ unsigned char sst[8];
     __shared__ double red[kAbs ? 6 : 4][4];
+    __shared__ __align__(16) double sacc[kAbs ? 6 : 4];  // this block's gradient slots, prefetched
     const int blk = blocks ? blocks[blockIdx.x] : (int)blockIdx.x, t = threadIdx.x;
+    // thread 0 copies the block's gradient slots into shared memory once the
+    // launch is known to reach its end (cp.async: no register held, no wait
+    // until the slots are updated), so that their load is not the CTA's last
+    // round trip; every return after the copy waits for it first
+    auto prefetch_acc = [&]() {
+        const double *a = grad_acc + (int64_t)blk * kGradSlots;
+        cp_async16(sacc, a);
+        cp_async16(sacc + 2, a + 2);
+        if constexpr (kAbs) cp_async16(sacc + 4, a + 4);
+    };
     const double ih2 = ih2blk[blk];
     if constexpr (kHsm) {
         static_assert(kFacesPerBlock % 4 == 0, "float4 copies");
@@ -663,6 +712,7 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
         mw[0] = mw[1] = mw[2] = mw[3] = mm;
     }
     pdl_wait_then_release();
+    if (kMode == 1 && t == 0) prefetch_acc();
     Real p[4], ph_halo[3];
     if constexpr (kEarlyPhi) adj_load_phi(v, blk, phi, base, c0, t, p, ph_halo);
 
@@ -688,6 +738,7 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
             }
             return;
         }
+        if (kMode == 0 && t == 0) prefetch_acc();
         const Real *mu_p = (const Real *)prev.mu;
         const bool own = !(self & kAdjMuZero);
         Real m[4];
@@ -704,13 +755,9 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
             }
 #pragma unroll
             for (int i = 0; i < 3; i++) {
-                const int q = t + 128 * i;
-                const int f = q >> 6, pc = q & 63;
-                int lx, ly, lz, sc;
-                face_cell(f, pc, lx, ly, lz, sc);
-                const int l = lab_a(lx, ly, lz);
+                int f, l, sc, nb;
+                adj_halo(v, blk, i, t, f, l, sc, nb);
                 if (sst[f] == kAdjDom) {
-                    const int nb = face_neighbour(v, blk, f);
                     sm[l] = mu_p[(int64_t)nb * kBS3 + sc];
                     sfl[l] = prev.flags[(int64_t)nb * kBS3 + sc];
                 } else {
@@ -779,7 +826,10 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
             nz |= o[i] != (Real)0;
         }
         if (!__syncthreads_or(nz)) {
-            if (t == 0) out.status[blk] = kAdjMuZero;
+            if (t == 0) {
+                out.status[blk] = kAdjMuZero;
+                cp_async_wait_all();
+            }
             return;
         }
 #pragma unroll
@@ -787,7 +837,10 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
             mu_o[base + c0 + 64 * i] = o[i];
             out.flags[base + c0 + 64 * i] = 0;
         }
-        if (t == 0) out.status[blk] = 0;
+        if (t == 0) {
+            out.status[blk] = 0;
+            cp_async_wait_all();
+        }
         return;
     }
     Real *ph = sm;
@@ -795,10 +848,9 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
     for (int i = 0; i < 4; i++) ph[l0 + kAPlane * i] = p[i];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        const int q = t + 128 * i;
-        int lx, ly, lz, sc;
-        face_cell(q >> 6, q & 63, lx, ly, lz, sc);
-        ph[lab_a(lx, ly, lz)] = ph_halo[i];
+        int f, lab, sc, nb;
+        adj_halo(v, blk, i, t, f, lab, sc, nb);
+        ph[lab] = ph_halo[i];
     }
     __syncthreads();
     const Real eps = (Real)0.1;
@@ -923,14 +975,20 @@ adj_fused_kernel(PoolView<Real> v, const Real *__restrict__ H, const unsigned sh
             neumaier_add(red[2][0], red[3][0], red[2][w]);
             neumaier_add(red[2][0], red[3][0], red[3][w]);
         }
+        cp_async_wait_all();
+        double a0 = sacc[0], a1 = sacc[1], a2 = sacc[2], a3 = sacc[3];
+        neumaier_add(a0, a1, red[0][0]);
+        neumaier_add(a0, a1, red[1][0]);
+        neumaier_add(a2, a3, red[2][0]);
+        neumaier_add(a2, a3, red[3][0]);
         double *acc = grad_acc + (int64_t)blk * kGradSlots;
-        neumaier_add(acc[0], acc[1], red[0][0]);
-        neumaier_add(acc[0], acc[1], red[1][0]);
-        neumaier_add(acc[2], acc[3], red[2][0]);
-        neumaier_add(acc[2], acc[3], red[3][0]);
+        acc[0] = a0;
+        acc[1] = a1;
+        acc[2] = a2;
+        acc[3] = a3;
         if constexpr (kAbs) {
-            acc[4] += red[4][0] + red[4][1] + red[4][2] + red[4][3];
-            acc[5] += red[5][0] + red[5][1] + red[5][2] + red[5][3];
+            acc[4] = sacc[4] + (red[4][0] + red[4][1] + red[4][2] + red[4][3]);
+            acc[5] = sacc[5] + (red[5][0] + red[5][1] + red[5][2] + red[5][3]);
         }
     }
 }
