@@ -1652,6 +1652,11 @@ int forward_adjoint_impl(gbfk_ctx *ctx, const gbfk_adjoint_params *p, gbfk_adjoi
     auto release = [&]() {
         cudaStreamSynchronize(ctx->stream);
         if (ctx->adj_fstream) cudaStreamSynchronize(ctx->adj_fstream);
+        // the per-buffer events belong to the buffers being freed
+        for (auto *m : {&ctx->adj_ev_write, &ctx->adj_ev_read}) {
+            for (auto &kv : *m) cudaEventDestroy(kv.second);
+            m->clear();
+        }
         for (void *q : ctx->adj_mem)
             if (q) cudaFree(q);
         ctx->adj_mem.clear();
